@@ -1,0 +1,62 @@
+"""ctypes access to ``oracle/_ref/lib<config>.so`` (see build_ref.py, ref_harness.c).
+
+TEST INFRASTRUCTURE ONLY.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+
+def available(config: str) -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "lib%s.so" % config))
+
+
+class RefOracle:
+    """The reference C backend for one grammar configuration."""
+
+    def __init__(self, config: str):
+        path = os.path.join(REF_DIR, "lib%s.so" % config)
+        if not os.path.exists(path):
+            raise FileNotFoundError("%s missing: run oracle/build_ref.py %s" % (path, config))
+        self.config = config
+        self.lib = ctypes.CDLL(path)
+        self.lib.ref_run_case.argtypes = [ctypes.c_uint64, ctypes.c_char_p,
+                                          ctypes.POINTER(ctypes.POINTER(ctypes.c_uint8)),
+                                          ctypes.POINTER(ctypes.c_size_t)]
+        self.lib.ref_run_case.restype = ctypes.c_int
+        self.lib.ref_pipeline.argtypes = [ctypes.c_uint64, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64),
+                                          ctypes.POINTER(ctypes.c_uint64)]
+        self.lib.ref_pipeline.restype = ctypes.c_int
+        self.lib.ref_free.argtypes = [ctypes.c_void_p]
+        self.lib.ref_layout.argtypes = [ctypes.POINTER(ctypes.c_uint64)]
+
+    def run_case(self, data: bytes) -> bytes:
+        """The exact response record ``run_case`` writes for ``data``."""
+        out = ctypes.POINTER(ctypes.c_uint8)()
+        n = ctypes.c_size_t()
+        if self.lib.ref_run_case(len(data), data, ctypes.byref(out), ctypes.byref(n)) != 0:
+            raise RuntimeError("open_memstream failed")
+        try:
+            return ctypes.string_at(out, n.value)
+        finally:
+            self.lib.ref_free(out)
+
+    def pipeline(self, buf, n=None):
+        """lex -> parse -> parents -> compact without serialisation.
+        ``buf`` is anything exposing a buffer address (numpy array / bytes)."""
+        import numpy as np
+        a = np.frombuffer(buf, dtype=np.uint8) if isinstance(buf, (bytes, bytearray)) else buf
+        nt = ctypes.c_uint64()
+        nn = ctypes.c_uint64()
+        ok = self.lib.ref_pipeline(len(a) if n is None else n, a.ctypes.data, ctypes.byref(nt), ctypes.byref(nn))
+        return bool(ok), nt.value, nn.value
+
+    def layout(self):
+        s = (ctypes.c_uint64 * 4)()
+        self.lib.ref_layout(s)
+        return tuple(s)

@@ -1,0 +1,76 @@
+/*
+ * In-memory harness around the reference's generated C program (oracle/_ref).
+ *
+ * TEST INFRASTRUCTURE ONLY: used by the tests and by bench.py's CPU-baseline
+ * leg as the checker / baseline, never by the product path.
+ *
+ * The generated program (assembled by oracle/build_ref.py from the reference's
+ * backends/c/{lexer,parser,cli}.c and its run_case text) is #included with its
+ * main() renamed, so its static functions can be called directly:
+ *   - ref_run_case: the exact response record bytes that run_case
+ *     (src/Alpacc/Generator/C/Generator.hs:114-152) writes, captured with
+ *     open_memstream;
+ *   - ref_pipeline: lex_string -> parse_test -> compute_parents -> compact_tree
+ *     without serialisation, the in-memory timing harness for the CPU baseline;
+ *   - ref_layout: the type sizes print_layout reports.
+ */
+#define main alpacc_generated_main
+#include ALPACC_GENERATED
+#undef main
+
+int ref_run_case(uint64_t n, const uint8_t *in, uint8_t **out, size_t *out_len) {
+  char *buf = NULL;
+  size_t len = 0;
+  FILE *f = open_memstream(&buf, &len);
+  if (!f) return -1;
+  run_case(n, in, f);
+  fclose(f);
+  *out = (uint8_t *)buf;
+  *out_len = len;
+  return 0;
+}
+
+void ref_free(void *p) { free(p); }
+
+/* Returns 1 when accepted (sets the counts), 0 when rejected. */
+int ref_pipeline(uint64_t n, const uint8_t *in, uint64_t *num_tokens, uint64_t *num_nodes) {
+  lexeme_t *lexemes;
+  uint64_t num_lexemes;
+  *num_tokens = 0;
+  *num_nodes = 0;
+  if (!lex_string(in, n, &lexemes, &num_lexemes)) return 0;
+  terminal_t *tokens = (terminal_t *)malloc((num_lexemes ? num_lexemes : 1) * sizeof(terminal_t));
+  for (uint64_t i = 0; i < num_lexemes; i++) tokens[i] = lexemes[i].terminal;
+  production_t *prods;
+  uint64_t num_prods;
+  if (!parse_test(tokens, num_lexemes, &prods, &num_prods)) {
+    free(tokens);
+    free(lexemes);
+    return 0;
+  }
+  free(tokens);
+  index_t *parents = (index_t *)malloc((num_prods ? num_prods : 1) * sizeof(index_t));
+  compute_parents(prods, num_prods, parents);
+  production_t *tree_prods = (production_t *)malloc((num_prods ? num_prods : 1) * sizeof(production_t));
+  index_t *tree_parents = (index_t *)malloc((num_prods ? num_prods : 1) * sizeof(index_t));
+  index_t *token_parents = (index_t *)malloc((num_lexemes ? num_lexemes : 1) * sizeof(index_t));
+  int ok = compact_tree(prods, num_prods, parents, num_lexemes, tree_prods, tree_parents, token_parents);
+  if (ok) {
+    *num_tokens = num_lexemes;
+    *num_nodes = num_prods - num_lexemes;
+  }
+  free(prods);
+  free(parents);
+  free(lexemes);
+  free(tree_prods);
+  free(tree_parents);
+  free(token_parents);
+  return ok ? 1 : 0;
+}
+
+void ref_layout(uint64_t *sizes) {
+  sizes[0] = sizeof(terminal_t);
+  sizes[1] = sizeof(production_t);
+  sizes[2] = sizeof(index_t);
+  sizes[3] = sizeof(length_t);
+}
