@@ -1,0 +1,203 @@
+// Shared device utilities for the sm_100a lex + parse kernels.
+//
+// * Status words: every kernel reports into a DeviceStatus in device memory
+//   (reject / error / timeout) instead of trapping, so a bad input or an
+//   exhausted wait never faults or hangs the GPU.
+// * Tile publication for single-pass scans: payload words are written first,
+//   then a flag with release semantics; readers spin on the flag with acquire
+//   semantics and a bounded number of iterations (decoupled look-back,
+//   Merrill & Garland 2016). A wait that runs out records ALPACC_E_TIMEOUT and
+//   the kernel proceeds with a neutral value, so every CTA still finishes.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace alpacc {
+
+constexpr int kWarp = 32;
+
+// Where a bounded wait gave up (recorded in DeviceStatus::timeout_site).
+enum TimeoutSite : int {
+  kSiteNone = 0,
+  kSiteLexState = 1,
+  kSiteLexCount = 2,
+  kSitePairs = 3,
+  kSitePse = 4,
+  kSiteCompact = 5,
+};
+
+struct DeviceStatus {
+  int reject;        // 1 when the input is rejected
+  int error;         // ALPACC_E_* (negative) on an internal failure
+  int timeout_site;  // TimeoutSite of the first wait that ran out
+  int reserved;
+  unsigned long long num_tokens;
+  unsigned long long num_brackets;
+  unsigned long long num_productions;
+  unsigned long long num_nodes;
+  int lex_reject_reason;    // 1 dead state, 2 not accepting, 3 length overflow
+  int parse_reject_reason;  // 1 missing pair, 2 bracket mismatch, 3 unbalanced, 4 terminal count
+  unsigned long long scratch[4];
+};
+
+// Upper bound on spin iterations of one wait; with the back-off below this is
+// several seconds, far beyond any legitimate wait on a healthy device.
+constexpr unsigned kSpinLimit = 1u << 22;
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ void record_timeout(DeviceStatus *st, int site) {
+  atomicCAS(&st->timeout_site, 0, site);
+  atomicCAS(&st->error, 0, -5 /* ALPACC_E_TIMEOUT */);
+}
+
+__device__ __forceinline__ void record_reject(DeviceStatus *st, int *reason, int why) {
+  if (st->reject == 0) atomicExch(&st->reject, 1);
+  if (reason) atomicCAS(reason, 0, why);
+}
+
+// Spin until *flag >= want (acquire). Returns the flag value, or 0 after the
+// iteration limit (and records a timeout).
+__device__ __forceinline__ unsigned wait_flag(const unsigned *flag, unsigned want, DeviceStatus *st, int site) {
+  unsigned ns = 32;
+  for (unsigned it = 0; it < kSpinLimit; ++it) {
+    unsigned v = ld_acquire_u32(flag);
+    if (v >= want) return v;
+    if (*reinterpret_cast<volatile int *>(&st->error) != 0) return 0;  // a CTA already failed
+    __nanosleep(ns);
+    if (ns < 1024) ns <<= 1;
+  }
+  record_timeout(st, site);
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Block-wide scans (warp shuffles + one shared-memory pass).
+// ---------------------------------------------------------------------------
+
+template <typename T, typename Op>
+__device__ __forceinline__ T warp_inclusive_scan(T v, Op op) {
+  const int lane = threadIdx.x & (kWarp - 1);
+#pragma unroll
+  for (int d = 1; d < kWarp; d <<= 1) {
+    T o = __shfl_up_sync(0xffffffffu, v, d);
+    if (lane >= d) v = op(o, v);
+  }
+  return v;
+}
+
+// Exclusive scan over the block; `identity` is the neutral element. Returns
+// this thread's exclusive prefix and writes the block total to *total.
+// `smem` needs (blockDim.x / 32) elements.
+template <typename T, typename Op>
+__device__ __forceinline__ T block_exclusive_scan(T v, Op op, T identity, T *smem, T *total) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  T inc = warp_inclusive_scan(v, op);
+  if (lane == kWarp - 1) smem[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    T w = lane < nwarps ? smem[lane] : identity;
+    T wi = warp_inclusive_scan(w, op);
+    if (lane < nwarps) smem[lane] = wi;  // inclusive prefix of warp totals
+  }
+  __syncthreads();
+  T warp_prefix = warp == 0 ? identity : smem[warp - 1];
+  T excl_in_warp = __shfl_up_sync(0xffffffffu, inc, 1);
+  if (lane == 0) excl_in_warp = identity;
+  T res = op(warp_prefix, excl_in_warp);
+  *total = smem[nwarps - 1];
+  __syncthreads();
+  return res;
+}
+
+struct AddU64 {
+  __device__ __forceinline__ unsigned long long operator()(unsigned long long a, unsigned long long b) const {
+    return a + b;
+  }
+};
+struct AddI64 {
+  __device__ __forceinline__ long long operator()(long long a, long long b) const { return a + b; }
+};
+struct MaxI64 {
+  __device__ __forceinline__ long long operator()(long long a, long long b) const { return a > b ? a : b; }
+};
+struct MinI64 {
+  __device__ __forceinline__ long long operator()(long long a, long long b) const { return a < b ? a : b; }
+};
+
+// A pair scanned component-wise (used for (count, position) and (brackets,
+// productions) carries).
+struct Pair64 {
+  long long a, b;
+};
+
+// ---------------------------------------------------------------------------
+// Decoupled look-back over tiles for an associative pair carry.
+//
+// Tile i publishes its aggregate (flag 1) as soon as it is known and its
+// inclusive prefix (flag 2) once the look-back resolved. A tile walks back
+// from i-1, combining aggregates until it meets an inclusive prefix.
+// `tiles` holds per tile: flag (u32) in flags[i], aggregate in agg[i], inclusive
+// in inc[i] (two u64 each).
+// ---------------------------------------------------------------------------
+
+struct PairTileState {
+  unsigned *flags;            // [num_tiles]
+  unsigned long long *agg;    // [num_tiles * 2]
+  unsigned long long *inc;    // [num_tiles * 2]
+};
+
+template <typename Op>
+__device__ __forceinline__ Pair64 combine(Pair64 x, Pair64 y, Op op) {
+  return op(x, y);
+}
+
+__device__ __forceinline__ void publish_pair(PairTileState ts, long long tile, Pair64 v, bool inclusive) {
+  unsigned long long *dst = inclusive ? ts.inc : ts.agg;
+  st_relaxed_u64(dst + 2 * tile, (unsigned long long)v.a);
+  st_relaxed_u64(dst + 2 * tile + 1, (unsigned long long)v.b);
+  __threadfence();
+  st_release_u32(ts.flags + tile, inclusive ? 2u : 1u);
+}
+
+// Exclusive prefix of tile `tile` (called by one thread). `op(earlier, later)`.
+template <typename Op>
+__device__ Pair64 lookback_pair(PairTileState ts, long long tile, Pair64 identity, Op op, DeviceStatus *st, int site) {
+  Pair64 acc = identity;
+  long long j = tile - 1;
+  while (j >= 0) {
+    unsigned f = wait_flag(ts.flags + j, 1u, st, site);
+    if (f == 0) return acc;  // timed out: neutral continuation
+    if (f >= 2) {
+      Pair64 v{(long long)ld_relaxed_u64(ts.inc + 2 * j), (long long)ld_relaxed_u64(ts.inc + 2 * j + 1)};
+      return op(v, acc);
+    }
+    Pair64 v{(long long)ld_relaxed_u64(ts.agg + 2 * j), (long long)ld_relaxed_u64(ts.agg + 2 * j + 1)};
+    acc = op(v, acc);
+    --j;
+  }
+  return acc;
+}
+
+}  // namespace alpacc

@@ -1,0 +1,67 @@
+// Device forms of alpacc's grammar tables, derived once per grammar on the host.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/alpacc_b200.h"
+
+namespace alpacc {
+
+constexpr int kMaxLanes = 16;     // distinct live states a chunk may start with
+constexpr int kMaxMachine = 255;  // states of the minimised lexer automaton (u8)
+
+// The sequential lexer of backends/c/lexer.c run over encoded endomorphism
+// states is a Moore machine: state = encoded state_t, input = byte,
+// delta(s, b) = COMPOSE[idx(s)][idx(TO_STATE[b])], outputs terminal(s),
+// produce(s) and ACCEPT[idx(s)]. This is that machine restricted to the states
+// reachable from IDENTITY and minimised, with bytes grouped into classes that
+// act identically. Running it reproduces lex_string exactly.
+struct LexerMachine {
+  int M = 0;                  // states
+  int C = 0;                  // byte classes
+  int m0 = 0;                 // state for IDENTITY (before the first byte)
+  int dead = -1;              // absorbing non-accepting state, or -1
+  int max_lanes = 0;          // largest number of distinct live targets of a class
+  int reachable = 0;          // endomorphism states reachable from IDENTITY
+  std::vector<uint8_t> cls;   // [256] byte -> class
+  std::vector<uint8_t> trans; // [M*C] next state
+  std::vector<uint8_t> term;  // [M] terminal of the state
+  std::vector<uint8_t> flags; // [M] bit0 produce, bit1 accept, bit2 kept (terminal != ignore)
+  std::vector<uint8_t> img;       // [C*kMaxLanes] distinct live targets of each class
+  std::vector<uint8_t> img_cnt;   // [C]
+  std::vector<uint8_t> lane_of;   // [C*M] slot of trans[s][c] in img[c] or 0xff (dead)
+};
+
+// LLP pair table as a dense array indexed by the key's terminals in base NT
+// (NT = END + 1): entry = record index or 0xffffffff when the reference's
+// lookup_key (backends/c/parser.c:17-45) would fail for that key.
+struct PairTable {
+  int nt = 0;                     // terminal ids 0..nt-1
+  int q = 0, k = 0;
+  uint64_t dense_size = 0;
+  std::vector<uint32_t> dense;    // [nt^(q+k)]
+  // record r: STACKS[rec_ss[r] .. +rec_nb[r]) and PRODUCTIONS[rec_ps[r] .. +rec_np[r])
+  std::vector<uint32_t> rec_ss, rec_ps;
+  std::vector<uint8_t> rec_nb, rec_np;
+  std::vector<uint32_t> stacks;   // bracket: bit31 = left, low bits = unpacked symbol
+  std::vector<uint32_t> prods;    // production ids
+  std::vector<int32_t> arity;     // per production
+  std::vector<uint8_t> is_term;   // per production: terminal production flag
+  int max_br = 0, max_pr = 0;
+};
+
+struct HostGrammar {
+  alpacc_tables t;    // widths and scalars (pointers not retained)
+  LexerMachine lex;
+  PairTable pairs;
+  uint64_t len_max = 0;
+  int ignore = -1;
+};
+
+// Validates the tables and builds the device forms. Returns ALPACC_OK or an
+// error code with a message in *why.
+int build_host_grammar(const alpacc_tables *t, HostGrammar *out, std::string *why);
+
+}  // namespace alpacc

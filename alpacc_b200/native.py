@@ -1,0 +1,264 @@
+"""ctypes binding of the C ABI (include/alpacc_b200.h) and the host-side mirror
+of a generated parser's interface.
+
+``Parser(tables)`` uploads one grammar to the GPU; ``parse(data)`` is the
+in-memory form of the generated program's ``run_case`` for combined mode
+(src/Alpacc/Generator/C/Generator.hs:114-152): it returns a
+``wire.ParseResult`` that is either a reject or the tokens with spans plus the
+preorder production tree with parents and token parents. ``run_case(data)``
+returns the exact response record bytes.
+
+There is no CPU fallback: constructing a ``Parser`` without the native library
+or without a GPU raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import wire
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libalpacc_b200.so")
+
+OK, REJECT = 0, 1
+E_INVALID, E_CUDA, E_NOMEM, E_CAPACITY, E_TIMEOUT, E_UNSUPPORTED = -1, -2, -3, -4, -5, -6
+ABI_VERSION = 1
+
+
+class AlpaccError(RuntimeError):
+    def __init__(self, status: int, msg: str = ""):
+        super().__init__("alpacc status %d: %s" % (status, msg))
+        self.status = status
+
+
+class Tables(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", ctypes.c_uint32), ("terminal_size", ctypes.c_uint32), ("production_size", ctypes.c_uint32),
+        ("bracket_size", ctypes.c_uint32), ("state_size", ctypes.c_uint32), ("index_size", ctypes.c_uint32),
+        ("length_size", ctypes.c_uint32), ("reserved0", ctypes.c_uint32),
+        ("num_states", ctypes.c_uint64), ("endo_mask", ctypes.c_uint64), ("endo_offset", ctypes.c_uint64),
+        ("terminal_mask", ctypes.c_uint64), ("terminal_offset", ctypes.c_uint64), ("produce_mask", ctypes.c_uint64),
+        ("produce_offset", ctypes.c_uint64), ("identity", ctypes.c_uint64), ("ignore_token", ctypes.c_int64),
+        ("to_state", ctypes.c_void_p), ("compose", ctypes.c_void_p), ("accept", ctypes.c_void_p),
+        ("q", ctypes.c_uint64), ("k", ctypes.c_uint64), ("empty_terminal", ctypes.c_uint64),
+        ("start_terminal", ctypes.c_uint64), ("end_terminal", ctypes.c_uint64), ("hash_table_size", ctypes.c_uint64),
+        ("max_iters", ctypes.c_uint64), ("stacks_size", ctypes.c_uint64), ("productions_size", ctypes.c_uint64),
+        ("max_brackets_per_position", ctypes.c_uint64), ("max_prods_per_position", ctypes.c_uint64),
+        ("stacks", ctypes.c_void_p), ("productions", ctypes.c_void_p), ("hash_table_is_valid", ctypes.c_void_p),
+        ("hash_table_keys", ctypes.c_void_p), ("hash_table_stacks_span", ctypes.c_void_p),
+        ("hash_table_productions_span", ctypes.c_void_p), ("number_of_productions", ctypes.c_uint64),
+        ("production_to_arity", ctypes.c_void_p), ("production_to_terminal_is_valid", ctypes.c_void_p),
+    ]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [
+        ("valid", ctypes.c_uint8), ("on_device", ctypes.c_uint8), ("reserved0", ctypes.c_uint16),
+        ("reserved1", ctypes.c_uint32), ("num_tokens", ctypes.c_uint64), ("num_nodes", ctypes.c_uint64),
+        ("token_ids", ctypes.c_void_p), ("token_starts", ctypes.c_void_p), ("token_lengths", ctypes.c_void_p),
+        ("node_productions", ctypes.c_void_p), ("node_parents", ctypes.c_void_p), ("token_parents", ctypes.c_void_p),
+        ("internal", ctypes.c_void_p),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """The native library; raises when it is not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise AlpaccError(E_INVALID, "native library missing: %s (run python -m alpacc_b200.build)" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        L.alpacc_gpu_load.restype = ctypes.c_void_p
+        L.alpacc_gpu_load.argtypes = [ctypes.POINTER(Tables), ctypes.c_int, ctypes.c_uint64,
+                                      ctypes.POINTER(ctypes.c_int)]
+        L.alpacc_gpu_free.argtypes = [ctypes.c_void_p]
+        for name in ("alpacc_gpu_parse", "alpacc_gpu_parse_device"):
+            f = getattr(L, name)
+            f.restype = ctypes.c_int
+            f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Result)]
+        L.alpacc_gpu_enqueue.restype = ctypes.c_int
+        L.alpacc_gpu_enqueue.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64]
+        L.alpacc_gpu_collect.restype = ctypes.c_int
+        L.alpacc_gpu_collect.argtypes = [ctypes.c_void_p, ctypes.POINTER(Result)]
+        L.alpacc_gpu_parse_batch.restype = ctypes.c_int
+        L.alpacc_gpu_parse_batch.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                             ctypes.POINTER(Result)]
+        L.alpacc_result_free.argtypes = [ctypes.POINTER(Result)]
+        L.alpacc_gpu_layout.restype = ctypes.c_int
+        L.alpacc_gpu_layout.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
+        L.alpacc_strerror.restype = ctypes.c_char_p
+        L.alpacc_strerror.argtypes = [ctypes.c_int]
+        L.alpacc_gpu_last_ms.restype = ctypes.c_double
+        L.alpacc_gpu_last_ms.argtypes = [ctypes.c_void_p]
+        L.alpacc_gpu_info.restype = ctypes.c_int
+        L.alpacc_gpu_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
+        L.alpacc_gpu_last_error.restype = ctypes.c_char_p
+        L.alpacc_gpu_last_error.argtypes = [ctypes.c_void_p]
+        _lib = L
+    return _lib
+
+
+def make_tables(t):
+    """Fill the C struct from generated tables; returns (struct, keepalive)."""
+    L = t.lexer
+    keep = []
+
+    def arr(a, dtype=None):
+        a = np.ascontiguousarray(a if dtype is None else np.asarray(a).astype(dtype))
+        keep.append(a)
+        return a.ctypes.data
+
+    s = Tables()
+    s.abi_version = ABI_VERSION
+    s.terminal_size = t.terminal_bits // 8
+    s.production_size = t.production_bits // 8
+    s.bracket_size = t.bracket_bits // 8
+    s.state_size = L.state_bits // 8
+    s.index_size = t.index_bits // 8
+    s.length_size = t.length_bits // 8
+    s.num_states = L.num_states
+    s.endo_mask, s.endo_offset = L.index_mask, L.index_offset
+    s.terminal_mask, s.terminal_offset = L.token_mask, L.token_offset
+    s.produce_mask, s.produce_offset = L.produce_mask, L.produce_offset
+    s.identity = L.identity
+    s.ignore_token = -1 if t.ignore_token is None else t.ignore_token
+    s.to_state = arr(L.to_state)
+    s.compose = arr(L.compose)
+    s.accept = arr(L.accept, np.uint8)
+    s.q, s.k = t.q, t.k
+    s.empty_terminal, s.start_terminal, s.end_terminal = t.empty_terminal, t.start_terminal, t.end_terminal
+    s.hash_table_size = t.hash_size
+    s.max_iters = t.max_iters
+    s.stacks_size, s.productions_size = len(t.stacks), len(t.productions)
+    s.max_brackets_per_position, s.max_prods_per_position = t.max_brackets_per_pos, t.max_prods_per_pos
+    s.stacks = arr(t.stacks)
+    s.productions = arr(t.productions)
+    s.hash_table_is_valid = arr(t.ht_valid, np.uint8)
+    tw = {1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}[t.terminal_bits // 8]
+    s.hash_table_keys = arr(t.ht_keys, tw)
+    s.hash_table_stacks_span = arr(t.ht_stack_span, np.int64)
+    s.hash_table_productions_span = arr(t.ht_prod_span, np.int64)
+    s.number_of_productions = t.num_productions
+    s.production_to_arity = arr(t.arity, np.uint64)
+    s.production_to_terminal_is_valid = arr(t.prod_is_terminal, np.uint8)
+    return s, keep
+
+
+def _np_from(ptr, count, nbytes, signed=False):
+    if count == 0:
+        return np.zeros(0, dtype=np.dtype(("i" if signed else "u") + str(nbytes)))
+    dt = np.dtype(("i" if signed else "u") + str(nbytes))
+    buf = (ctypes.c_char * (count * nbytes)).from_address(ptr)
+    return np.frombuffer(buf, dtype=dt, count=count).copy()
+
+
+class Parser:
+    """One grammar resident on one GPU (``alpacc_gpu_load``)."""
+
+    def __init__(self, tables, device: int = 0, max_input: int = 0):
+        self.tables = tables
+        self.layout = wire.Layout.of(tables)
+        self._struct, self._keep = make_tables(tables)
+        err = ctypes.c_int(0)
+        self._h = lib().alpacc_gpu_load(ctypes.byref(self._struct), device, max_input, ctypes.byref(err))
+        if not self._h:
+            raise AlpaccError(err.value, lib().alpacc_strerror(err.value).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().alpacc_gpu_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def info(self) -> dict:
+        vals = (ctypes.c_int64 * 16)()
+        n = lib().alpacc_gpu_info(self._h, vals, 16)
+        keys = ["M", "C", "max_lanes", "reachable", "dead", "nt", "records", "trans_rep", "lex_reject_reason",
+                "parse_reject_reason", "timeout_site"]
+        return dict(zip(keys, [vals[i] for i in range(min(n, len(keys)))]))
+
+    def _check(self, rc: int) -> int:
+        if rc < 0:
+            raise AlpaccError(rc, "%s (%s)" % (lib().alpacc_strerror(rc).decode(),
+                                              lib().alpacc_gpu_last_error(self._h).decode()))
+        return rc
+
+    def _result(self, r: Result, rc: int) -> wire.ParseResult:
+        if rc != OK:
+            return wire.ParseResult(False)
+        lay = self.layout
+        T, N = r.num_tokens, r.num_nodes
+        return wire.ParseResult(
+            True,
+            _np_from(r.token_ids, T, lay.terminal), _np_from(r.token_starts, T, lay.index, True),
+            _np_from(r.token_lengths, T, lay.length), _np_from(r.node_productions, N, lay.production),
+            _np_from(r.node_parents, N, lay.index, True), _np_from(r.token_parents, T, lay.index, True))
+
+    def parse(self, data) -> wire.ParseResult:
+        """Host bytes in, host result out (H2D, device path, D2H)."""
+        a = np.frombuffer(bytes(data), dtype=np.uint8) if not isinstance(data, np.ndarray) else data
+        a = np.ascontiguousarray(a, dtype=np.uint8)
+        r = Result()
+        rc = self._check(lib().alpacc_gpu_parse(self._h, a.ctypes.data, a.size, ctypes.byref(r)))
+        try:
+            return self._result(r, rc)
+        finally:
+            lib().alpacc_result_free(ctypes.byref(r))
+
+    def parse_device(self, dev_ptr: int, n: int):
+        """Bytes already on the device. Returns (status, Result with device pointers)."""
+        r = Result()
+        rc = self._check(lib().alpacc_gpu_parse_device(self._h, dev_ptr, n, ctypes.byref(r)))
+        return rc, r
+
+    def device_result(self, r: Result, rc: int) -> wire.ParseResult:
+        """Copy a device result (from ``parse_device``) to host arrays."""
+        if rc != OK:
+            return wire.ParseResult(False)
+        import torch
+
+        lay = self.layout
+
+        def dl(ptr, count, nbytes, signed=False):
+            if count == 0:
+                return np.zeros(0, dtype=np.dtype(("i" if signed else "u") + str(nbytes)))
+            host = np.empty(count * nbytes, dtype=np.uint8)
+            torch.cuda.synchronize()
+            _cudart_memcpy_d2h(host.ctypes.data, ptr, count * nbytes)
+            return host.view(np.dtype(("i" if signed else "u") + str(nbytes)))
+
+        T, N = r.num_tokens, r.num_nodes
+        return wire.ParseResult(True, dl(r.token_ids, T, lay.terminal), dl(r.token_starts, T, lay.index, True),
+                                dl(r.token_lengths, T, lay.length), dl(r.node_productions, N, lay.production),
+                                dl(r.node_parents, N, lay.index, True), dl(r.token_parents, T, lay.index, True))
+
+    def run_case(self, data) -> bytes:
+        """The response record bytes ``run_case`` would write."""
+        return wire.encode_record(self.parse(data), self.layout)
+
+    def last_ms(self) -> float:
+        return lib().alpacc_gpu_last_ms(self._h)
+
+
+_cudart = None
+
+
+def _cudart_memcpy_d2h(dst: int, src: int, nbytes: int):
+    global _cudart
+    if _cudart is None:
+        import glob
+        cands = glob.glob("/usr/local/cuda/lib64/libcudart.so*")
+        _cudart = ctypes.CDLL(cands[0]) if cands else ctypes.CDLL("libcudart.so")
+        _cudart.cudaMemcpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    rc = _cudart.cudaMemcpy(dst, src, nbytes, 2)
+    if rc != 0:
+        raise AlpaccError(E_CUDA, "cudaMemcpy failed (%d)" % rc)

@@ -1,0 +1,194 @@
+/*
+ * alpacc_b200 — C ABI of the B200 (sm_100a) lex + LLP-parse path.
+ *
+ * A drop-in for the combined-mode ``run_case`` of a program generated by
+ * alpacc (CoderDue/alpacc): bytes in, and either reject or the token sequence
+ * with spans plus the preorder production tree with parent indices out.
+ *
+ * Reference interfaces replaced (paths within the alpacc project):
+ *   - the grammar constants a generated program bakes in, emitted by
+ *     src/Alpacc/Generator/C/Lexer.hs:16-58 (TO_STATE, COMPOSE, ACCEPT, masks,
+ *     IDENTITY, IGNORE_TOKEN) and src/Alpacc/Generator/C/Parser.hs:21-95
+ *     (Q, K, sentinels, hash table, STACKS, PRODUCTIONS, arities,
+ *     PRODUCTION_TO_TERMINAL_IS_VALID)                  -> alpacc_tables
+ *   - the per-input device set-up of the CUDA backend
+ *     (backends/cuda/cli.cu:739-792 ``both_one``, lexer.cu:274-302 ``LexerCtx``,
+ *     parser.cu:700-811 ``allocParserFused``)           -> alpacc_gpu_load
+ *   - ``run_case(uint64_t n, const uint8_t *in, FILE *out)``
+ *     (src/Alpacc/Generator/C/Generator.hs:114-152)      -> alpacc_gpu_run_case
+ *     and its in-memory form                            -> alpacc_gpu_parse
+ *   - ``print_layout`` (C/Generator.hs:153-158, cli.c --layout)
+ *                                                       -> alpacc_gpu_layout
+ *
+ * Results are bit-identical to the reference's C backend (backends/c/lexer.c,
+ * backends/c/parser.c) on the same tables and input. Unlike the reference,
+ * errors (CUDA failure, allocation failure, a device wait that timed out, an
+ * input beyond capacity) are reported as negative status codes and never as
+ * a reject.
+ */
+#ifndef ALPACC_B200_H
+#define ALPACC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ALPACC_ABI_VERSION 1
+
+/* Status codes. */
+#define ALPACC_OK 0          /* input accepted, result filled */
+#define ALPACC_REJECT 1      /* input rejected (the reference writes byte 0) */
+#define ALPACC_E_INVALID (-1)  /* bad argument or malformed tables */
+#define ALPACC_E_CUDA (-2)     /* a CUDA call failed */
+#define ALPACC_E_NOMEM (-3)    /* device or pinned allocation failed */
+#define ALPACC_E_CAPACITY (-4) /* input larger than the configured capacity */
+#define ALPACC_E_TIMEOUT (-5)  /* a bounded device wait gave up */
+#define ALPACC_E_UNSUPPORTED (-6) /* tables exceed what the kernels handle */
+
+/*
+ * Grammar tables exactly as alpacc's C emitter produces them. Element widths
+ * are given in bytes; arrays use those native widths, little-endian.
+ */
+typedef struct alpacc_tables {
+  uint32_t abi_version;        /* ALPACC_ABI_VERSION */
+  uint32_t terminal_size;      /* sizeof(terminal_t)   */
+  uint32_t production_size;    /* sizeof(production_t) */
+  uint32_t bracket_size;       /* sizeof(bracket_t)    */
+  uint32_t state_size;         /* sizeof(state_t)      */
+  uint32_t index_size;         /* sizeof(index_t): 4 (--index32) or 8 */
+  uint32_t length_size;        /* sizeof(length_t)     */
+  uint32_t reserved0;
+  /* lexer: C/Lexer.hs:16-58 */
+  uint64_t num_states;         /* NUM_STATES (endomorphisms) */
+  uint64_t endo_mask, endo_offset;
+  uint64_t terminal_mask, terminal_offset;
+  uint64_t produce_mask, produce_offset;
+  uint64_t identity;           /* IDENTITY */
+  int64_t ignore_token;        /* IGNORE_TOKEN, or -1 when the grammar has none */
+  const void *to_state;        /* state_t[256]                      TO_STATE */
+  const void *compose;         /* state_t[num_states * num_states]  COMPOSE  */
+  const uint8_t *accept;       /* bool[num_states]                  ACCEPT   */
+  /* parser: C/Parser.hs:21-95 */
+  uint64_t q, k;               /* Q, K */
+  uint64_t empty_terminal, start_terminal, end_terminal;
+  uint64_t hash_table_size;    /* HASH_TABLE_SIZE */
+  uint64_t max_iters;          /* MAX_ITERS */
+  uint64_t stacks_size, productions_size;
+  uint64_t max_brackets_per_position, max_prods_per_position;
+  const void *stacks;          /* bracket_t[stacks_size]            STACKS */
+  const void *productions;     /* production_t[productions_size]    PRODUCTIONS */
+  const uint8_t *hash_table_is_valid;        /* bool[hash_table_size] */
+  const void *hash_table_keys;               /* terminal_t[hash_table_size][q + k] */
+  const int64_t *hash_table_stacks_span;     /* int64_t[hash_table_size][2] */
+  const int64_t *hash_table_productions_span;/* int64_t[hash_table_size][2] */
+  uint64_t number_of_productions;            /* NUMBER_OF_PRODUCTIONS */
+  const uint64_t *production_to_arity;       /* uint64_t[number_of_productions] */
+  const uint8_t *production_to_terminal_is_valid; /* bool[number_of_productions] */
+} alpacc_tables;
+
+/* Opaque handle: the grammar's device tables, a stream and resident scratch. */
+typedef struct alpacc_gpu_grammar alpacc_gpu_grammar;
+
+/*
+ * Result of one parse (SoA, native widths; matches the combined-mode record of
+ * docs/wire-protocols.md). Host results live in library-owned pinned memory
+ * released by alpacc_result_free; device results point into the grammar's
+ * resident scratch and stay valid until the next call on that handle.
+ */
+typedef struct alpacc_result {
+  uint8_t valid;               /* 1 accepted, 0 rejected */
+  uint8_t on_device;           /* 1 when the arrays are device pointers */
+  uint16_t reserved0;
+  uint32_t reserved1;
+  uint64_t num_tokens;
+  uint64_t num_nodes;
+  void *token_ids;             /* terminal_t[num_tokens] */
+  void *token_starts;          /* index_t[num_tokens]    */
+  void *token_lengths;         /* length_t[num_tokens]   */
+  void *node_productions;      /* production_t[num_nodes] (preorder) */
+  void *node_parents;          /* index_t[num_nodes]     */
+  void *token_parents;         /* index_t[num_tokens]    */
+  void *internal;              /* owned buffer, freed by alpacc_result_free */
+} alpacc_result;
+
+/*
+ * Upload the tables of one grammar to `device` once and derive the device
+ * forms (the minimised lexer automaton, the pair-lookup table). `max_input`
+ * bytes of scratch capacity are reserved up front (0 = grow on demand).
+ * Returns NULL and sets *err on failure.
+ */
+alpacc_gpu_grammar *alpacc_gpu_load(const alpacc_tables *tables, int device, uint64_t max_input, int *err);
+
+/* Release the handle, its device tables and its scratch. */
+void alpacc_gpu_free(alpacc_gpu_grammar *g);
+
+/*
+ * Parse host bytes: H2D copy, the device path, D2H copy of the result into
+ * pinned memory owned by *out. Returns ALPACC_OK, ALPACC_REJECT or an error.
+ */
+int alpacc_gpu_parse(alpacc_gpu_grammar *g, const uint8_t *in, uint64_t n, alpacc_result *out);
+
+/*
+ * Parse bytes already resident on the device (`d_in`, n bytes) on the
+ * handle's stream; the result arrays are device pointers into the handle's
+ * scratch (out->on_device = 1). Blocks until the status is known.
+ */
+int alpacc_gpu_parse_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, alpacc_result *out);
+
+/*
+ * Enqueue the device path for device-resident input without waiting; the
+ * status and counts are written to device memory and read back later with
+ * alpacc_gpu_collect. For timing loops and CUDA-graph capture.
+ */
+int alpacc_gpu_enqueue(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n);
+int alpacc_gpu_collect(alpacc_gpu_grammar *g, alpacc_result *out);
+
+/*
+ * Many independent inputs at once: `bytes` holds them back to back, input i is
+ * bytes[offsets[i] .. offsets[i+1]). `outs` receives `count` results.
+ * Returns ALPACC_OK when every input was processed (each outs[i].valid says
+ * accept/reject) or the first error.
+ */
+int alpacc_gpu_parse_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offsets, uint32_t count,
+                           alpacc_result *outs);
+
+/* Free the buffer behind a host result. */
+void alpacc_result_free(alpacc_result *r);
+
+/*
+ * Write the combined-mode response record for input `in` to `out`, byte for
+ * byte what the generated run_case writes: u8 valid, then (when valid) the
+ * token and tree sections. Returns the status of the parse.
+ */
+int alpacc_gpu_run_case(alpacc_gpu_grammar *g, uint64_t n, const uint8_t *in, FILE *out);
+
+/* `--layout` text ("terminal_t=1\nproduction_t=1\n..."); returns its length. */
+int alpacc_gpu_layout(const alpacc_gpu_grammar *g, char *buf, size_t len);
+
+/* Human-readable text of a status code. */
+const char *alpacc_strerror(int status);
+
+/*
+ * Device time of the last enqueued device path in milliseconds (CUDA events
+ * around the launches on the handle's stream), or a negative value.
+ */
+double alpacc_gpu_last_ms(alpacc_gpu_grammar *g);
+
+/*
+ * Diagnostics (no counterpart in the reference): sizes of the derived device
+ * tables (states and byte classes of the minimised lexer automaton, lanes,
+ * reachable endomorphisms, pair records) and the reject reason / wait site of
+ * the last call; and the text of the last internal error.
+ */
+int alpacc_gpu_info(const alpacc_gpu_grammar *g, int64_t *vals, int nvals);
+const char *alpacc_gpu_last_error(const alpacc_gpu_grammar *g);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ALPACC_B200_H */
