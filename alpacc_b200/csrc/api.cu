@@ -423,7 +423,7 @@ alpacc_gpu_grammar *alpacc_gpu_load(const alpacc_tables *tables, int device, uin
     return nullptr;
   }
   rc = upload_tables(g);
-  if (rc == ALPACC_OK && lex_smem_bytes(g) > 48 * 1024) {
+  if (rc == ALPACC_OK) {
     if (cudaFuncSetAttribute(lex_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lex_smem_bytes(g)) !=
         cudaSuccess) {
       cudaGetLastError();

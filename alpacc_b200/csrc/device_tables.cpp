@@ -285,6 +285,11 @@ int build_host_grammar(const alpacc_tables *t, HostGrammar *out, std::string *wh
   out->len_max = t->length_size >= 8 ? ~0ull : ((1ull << (8 * t->length_size)) - 1);
   int rc = build_lexer(t, out->ignore, &out->lex, why);
   if (rc != ALPACC_OK) return rc;
+  for (uint8_t tm : out->lex.term)
+    if ((uint64_t)tm > t->end_terminal) {
+      *why = "a lexer terminal id is not a parser terminal";
+      return ALPACC_E_INVALID;
+    }
   return build_pairs(t, &out->pairs, why);
 }
 

@@ -364,18 +364,23 @@ __global__ void pse_resolve_kernel(PseArgs a) {
 
 __global__ void compact_kernel(CompactArgs a) {
   const unsigned long long P = *a.count;
+  const long long T = (long long)*a.num_tokens;
   for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; e < P;
        e += (unsigned long long)gridDim.x * blockDim.x) {
     const uint32_t prod = a.prods[e];
-    const long long p = e == 0 ? 0 : a.parent[e];
+    long long p = e == 0 ? 0 : a.parent[e];
+    if (p < 0 || (unsigned long long)p >= P) p = 0;  // only after a recorded reject or error
     const long long p_new = p - (long long)a.tinc[p];
     const long long ti = a.tinc[e];
     if (__ldg(a.is_term + prod)) {
-      store_uint(a.token_parents, (unsigned long long)(ti - 1), a.idx_w, (unsigned long long)p_new);
+      if (ti >= 1 && ti <= T)
+        store_uint(a.token_parents, (unsigned long long)(ti - 1), a.idx_w, (unsigned long long)p_new);
     } else {
-      const unsigned long long o = e - (unsigned long long)ti;
-      store_uint(a.node_prods, o, a.prod_w, prod);
-      store_uint(a.node_parents, o, a.idx_w, (unsigned long long)p_new);
+      const long long o = (long long)e - ti;
+      if (o >= 0) {
+        store_uint(a.node_prods, (unsigned long long)o, a.prod_w, prod);
+        store_uint(a.node_parents, (unsigned long long)o, a.idx_w, (unsigned long long)p_new);
+      }
     }
   }
 }
