@@ -66,10 +66,16 @@ struct alpacc_gpu_grammar {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = -1.0;
+  // per-kernel timing: event pairs around each launch of the last call
+  static constexpr int kStages = 8;
+  cudaEvent_t sev[2 * kStages] = {};
+  bool stage_used[kStages] = {};
+  double stage_ms[kStages] = {};
   // tables
   DevBuf cls_words, trans_words, lane_of, img, img_cnt, sterm, sflags;
   DevBuf dense, rec_ss, rec_ps, rec_nb, rec_np, stacks, prods, arity, is_term;
   int trans_word_count = 0, trans_rep = 32;
+  int diag = 0;
   // status
   DeviceStatus *d_status = nullptr;
   DeviceStatus *h_status = nullptr;  // pinned
@@ -80,6 +86,9 @@ struct alpacc_gpu_grammar {
   DevBuf pair_ticket, pst_flags, pst_agg, pst_inc, br, pr;
   DevBuf pse_ticket, pse_flags, pse_agg, pse_inc, h, answer, tinc, tile_min, chunk_min, queue, queue_len;
   DevBuf node_prods, node_parents, token_parents;
+  // pinned host result buffers kept for reuse (released results come back here)
+  void *pinned_cache = nullptr;
+  size_t pinned_cache_size = 0;
   // last result (device)
   uint64_t last_T = 0, last_N = 0;
   int last_status = ALPACC_E_INVALID;
@@ -140,6 +149,20 @@ int sync_status(alpacc_gpu_grammar *g) {
   return ALPACC_OK;
 }
 
+void stage_begin(alpacc_gpu_grammar *g, int k) {
+  cudaEventRecord(g->sev[2 * k], g->stream);
+  g->stage_used[k] = true;
+}
+void stage_end(alpacc_gpu_grammar *g, int k) { cudaEventRecord(g->sev[2 * k + 1], g->stream); }
+void collect_stages(alpacc_gpu_grammar *g) {
+  for (int k = 0; k < alpacc_gpu_grammar::kStages; k++) {
+    float ms = 0;
+    g->stage_ms[k] = (g->stage_used[k] && cudaEventElapsedTime(&ms, g->sev[2 * k], g->sev[2 * k + 1]) == cudaSuccess)
+                         ? ms
+                         : 0.0;
+  }
+}
+
 size_t lex_smem_bytes(const alpacc_gpu_grammar *g) { return (size_t)g->trans_word_count * g->trans_rep * 4; }
 
 // The whole device path for d_in[0..n). Leaves counts in g->last_T / last_N.
@@ -152,6 +175,7 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
   const int prod_w = (int)tb.production_size;
   if (n > (1ull << 31) - 1) return ALPACC_E_CAPACITY;
   CK(cudaMemsetAsync(g->d_status, 0, sizeof(DeviceStatus), g->stream));
+  for (int k = 0; k < alpacc_gpu_grammar::kStages; k++) g->stage_used[k] = false;
   CK(cudaEventRecord(g->ev0, g->stream));
 
   // ---------------- lexer ----------------
@@ -203,7 +227,10 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     a.st2 = PairTileState{(unsigned *)g->st2_flags.p, (unsigned long long *)g->st2_agg.p,
                           (unsigned long long *)g->st2_inc.p};
     a.status = g->d_status;
+    a.diag = g->diag;
+    stage_begin(g, 0);
     lex_kernel<<<(unsigned)tiles, kLexThreads, lex_smem_bytes(g), g->stream>>>(a);
+    stage_end(g, 0);
     CK(cudaGetLastError());
     int rc = sync_status(g);
     if (rc) return rc;
@@ -253,7 +280,9 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     a.st = PairTileState{(unsigned *)g->pst_flags.p, (unsigned long long *)g->pst_agg.p,
                          (unsigned long long *)g->pst_inc.p};
     a.status = g->d_status;
+    stage_begin(g, 1);
     pair_kernel<<<(unsigned)tiles, kPairThreads, 0, g->stream>>>(a);
+    stage_end(g, 1);
     CK(cudaGetLastError());
     int rc = sync_status(g);
     if (rc) return rc;
@@ -302,9 +331,13 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     a.st = PairTileState{(unsigned *)g->pse_flags.p, (unsigned long long *)g->pse_agg.p,
                          (unsigned long long *)g->pse_inc.p};
     a.status = g->d_status;
+    stage_begin(g, 2 + 2 * mode);
     pse_tile_kernel<<<(unsigned)tiles, kPseThreads, 0, g->stream>>>(a);
+    stage_end(g, 2 + 2 * mode);
     CK(cudaGetLastError());
+    stage_begin(g, 3 + 2 * mode);
     pse_resolve_kernel<<<148 * 4, 256, 0, g->stream>>>(a);
+    stage_end(g, 3 + 2 * mode);
     CK(cudaGetLastError());
   }
   if (P == 0) CK(cudaMemsetAsync(&g->d_status->num_nodes, 0, 8, g->stream));
@@ -327,7 +360,9 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     a.prod_w = prod_w;
     a.idx_w = idx_w;
     a.status = g->d_status;
+    stage_begin(g, 6);
     compact_kernel<<<148 * 8, 256, 0, g->stream>>>(a);
+    stage_end(g, 6);
     CK(cudaGetLastError());
   }
   CK(cudaEventRecord(g->ev1, g->stream));
@@ -335,6 +370,7 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
   if (rc) return rc;
   float ms = 0;
   if (cudaEventElapsedTime(&ms, g->ev0, g->ev1) == cudaSuccess) g->last_ms = ms;
+  collect_stages(g);
   if (g->h_status->reject) return ALPACC_REJECT;
   if (P == 0 && T != 0) return ALPACC_REJECT;  // compact_tree: terminal count mismatch
   g->last_T = T;
@@ -357,22 +393,40 @@ void fill_device_result(alpacc_gpu_grammar *g, alpacc_result *out, int status) {
   out->token_parents = g->token_parents.p;
 }
 
-// Copy a device result to one pinned host allocation.
+// Header of a pinned host result block; the arrays follow it.
+struct PinnedBlock {
+  alpacc_gpu_grammar *owner;
+  size_t size;
+  size_t pad[6];
+};
+
+// Copy a device result to one pinned host block (reused across calls once the
+// caller frees the previous result).
 int copy_result_to_host(alpacc_gpu_grammar *g, alpacc_result *out) {
   const alpacc_tables &tb = g->hg.t;
   const uint64_t T = g->last_T, N = g->last_N;
   const size_t sz[6] = {T * tb.terminal_size, T * tb.index_size, T * tb.length_size,
                         N * tb.production_size, N * tb.index_size, T * tb.index_size};
-  size_t off[6], total = 0;
+  size_t off[6], total = sizeof(PinnedBlock);
   for (int i = 0; i < 6; i++) {
     off[i] = total;
     total += (sz[i] + 15) & ~(size_t)15;
   }
   void *host = nullptr;
-  if (cudaMallocHost(&host, std::max<size_t>(total, 16)) != cudaSuccess) {
-    cudaGetLastError();
-    return ALPACC_E_NOMEM;
+  if (g->pinned_cache && g->pinned_cache_size >= total) {
+    host = g->pinned_cache;
+    g->pinned_cache = nullptr;
+  } else {
+    if (g->pinned_cache) cudaFreeHost(g->pinned_cache);
+    g->pinned_cache = nullptr;
+    size_t want = total + total / 8;
+    if (cudaMallocHost(&host, want) != cudaSuccess) {
+      cudaGetLastError();
+      return ALPACC_E_NOMEM;
+    }
+    reinterpret_cast<PinnedBlock *>(host)->size = want;
   }
+  reinterpret_cast<PinnedBlock *>(host)->owner = g;
   const void *src[6] = {g->tok_ids.p, g->tok_starts.p, g->tok_lens.p, g->node_prods.p, g->node_parents.p,
                         g->token_parents.p};
   for (int i = 0; i < 6; i++)
@@ -415,6 +469,11 @@ alpacc_gpu_grammar *alpacc_gpu_load(const alpacc_tables *tables, int device, uin
   g->device = device;
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&g->ev0) != cudaSuccess || cudaEventCreate(&g->ev1) != cudaSuccess ||
+      [&] {
+        for (auto &e : g->sev)
+          if (cudaEventCreate(&e) != cudaSuccess) return true;
+        return false;
+      }() ||
       cudaMalloc(&g->d_status, sizeof(DeviceStatus)) != cudaSuccess ||
       cudaMallocHost(&g->h_status, sizeof(DeviceStatus)) != cudaSuccess) {
     cudaGetLastError();
@@ -422,6 +481,7 @@ alpacc_gpu_grammar *alpacc_gpu_load(const alpacc_tables *tables, int device, uin
     alpacc_gpu_free(g);
     return nullptr;
   }
+  std::memset(g->h_status, 0, sizeof(DeviceStatus));
   rc = upload_tables(g);
   if (rc == ALPACC_OK) {
     if (cudaFuncSetAttribute(lex_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lex_smem_bytes(g)) !=
@@ -453,10 +513,13 @@ void alpacc_gpu_free(alpacc_gpu_grammar *g) {
                     &g->chunk_min, &g->queue, &g->queue_len, &g->node_prods, &g->node_parents,
                     &g->token_parents};
   for (DevBuf *b : bufs) release(*b);
+  if (g->pinned_cache) cudaFreeHost(g->pinned_cache);
   if (g->d_status) cudaFree(g->d_status);
   if (g->h_status) cudaFreeHost(g->h_status);
   if (g->ev0) cudaEventDestroy(g->ev0);
   if (g->ev1) cudaEventDestroy(g->ev1);
+  for (auto &e : g->sev)
+    if (e) cudaEventDestroy(e);
   if (g->stream) cudaStreamDestroy(g->stream);
   delete g;
 }
@@ -513,7 +576,16 @@ int alpacc_gpu_parse_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const in
 
 void alpacc_result_free(alpacc_result *r) {
   if (!r) return;
-  if (r->internal) cudaFreeHost(r->internal);
+  if (r->internal) {
+    PinnedBlock *b = reinterpret_cast<PinnedBlock *>(r->internal);
+    alpacc_gpu_grammar *g = b->owner;
+    if (g && !g->pinned_cache) {
+      g->pinned_cache = b;
+      g->pinned_cache_size = b->size;
+    } else {
+      cudaFreeHost(b);
+    }
+  }
   std::memset(r, 0, sizeof(*r));
 }
 
@@ -563,6 +635,8 @@ const char *alpacc_strerror(int status) {
 
 double alpacc_gpu_last_ms(alpacc_gpu_grammar *g) { return g ? g->last_ms : -1.0; }
 
+void *alpacc_gpu_stream(alpacc_gpu_grammar *g) { return g ? (void *)g->stream : nullptr; }
+
 // Diagnostics for tests: derived machine sizes and the last error text.
 int alpacc_gpu_info(const alpacc_gpu_grammar *g, int64_t *vals, int nvals) {
   if (!g || !vals) return ALPACC_E_INVALID;
@@ -577,5 +651,25 @@ int alpacc_gpu_info(const alpacc_gpu_grammar *g, int64_t *vals, int nvals) {
 }
 
 const char *alpacc_gpu_last_error(const alpacc_gpu_grammar *g) { return g ? g->last_error.c_str() : ""; }
+
+int alpacc_gpu_counts(const alpacc_gpu_grammar *g, int64_t *vals, int n) {
+  if (!g || !vals || !g->h_status) return ALPACC_E_INVALID;
+  const int64_t v[8] = {(int64_t)g->h_status->num_tokens, (int64_t)g->h_status->num_brackets,
+                        (int64_t)g->h_status->num_productions, (int64_t)g->h_status->num_nodes,
+                        (int64_t)g->h_status->scratch[0], (int64_t)g->h_status->scratch[1],
+                        (int64_t)g->h_status->scratch[2], (int64_t)g->h_status->scratch[3]};
+  for (int i = 0; i < n && i < 8; i++) vals[i] = v[i];
+  return 8;
+}
+
+void alpacc_gpu_set_diagnostics(alpacc_gpu_grammar *g, int on) {
+  if (g) g->diag = on;
+}
+
+int alpacc_gpu_stage_ms(const alpacc_gpu_grammar *g, double *out, int n) {
+  if (!g || !out) return ALPACC_E_INVALID;
+  for (int k = 0; k < n && k < alpacc_gpu_grammar::kStages; k++) out[k] = g->stage_ms[k];
+  return alpacc_gpu_grammar::kStages;
+}
 
 }  // extern "C"

@@ -40,6 +40,7 @@ struct LexArgs {
   uint8_t *st1_vec;     // [tiles * M]
   PairTileState st2;    // (kept-token count, last boundary position)
   DeviceStatus *status;
+  int diag;             // 1: accumulate diagnostic counters in status->scratch
 };
 
 __global__ void lex_kernel(LexArgs args);

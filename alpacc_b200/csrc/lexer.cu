@@ -147,6 +147,7 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
   {
     uint32_t active = 0;
     int c0 = 0;
+    int multi_bytes = 0;
     if (nb > 0) {
       c0 = cls_of(c, chunk_byte(sm, t, 0));
       const int cnt = __ldg(a->img_cnt + c0);
@@ -178,6 +179,7 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
           }
         }
         ++j;
+        ++multi_bytes;
       }
       // one lane: the hot loop, one lookup per byte
       if (active && __popc(active) == 1 && j < nb) {
@@ -193,6 +195,10 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
     }
     sm->active[t] = (uint16_t)active;
     sm->c0[t] = (uint8_t)c0;
+    if (a->diag) {
+      const unsigned w = __reduce_add_sync(0xffffffffu, (unsigned)multi_bytes);
+      if ((t & 31) == 0) atomicAdd(&st->scratch[3], (unsigned long long)w);
+    }
   }
   __syncthreads();
 
@@ -202,6 +208,16 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
   long long kex = block_exclusive_scan<long long>(is_const ? (long long)t : -1ll, MaxI64(), -1ll, sm->scan_tmp, &ktot);
   sm->kconst[t] = (int)kex;
   if (t == 0) sm->out_published = 0;
+  if (a->diag) {
+    const int nconst = __syncthreads_count(is_const);
+    if (t == 0) {
+      atomicAdd(&st->scratch[1], (unsigned long long)nconst);
+      if (ktot < 0) atomicAdd(&st->scratch[0], 1ull);
+    }
+    const unsigned chain = (unsigned)(kex >= 0 ? t - 1 - kex : t);
+    const unsigned w = __reduce_add_sync(0xffffffffu, chain);
+    if ((t & 31) == 0) atomicAdd(&st->scratch[2], (unsigned long long)w);
+  }
   __syncthreads();
 
   // value of a constant chunk (its single live lane, or dead)

@@ -99,6 +99,13 @@ def lib():
         L.alpacc_gpu_last_ms.argtypes = [ctypes.c_void_p]
         L.alpacc_gpu_info.restype = ctypes.c_int
         L.alpacc_gpu_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
+        L.alpacc_gpu_stage_ms.restype = ctypes.c_int
+        L.alpacc_gpu_stage_ms.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+        L.alpacc_gpu_counts.restype = ctypes.c_int
+        L.alpacc_gpu_counts.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
+        L.alpacc_gpu_set_diagnostics.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.alpacc_gpu_stream.restype = ctypes.c_void_p
+        L.alpacc_gpu_stream.argtypes = [ctypes.c_void_p]
         L.alpacc_gpu_last_error.restype = ctypes.c_char_p
         L.alpacc_gpu_last_error.argtypes = [ctypes.c_void_p]
         _lib = L
@@ -245,8 +252,40 @@ class Parser:
         """The response record bytes ``run_case`` would write."""
         return wire.encode_record(self.parse(data), self.layout)
 
+    def counts(self) -> dict:
+        """Tokens, brackets, productions, nodes of the last call."""
+        vals = (ctypes.c_int64 * 8)()
+        lib().alpacc_gpu_counts(self._h, vals, 8)
+        return {"T": vals[0], "B": vals[1], "P": vals[2], "N": vals[3], "vector_tiles": vals[4],
+                "const_chunks": vals[5], "chain_evals": vals[6], "multi_lane_bytes": vals[7]}
+
+    def set_diagnostics(self, on: bool):
+        lib().alpacc_gpu_set_diagnostics(self._h, 1 if on else 0)
+
+    def stream_handle(self) -> int:
+        """The cudaStream_t the handle launches on."""
+        return lib().alpacc_gpu_stream(self._h)
+
+    def parse_raw(self, host_ptr: int, n: int):
+        """Host pointer in (ideally pinned), host result out; returns (status,
+        Result); release it with ``free_result``."""
+        r = Result()
+        rc = self._check(lib().alpacc_gpu_parse(self._h, host_ptr, n, ctypes.byref(r)))
+        return rc, r
+
+    @staticmethod
+    def free_result(r: Result):
+        lib().alpacc_result_free(ctypes.byref(r))
+
     def last_ms(self) -> float:
         return lib().alpacc_gpu_last_ms(self._h)
+
+    STAGES = ("lex", "pairs", "bracket_walk", "bracket_resolve", "parent_walk", "parent_resolve", "compact")
+
+    def stage_ms(self) -> dict:
+        vals = (ctypes.c_double * 8)()
+        lib().alpacc_gpu_stage_ms(self._h, vals, 8)
+        return {k: vals[i] for i, k in enumerate(self.STAGES)}
 
 
 _cudart = None

@@ -1,0 +1,357 @@
+#!/usr/bin/env python
+"""Throughput of the lex + LLP-parse path on B200.
+
+Workload (default): one 256 MiB JSON document (grammar ``grammars/json_ext.alp``:
+the reference JSON productions with full JSON lexical rules, lookback 1,
+lookahead 3, 16-bit token lengths, 32-bit indices), seeded synthetic data.
+
+A step is one pass of the whole path over the document: lexing, pair
+expansion, bracket matching, parents, compaction. ``value`` is input GB/s with
+the input resident in device memory (CUDA events on the library's stream
+around K steps, max over ranks); ``e2e`` is the same through the public host
+API: pinned host input -> device -> host result arrays, every step.
+
+``--impl reference`` times the reference's own C backend (oracle/_ref, built
+from alpacc's backends/c sources) on the host cores instead: one independent
+document per core.
+
+Multi-GPU: replicas only (each rank parses its own document; no collective on
+the data path); ``scaling`` is "weak".
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "input GB/s lex+parse at 1 B200 (% HBM peak); serve p99 ms vs per-input launch"
+GRAMMAR = os.path.join(REPO, "grammars", "json_ext.alp")
+REF_CONFIG = "json_ext_i32"
+
+
+def peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join("/tmp", "alpacc_clocks_%d_%d.csv" % (os.getpid(), device))
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        os.remove(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(n, T, N, lay):
+    """bytes(n) of the whole path: input once plus the compulsory outputs."""
+    return n + T * (lay.terminal + lay.index + lay.length) + N * (lay.production + lay.index) + T * lay.index
+
+
+def kernel_bytes(stage, n, T, B, P, N, lay):
+    """Algorithmic bytes of one launch of each kernel (its compulsory inputs and
+    outputs; the intermediate arrays count where they are the kernel's contract)."""
+    if stage == "lex":
+        return n + T * (lay.terminal + lay.index + lay.length)
+    if stage == "pairs":
+        return T * lay.terminal + 4 * (B + P)
+    if stage == "bracket_walk":
+        return 4 * B + 4 * B
+    if stage == "parent_walk":
+        return 4 * P + 4 * P + 4 * P + 4 * P
+    if stage == "compact":
+        return 4 * P * 3 + N * (lay.production + lay.index) + T * lay.index
+    return 0
+
+
+def cpu_baseline_sample(n_sample: int, seed: int):
+    """The reference C backend, single thread, on one bounded document."""
+    from alpacc_b200 import workloads as W
+    from oracle.ref import RefOracle, available
+    import numpy as np
+
+    if not available(REF_CONFIG):
+        return None
+    doc = np.frombuffer(W.json_doc(n_sample, seed), dtype=np.uint8)
+    ref = RefOracle(REF_CONFIG)
+    ref.pipeline(doc[: 1 << 20])  # warm
+    times = []
+    ok = None
+    for _ in range(3):
+        t0 = time.perf_counter()
+        ok = ref.pipeline(doc)
+        times.append(time.perf_counter() - t0)
+    t = min(times)
+    return {"value": n_sample / t / 1e9, "unit": "GB/s", "cores": 1, "kind": "reference",
+            "sample": "one %d MiB document of the same generator (seed %d), lex_string -> parse_test -> "
+                      "compute_parents -> compact_tree in memory, best of 3 (%.2fs), accepted=%s"
+                      % (n_sample >> 20, seed, t, ok[0])}
+
+
+def reference_arm(a, rank, world):
+    if rank != 0:
+        return
+    import multiprocessing as mp
+
+    from oracle.ref import available
+
+    if not available(REF_CONFIG):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/lib%s.so is not built" % REF_CONFIG}))
+        return
+    cores = os.cpu_count() or 1
+    sample = a.ref_sample
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores, initializer=_pool_init, initargs=(sample,)) as pool:
+        pool.map(_pool_step, range(cores))  # load
+        for _ in range(a.warmup):
+            pool.map(_pool_step, range(cores))
+        t0 = time.perf_counter()
+        oks = []
+        for _ in range(a.steps):
+            oks.extend(pool.map(_pool_step, range(cores)))
+        t = time.perf_counter() - t0
+    value = a.steps * cores * sample / t / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": 0, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": t / a.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "json_ext %d MiB documents, one per host core" % (sample >> 20),
+                   "grammar": "json_ext.alp", "index": "i32"},
+        "cpu_baseline": {"value": value, "unit": "GB/s", "cores": cores, "kind": "reference",
+                         "sample": "%d independent %d MiB JSON documents per step (one per core), reference C "
+                                   "backend in memory; all accepted=%s" % (cores, sample >> 20, all(oks))},
+        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+_POOL = {}
+
+
+def _pool_init(sample):
+    from alpacc_b200 import workloads as W
+    from oracle.ref import RefOracle
+    import numpy as np
+
+    pid = os.getpid()
+    _POOL["doc"] = np.frombuffer(W.json_doc(sample, 2 + (pid % 97)), dtype=np.uint8)
+    _POOL["ref"] = RefOracle(REF_CONFIG)
+
+
+def _pool_step(_):
+    return _POOL["ref"].pipeline(_POOL["doc"])[0]
+
+
+def ours(a, rank, world, local_rank, dist):
+    import numpy as np
+    import torch
+
+    from alpacc_b200 import wire, workloads as W
+    from alpacc_b200.grammar.cache import load_tables
+    from alpacc_b200.native import Parser
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    n = a.size
+    tables = load_tables(GRAMMAR, index32=True)
+    lay = wire.Layout.of(tables)
+    host = W.json_doc(n, 2 + rank)
+    parser = Parser(tables, device=local_rank, max_input=n)
+    d_in = torch.frombuffer(bytearray(host), dtype=torch.uint8).to(dev)
+    ext = torch.cuda.ExternalStream(parser.stream_handle(), device=dev)
+    stages = {k: [] for k in Parser.STAGES}
+
+    def step():
+        rc, r = parser.parse_device(d_in.data_ptr(), n)
+        return rc, r
+
+    for _ in range(a.warmup):
+        rc, r = step()
+    if rc != 0:
+        raise SystemExit("warm-up parse did not accept the document (status %d)" % rc)
+    T, N = r.num_tokens, r.num_nodes
+    info = parser.info()
+    # ---- device-resident timing ----
+    clocks = ClockSampler(local_rank)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    for _ in range(a.steps):
+        rc, r = step()
+        for k, v in parser.stage_ms().items():
+            stages[k].append(v)
+    e1.record(ext)
+    torch.cuda.synchronize()
+    ms_total = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    if dist:
+        t = torch.tensor([ms_total], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / a.steps
+    value = world * n * a.steps / (ms_total / 1e3) / 1e9
+
+    # ---- end to end: pinned host input, host results ----
+    pin = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+    pin.numpy()[:] = np.frombuffer(host, dtype=np.uint8)
+    for _ in range(max(1, a.warmup)):
+        rc2, r2 = parser.parse_raw(pin.data_ptr(), n)
+        Parser.free_result(r2)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(ext)
+    for _ in range(a.steps):
+        rc2, r2 = parser.parse_raw(pin.data_ptr(), n)
+        Parser.free_result(r2)
+    f1.record(ext)
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    if dist:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = world * n * a.steps / (e2e_ms / 1e3) / 1e9
+    d2h = T * (lay.terminal + lay.index + lay.length) + N * (lay.production + lay.index) + T * lay.index
+
+    if rank != 0:
+        return
+    peak, peak_kind = peaks()
+    mean = {k: (sum(v) / len(v) if v else 0.0) for k, v in stages.items()}
+    dom = max(mean, key=lambda k: mean[k])
+    st = parser.counts()
+    B, P = st.get("B", 0), st.get("P", 0)
+    kb = kernel_bytes(dom, n, T, B, P, N, lay)
+    achieved = kb / (mean[dom] / 1e3) / 1e9 if mean[dom] > 0 else 0.0
+    path_bytes = algorithmic_bytes(n, T, N, lay)
+    traffic = committed_traffic(dom)
+    line = {
+        "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded JSON generator, one document per rank)",
+        "config": {"workload": "json_ext %d MiB single document (BASELINE config 2 shape)" % (n >> 20),
+                   "grammar": "json_ext.alp", "bytes": n, "index": "i32", "tokens": T, "nodes": N,
+                   "brackets": B, "productions": P, "parallelism": "replicas x%d" % world,
+                   "l2": "input larger than L2 (no flush)"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                     "algorithmic_bytes": kb, "ms": mean[dom]},
+        "path_roofline": {"algorithmic_bytes": path_bytes, "achieved": path_bytes / (ms_step / 1e3) / 1e9,
+                          "frac": path_bytes / (ms_step / 1e3) / 1e9 / peak},
+        "stage_ms": mean,
+        "e2e": {"value": e2e, "unit": "GB/s", "h2d_bytes_per_step": n, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_ms / a.steps},
+        "gpu_launches": 7 * a.steps,
+        "clocks": clk,
+        "machine": info,
+    }
+    if not a.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(a.cpu_sample, 2)
+    print(json.dumps(line))
+
+
+def committed_traffic(kernel: str):
+    """DRAM bytes per launch from the committed ncu summary, if one exists."""
+    p = os.path.join(REPO, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    v = d.get(kernel)
+    return v.get("bytes_per_launch_full_size") if isinstance(v, dict) else None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=256 << 20)
+    ap.add_argument("--cpu-sample", type=int, default=64 << 20)
+    ap.add_argument("--ref-sample", type=int, default=16 << 20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        if a.impl == "ours":
+            torch.cuda.set_device(local_rank)
+            tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            dist = tdist
+    if a.impl == "reference":
+        reference_arm(a, rank, world)
+    else:
+        ours(a, rank, world, local_rank, dist)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

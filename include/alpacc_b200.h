@@ -156,7 +156,8 @@ int alpacc_gpu_collect(alpacc_gpu_grammar *g, alpacc_result *out);
 int alpacc_gpu_parse_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offsets, uint32_t count,
                            alpacc_result *outs);
 
-/* Free the buffer behind a host result. */
+/* Release a host result. Its pinned block returns to the handle for reuse, so
+   results must be released before the handle that produced them. */
 void alpacc_result_free(alpacc_result *r);
 
 /*
@@ -178,6 +179,10 @@ const char *alpacc_strerror(int status);
  */
 double alpacc_gpu_last_ms(alpacc_gpu_grammar *g);
 
+/* The cudaStream_t the handle launches on, so a caller can order its own work
+   (copies, events) with it. */
+void *alpacc_gpu_stream(alpacc_gpu_grammar *g);
+
 /*
  * Diagnostics (no counterpart in the reference): sizes of the derived device
  * tables (states and byte classes of the minimised lexer automaton, lanes,
@@ -186,6 +191,14 @@ double alpacc_gpu_last_ms(alpacc_gpu_grammar *g);
  */
 int alpacc_gpu_info(const alpacc_gpu_grammar *g, int64_t *vals, int nvals);
 const char *alpacc_gpu_last_error(const alpacc_gpu_grammar *g);
+/* Device time of each kernel of the last call (ms): lexer, pair expansion,
+   bracket walk, bracket resolve, parent walk, parent resolve, compaction. */
+int alpacc_gpu_stage_ms(const alpacc_gpu_grammar *g, double *out, int n);
+/* Tokens, brackets, productions and tree nodes of the last call, then four
+   lexer diagnostic counters (collected when diagnostics are on): tiles without
+   a constant chunk, constant chunks, chain evaluations, multi-lane bytes. */
+int alpacc_gpu_counts(const alpacc_gpu_grammar *g, int64_t *vals, int n);
+void alpacc_gpu_set_diagnostics(alpacc_gpu_grammar *g, int on);
 
 #ifdef __cplusplus
 }
