@@ -193,7 +193,7 @@ def arithmetic(n: int, seed: int = 1) -> bytes:
         pool.append("".join(parts).encode())
     # join sub-expressions with "+" so the whole input is one expression
     body = _pool_concat(pool, rng, n, b" + ")
-    if len(body) > n:
+    if len(body) > n or not body:
         body = b"0"
     return body + b" " * (n - len(body))
 

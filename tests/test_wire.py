@@ -1,0 +1,40 @@
+"""Wire protocol (docs/wire-protocols.md): record and batch round trips."""
+
+import json
+import os
+
+import numpy as np
+
+from alpacc_b200 import wire
+from tests import cases
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def test_record_round_trip_golden():
+    records = json.load(open(os.path.join(HERE, "golden", "records.json")))
+    for config, items in records.items():
+        lay = wire.Layout.of(cases.tables(config))
+        for it in items:
+            rec = bytes.fromhex(it["record"])
+            r, end = wire.decode_record(rec, lay)
+            assert end == len(rec)
+            assert wire.encode_record(r, lay) == rec
+
+
+def test_batch_framing():
+    payloads = [b"", b"1+2", b"x" * 300]
+    buf = wire.encode_batch(payloads)
+    assert int.from_bytes(buf[:8], "little") == 3
+    assert int.from_bytes(buf[8:16], "little") == 8
+    lay = wire.Layout(1, 1, 8, 8)
+    recs = [wire.ParseResult(False), wire.ParseResult(True, np.array([1]), np.array([0]), np.array([3]),
+                                                     np.array([2]), np.array([0]), np.array([0]))]
+    out = (2).to_bytes(8, "little") + b"".join(wire.encode_record(r, lay) for r in recs)
+    dec, end = wire.decode_batch(out, lay)
+    assert end == len(out) and not dec[0].valid and dec[1].equal(recs[1])
+
+
+def test_layout_text():
+    lay = wire.Layout.of(cases.tables("json_ext_i32"))
+    assert lay.text() == "terminal_t=1\nproduction_t=1\nindex_t=4\nlength_t=2\n"
