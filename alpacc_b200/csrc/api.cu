@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -72,9 +73,10 @@ struct alpacc_gpu_grammar {
   bool stage_used[kStages] = {};
   double stage_ms[kStages] = {};
   // tables
-  DevBuf cls_words, trans_words, lane_of, img, img_cnt, sterm, sflags;
+  DevBuf cls_id, trans_words, lane_of, img, img_cnt, sterm, sflags;
   DevBuf dense, rec_ss, rec_ps, rec_nb, rec_np, stacks, prods, arity, is_term;
   int trans_word_count = 0, trans_rep = 32;
+  int lex_grid = 0;
   int diag = 0;
   // status
   DeviceStatus *d_status = nullptr;
@@ -84,7 +86,7 @@ struct alpacc_gpu_grammar {
   DevBuf lex_ticket, st1_flag, st1_state, st1_vec, st2_flags, st2_agg, st2_inc;
   DevBuf tok_ids, tok_starts, tok_lens;
   DevBuf pair_ticket, pst_flags, pst_agg, pst_inc, br, pr;
-  DevBuf pse_ticket, pse_flags, pse_agg, pse_inc, h, answer, tinc, tile_min, chunk_min, queue, queue_len;
+  DevBuf pse_ticket, pse_flags, pse_agg, pse_inc, h, answer, tinc, tile_min, chunk_min, super_min, queue, queue_len;
   DevBuf node_prods, node_parents, token_parents;
   // pinned host result buffers kept for reuse (released results come back here)
   void *pinned_cache = nullptr;
@@ -114,15 +116,28 @@ namespace {
 
 int upload_tables(alpacc_gpu_grammar *g) {
   const LexerMachine &lm = g->hg.lex;
-  std::vector<uint32_t> clsw(64, 0);
-  for (int b = 0; b < 256; b++) clsw[b >> 2] |= (uint32_t)lm.cls[b] << ((b & 3) * 8);
+  if (lm.M > 128) return ALPACC_E_UNSUPPORTED;  // 7-bit states in the transition entries
+  // transition entries at class * M + state: next state | produce(next) << 7
   const size_t mc = (size_t)lm.M * lm.C;
   std::vector<uint32_t> trw((mc + 3) / 4, 0);
-  for (size_t i = 0; i < mc; i++) trw[i >> 2] |= (uint32_t)lm.trans[i] << ((i & 3) * 8);
+  for (int c = 0; c < lm.C; c++)
+    for (int m = 0; m < lm.M; m++) {
+      const size_t i = (size_t)c * lm.M + m;
+      const uint32_t nx = lm.trans[(size_t)m * lm.C + c];
+      const uint32_t e = nx | ((lm.flags[nx] & 1u) << 7);
+      trw[i >> 2] |= e << ((i & 3) * 8);
+    }
   g->trans_word_count = (int)trw.size();
-  // one copy per bank when it fits comfortably in shared memory
-  g->trans_rep = (trw.size() * 32 * 4 <= 96 * 1024) ? 32 : 1;
-  TRY(upload(g->cls_words, clsw));
+  // copies of the byte-class and transition tables in shared memory: as many
+  // as keep a CTA's tables within ~40 KB, at most one per bank
+  int copies = 32;
+  while (copies > 1 && (size_t)copies * (trw.size() * 4 + 512) > 40 * 1024) copies >>= 1;
+  if (const char *e = getenv("ALPACC_LEX_COPIES")) {
+    int v = atoi(e);
+    if (v >= 1 && v <= 32 && (v & (v - 1)) == 0) copies = v;
+  }
+  g->trans_rep = copies;
+  TRY(upload(g->cls_id, lm.cls));
   TRY(upload(g->trans_words, trw));
   TRY(upload(g->lane_of, lm.lane_of));
   TRY(upload(g->img, lm.img));
@@ -163,7 +178,23 @@ void collect_stages(alpacc_gpu_grammar *g) {
   }
 }
 
-size_t lex_smem_bytes(const alpacc_gpu_grammar *g) { return (size_t)g->trans_word_count * g->trans_rep * 4; }
+size_t lex_smem_bytes(const alpacc_gpu_grammar *g) {
+  return ((256 * (size_t)g->trans_rep * 2 + 15) & ~(size_t)15) + (size_t)g->trans_word_count * g->trans_rep * 4;
+}
+
+// The kernel attribute is per function, shared by every handle: only raise it.
+int ensure_lex_smem(size_t bytes) {
+  static std::mutex mu;
+  static size_t current = 0;
+  std::lock_guard<std::mutex> lock(mu);
+  if (bytes <= current) return ALPACC_OK;
+  if (cudaFuncSetAttribute(lex_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return ALPACC_E_CUDA;
+  }
+  current = bytes;
+  return ALPACC_OK;
+}
 
 // The whole device path for d_in[0..n). Leaves counts in g->last_T / last_N.
 int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
@@ -181,7 +212,7 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
   // ---------------- lexer ----------------
   uint64_t T = 0;
   if (n > 0) {
-    const uint64_t tiles = (n + kLexTile - 1) / kLexTile;
+    const uint64_t tiles = (n + kLexData - 1) / kLexData;
     TRY(grow(g->lex_ticket, 16));
     TRY(grow(g->st1_flag, tiles * 4));
     TRY(grow(g->st1_state, tiles));
@@ -199,10 +230,10 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     a.in = d_in;
     a.n = n;
     a.num_tiles = tiles;
-    a.cls_words = (const uint32_t *)g->cls_words.p;
+    a.cls_id = (const uint8_t *)g->cls_id.p;
     a.trans_words_ptr = (const uint32_t *)g->trans_words.p;
     a.trans_words = g->trans_word_count;
-    a.trans_rep = g->trans_rep;
+    a.copies = g->trans_rep;
     a.lane_of = (const uint8_t *)g->lane_of.p;
     a.img = (const uint8_t *)g->img.p;
     a.img_cnt = (const uint8_t *)g->img_cnt.p;
@@ -229,7 +260,8 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     a.status = g->d_status;
     a.diag = g->diag;
     stage_begin(g, 0);
-    lex_kernel<<<(unsigned)tiles, kLexThreads, lex_smem_bytes(g), g->stream>>>(a);
+    const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)g->lex_grid);
+    lex_kernel<<<grid, kLexThreads, lex_smem_bytes(g), g->stream>>>(a);
     stage_end(g, 0);
     CK(cudaGetLastError());
     int rc = sync_status(g);
@@ -303,6 +335,7 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
   TRY(grow(g->tinc, std::max<uint64_t>(P, 1) * 4));
   TRY(grow(g->tile_min, pse_tiles_max * 4));
   TRY(grow(g->chunk_min, pse_tiles_max * kPseThreads * 4));
+  TRY(grow(g->super_min, ((pse_tiles_max >> kPseSuperShift) + 1) * 4));
   TRY(grow(g->queue, Emax * 8));
   TRY(grow(g->queue_len, 16));
   for (int mode = 0; mode < 2; ++mode) {
@@ -312,6 +345,7 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     CK(cudaMemsetAsync(g->pse_ticket.p, 0, 16, g->stream));
     CK(cudaMemsetAsync(g->pse_flags.p, 0, tiles * 4, g->stream));
     CK(cudaMemsetAsync(g->queue_len.p, 0, 16, g->stream));
+    CK(cudaMemsetAsync(g->super_min.p, 0x7f, ((tiles >> kPseSuperShift) + 1) * 4, g->stream));
     PseArgs a{};
     a.mode = mode;
     a.elems = (const uint32_t *)(mode == kPseBrackets ? g->br.p : g->pr.p);
@@ -324,6 +358,7 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     a.tinc = (int32_t *)g->tinc.p;
     a.tile_min = (int32_t *)g->tile_min.p;
     a.chunk_min = (int32_t *)g->chunk_min.p;
+    a.super_min = (int32_t *)g->super_min.p;
     a.queue = (unsigned long long *)g->queue.p;
     a.queue_cap = Emax;
     a.queue_len = (unsigned long long *)g->queue_len.p;
@@ -483,11 +518,16 @@ alpacc_gpu_grammar *alpacc_gpu_load(const alpacc_tables *tables, int device, uin
   }
   std::memset(g->h_status, 0, sizeof(DeviceStatus));
   rc = upload_tables(g);
+  if (rc == ALPACC_OK) rc = ensure_lex_smem(lex_smem_bytes(g));
   if (rc == ALPACC_OK) {
-    if (cudaFuncSetAttribute(lex_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lex_smem_bytes(g)) !=
-        cudaSuccess) {
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lex_kernel, kLexThreads, lex_smem_bytes(g)) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || per_sm < 1) {
       cudaGetLastError();
       rc = ALPACC_E_CUDA;
+    } else {
+      g->lex_grid = per_sm * sms;
     }
   }
   if (rc == ALPACC_OK && max_input > 0) rc = grow(g->in, max_input + 16);
@@ -504,13 +544,13 @@ void alpacc_gpu_free(alpacc_gpu_grammar *g) {
   if (!g) return;
   cudaSetDevice(g->device);
   if (g->stream) cudaStreamSynchronize(g->stream);
-  DevBuf *bufs[] = {&g->cls_words, &g->trans_words, &g->lane_of, &g->img, &g->img_cnt, &g->sterm, &g->sflags,
+  DevBuf *bufs[] = {&g->cls_id, &g->trans_words, &g->lane_of, &g->img, &g->img_cnt, &g->sterm, &g->sflags,
                     &g->dense, &g->rec_ss, &g->rec_ps, &g->rec_nb, &g->rec_np, &g->stacks, &g->prods,
                     &g->arity, &g->is_term, &g->in, &g->lex_ticket, &g->st1_flag, &g->st1_state, &g->st1_vec,
                     &g->st2_flags, &g->st2_agg, &g->st2_inc, &g->tok_ids, &g->tok_starts, &g->tok_lens,
                     &g->pair_ticket, &g->pst_flags, &g->pst_agg, &g->pst_inc, &g->br, &g->pr, &g->pse_ticket,
                     &g->pse_flags, &g->pse_agg, &g->pse_inc, &g->h, &g->answer, &g->tinc, &g->tile_min,
-                    &g->chunk_min, &g->queue, &g->queue_len, &g->node_prods, &g->node_parents,
+                    &g->chunk_min, &g->super_min, &g->queue, &g->queue_len, &g->node_prods, &g->node_parents,
                     &g->token_parents};
   for (DevBuf *b : bufs) release(*b);
   if (g->pinned_cache) cudaFreeHost(g->pinned_cache);

@@ -8,26 +8,29 @@
 
 namespace alpacc {
 
-// ---- lexer tiles: 256 threads x 15 words (60 bytes) = 15360 bytes ----
+// ---- lexer tiles: 256 chunks x 15 words (60 bytes); the first 8 chunks are
+// a halo repeating the end of the previous tile ----
 constexpr int kLexThreads = 256;
 constexpr int kLexWords = 15;
 constexpr int kLexChunk = kLexWords * 4;
-constexpr int kLexTile = kLexThreads * kLexChunk;
+constexpr int kLexHalo = 8;
+constexpr int kLexLoad = kLexThreads * kLexChunk;               // bytes loaded per tile
+constexpr int kLexData = (kLexThreads - kLexHalo) * kLexChunk;  // new bytes per tile
 
 struct LexArgs {
   const uint8_t *in;
   unsigned long long n;
   unsigned long long num_tiles;
   // minimised machine
-  const uint32_t *cls_words;        // [64] byte classes packed 4 per word
-  const uint32_t *trans_words_ptr;  // [trans_words] M*C next states packed 4 per word
+  const uint8_t *cls_id;            // [256] byte -> class
+  const uint32_t *trans_words_ptr;  // [trans_words] u8 entries (next | produce << 7) at class * M + state
   int trans_words;
-  int trans_rep;                    // copies in shared memory: 32 (one per bank) or 1
+  int copies;                       // table copies in shared memory (power of two <= 32)
   const uint8_t *lane_of;           // [C*M]
   const uint8_t *img;               // [C*kMaxLanes]
   const uint8_t *img_cnt;           // [C]
   const uint8_t *sterm;             // [M]
-  const uint8_t *sflags;            // [M]
+  const uint8_t *sflags;            // [M] bit0 produce, bit1 accept, bit2 kept
   int M, C, dead, m0, ignore;
   unsigned long long len_max;
   // outputs (native widths)
@@ -77,6 +80,8 @@ constexpr int kPseThreads = 256;
 constexpr int kPseItems = 8;
 constexpr int kPseTile = kPseThreads * kPseItems;
 
+constexpr int kPseSuperShift = 8;  // 256 tiles per super-tile
+
 enum PseMode : int { kPseBrackets = 0, kPseParents = 1 };
 
 struct PseArgs {
@@ -91,6 +96,7 @@ struct PseArgs {
   int32_t *tinc;                  // parents: [E] inclusive terminal-production count
   int32_t *tile_min;              // [tiles]
   int32_t *chunk_min;             // [tiles * kPseThreads]
+  int32_t *super_min;             // [ceil(tiles / 256)] minimum over each run of 256 tiles
   unsigned long long *queue;      // pending (element) indices
   unsigned long long queue_cap;
   unsigned long long *queue_len;  // device counter

@@ -1,24 +1,33 @@
 // Data-parallel lexer for sm_100a: the sequential semantics of lex_string
 // (backends/c/lexer.c:39-97) computed tile-parallel.
 //
-// The lexer is a Moore machine over byte classes (device_tables.cpp derives
-// it from TO_STATE / COMPOSE / ACCEPT). A tile is 256 threads x 60 bytes,
-// loaded with 16-byte vector loads into shared memory; 60 bytes = 15 words
-// per thread, an odd stride, so the per-thread walks are bank-conflict free.
+// The lexer runs a Moore machine over byte classes that device_tables.cpp
+// derives from TO_STATE / COMPOSE / ACCEPT: a transition entry holds the next
+// state (7 bits) and that state's produce flag (bit 7), indexed by
+// class * M + state. Persistent CTAs load the tables into shared memory once
+// - the byte-class table and the transition table are replicated (`copies`
+// of each, lane l reading copy l % copies) so data-dependent lookups from one
+// warp rarely meet in a bank - and then take tiles by ticket.
 //
-// Pass 1: each thread computes its chunk's transition function without knowing
-//   its start state by running the machine from every live state the first
-//   byte can lead to ("lanes") and merging lanes that meet; after a few bytes
-//   one lane is left, so the walk costs one table lookup per byte. A chunk
-//   whose lanes merged into one has a constant function (up to death).
-// Tile resolution: thread t's start state follows from the nearest constant
-//   chunk before it (or the tile's incoming state), so a tile that contains
-//   any constant chunk knows its outgoing state before it knows its incoming
-//   state and publishes it at once; look-back therefore rarely waits.
-// Pass 2: every thread re-walks its chunk from its true start, marks token
-//   boundaries (produce flag of the next state) and counts kept tokens; a
-//   (count, last boundary) carry is scanned across the tile and across tiles
-//   by decoupled look-back; tokens are written as structure-of-arrays.
+// A tile is 256 chunks of 60 bytes (15 words: an odd stride, so per-thread
+// walks are bank-conflict free). The first 8 chunks are a halo - the 480
+// bytes before the tile's 14880 data bytes - walked again so that the tile
+// can almost always derive its incoming state by itself.
+//
+// Pass 1: every chunk computes its transition function without knowing its
+//   start state by running the machine from every live state its first byte
+//   can lead to ("lanes") and merging lanes that meet. Once one lane is left
+//   (after a few bytes) the walk costs one lookup per byte and records the
+//   token boundaries it passes: a 64-bit mask, and the state before each
+//   boundary written over the consumed byte. Such a chunk maps every live
+//   start state to one end state ("constant").
+// Resolution: a chunk's start state follows from the nearest constant chunk
+//   before it; only when no halo chunk is constant does the tile read its
+//   predecessor's published outgoing state (decoupled look-back, bounded).
+// Pass 2: each data chunk re-walks only the bytes before its lanes merged,
+//   from its true start, then counts kept tokens over the recorded
+//   boundaries; a (count, last boundary) carry is scanned across the tile and
+//   across tiles by decoupled look-back; tokens are written structure-of-arrays.
 //
 // Reference equivalents: backends/cuda/lexer.cu:437-760 (``lexer`` kernel) and
 // backends/cuda/scan.cu:181-400 (look-back).
@@ -40,59 +49,68 @@ __device__ __forceinline__ void store_uint(void *base, unsigned long long i, int
   }
 }
 
+constexpr int kNotConverged = 255;
+
 struct LexSmem {
-  uint32_t bytes[kLexThreads * kLexWords];      // the tile, linear
-  uint32_t cls[64 * 32];                        // byte -> class, one copy per bank
-  uint8_t lst[kMaxLanes * kLexThreads];         // lane states, slot-major
-  uint8_t lrm[kMaxLanes * kLexThreads];         // original slot -> merged slot
+  uint32_t bytes[kLexThreads * kLexWords];  // the tile; recorded boundary states overwrite consumed bytes
+  uint8_t lst[kMaxLanes * kLexThreads];     // lane states, slot-major
+  uint8_t lrm[kMaxLanes * kLexThreads];     // original slot -> merged slot
   uint16_t active[kLexThreads];
-  uint8_t c0[kLexThreads];
+  uint8_t c0[kLexThreads];      // class id of the chunk's first byte
   uint8_t nbytes[kLexThreads];
-  uint8_t start[kLexThreads];
-  long long scan_tmp[kLexThreads / 32 * 2];
+  uint8_t start[kLexThreads];   // true start state of data chunks
+  uint8_t cstate[kLexThreads];  // lane state just before the recorded part
+  uint8_t sterm[256];           // per machine state: terminal id
+  uint8_t sflags[256];          // bit1 accept, bit2 kept
+  uint8_t cls_id[256];          // byte -> class id (first byte of a chunk)
+  long long scan_tmp[kLexThreads / 32];
   int kconst[kLexThreads];
+  unsigned tile;
   int s_in;
+  int need_lookback;
   int out_published;
-  long long tile_cnt_prefix;
-  long long tile_pos_prefix;
+  long long cnt_prefix, pos_prefix;
 };
 
-struct LexCtx {
-  const LexArgs *a;
-  LexSmem *sm;
-  const uint32_t *trans;  // smem, replicated `rep` times
-  int rep;
-  int lane;
+struct Tabs {
+  const uint16_t *cls;    // [256 * copies] class * M
+  const uint32_t *trans;  // [words * copies] packed u8 entries
+  int copies;
+  int lane_copy;
 };
 
-__device__ __forceinline__ int cls_of(const LexCtx &c, uint32_t b) {
-  return (c.sm->cls[(b >> 2) * 32 + c.lane] >> ((b & 3) * 8)) & 0xff;
+__device__ __forceinline__ uint32_t cls_pre(const Tabs &tb, uint32_t b) {
+  return tb.cls[b * (uint32_t)tb.copies + (uint32_t)tb.lane_copy];
 }
 
-__device__ __forceinline__ int step(const LexCtx &c, int s, int cl) {
-  const uint32_t i = (uint32_t)s * (uint32_t)c.a->C + (uint32_t)cl;
-  const uint32_t w = c.trans[(i >> 2) * c.rep + (c.rep == 32 ? c.lane : 0)];
-  return (w >> ((i & 3) * 8)) & 0xff;
+// entry of (class premultiplied cp, state s): next state | produce << 7
+__device__ __forceinline__ uint32_t entry(const Tabs &tb, uint32_t cp, uint32_t s) {
+  const uint32_t i = cp + s;
+  const uint32_t w = tb.trans[(i >> 2) * (uint32_t)tb.copies + (uint32_t)tb.lane_copy];
+  return __byte_perm(w, 0, i & 3);
 }
 
-__device__ __forceinline__ uint32_t chunk_byte(const LexSmem *sm, int t, int j) {
-  const uint32_t w = sm->bytes[t * kLexWords + (j >> 2)];
-  return (w >> ((j & 3) * 8)) & 0xff;
-}
-
-// f_t(x): the state after thread t's chunk when it starts in state x.
-__device__ __forceinline__ int eval_chunk(const LexCtx &c, int t, int x) {
-  const LexSmem *sm = c.sm;
+// f_t(x): the state after chunk t when it starts in state x.
+__device__ __forceinline__ int eval_chunk(const LexArgs &a, const LexSmem *sm, int t, int x) {
   if (sm->nbytes[t] == 0) return x;
-  const int dead = c.a->dead;
+  const int dead = a.dead;
   if (x == dead) return dead;
-  const int c0 = sm->c0[t];
-  const int slot = __ldg(c.a->lane_of + (size_t)c0 * c.a->M + x);
+  const int slot = __ldg(a.lane_of + (size_t)sm->c0[t] * a.M + x);
   if (slot == 0xff) return dead;
   const int r = sm->lrm[slot * kLexThreads + t];
   if (!((sm->active[t] >> r) & 1)) return dead;
   return sm->lst[r * kLexThreads + t];
 }
+
+__device__ __forceinline__ int const_value(const LexArgs &a, const LexSmem *sm, int k) {
+  const uint32_t act = sm->active[k];
+  if (!act) return a.dead;
+  return sm->lst[(__ffs(act) - 1) * kLexThreads + k];
+}
+
+struct CntPosOp {
+  __device__ Pair64 operator()(Pair64 e, Pair64 l) const { return Pair64{e.a + l.a, e.b > l.b ? e.b : l.b}; }
+};
 
 }  // namespace
 
@@ -100,284 +118,306 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   __shared__ __align__(16) LexSmem sm_static;
   LexSmem *sm = &sm_static;
-  const LexArgs *a = &args;
+  const LexArgs &a = args;
   const int t = threadIdx.x;
   const int lane = t & 31;
-  uint32_t *s_trans = reinterpret_cast<uint32_t *>(dyn_smem);
-  LexCtx c{a, sm, s_trans, a->trans_rep, lane};
-  DeviceStatus *st = a->status;
+  DeviceStatus *st = a.status;
+  const int copies = a.copies;
 
-  // ---- tile ticket (tiles are processed in ticket order) ----
-  __shared__ unsigned s_tile;
-  if (t == 0) s_tile = atomicAdd(a->ticket, 1u);
-  // ---- replicated tables into shared memory ----
-  for (int i = t; i < 64 * 32; i += kLexThreads) sm->cls[i] = __ldg(a->cls_words + (i >> 5));
-  {
-    const int words = a->trans_words * a->trans_rep;
-    for (int i = t; i < words; i += kLexThreads) s_trans[i] = __ldg(a->trans_words_ptr + i / a->trans_rep);
+  // ---- tables, once per CTA ----
+  uint16_t *s_cls = reinterpret_cast<uint16_t *>(dyn_smem);
+  uint32_t *s_trans = reinterpret_cast<uint32_t *>(dyn_smem + ((256 * copies * 2 + 15) & ~15));
+  for (int i = t; i < 256 * copies; i += kLexThreads) s_cls[i] = (uint16_t)(__ldg(a.cls_id + i / copies) * a.M);
+  for (int i = t; i < a.trans_words * copies; i += kLexThreads) s_trans[i] = __ldg(a.trans_words_ptr + i / copies);
+  for (int i = t; i < 256; i += kLexThreads) {
+    sm->sterm[i] = i < a.M ? __ldg(a.sterm + i) : 0;
+    sm->sflags[i] = i < a.M ? __ldg(a.sflags + i) : 0;
+    sm->cls_id[i] = __ldg(a.cls_id + i);
   }
-  __syncthreads();
-  const unsigned long long tile = s_tile;
-  const unsigned long long n = a->n;
-  const unsigned long long base = tile * (unsigned long long)kLexTile;
+  const Tabs tb{s_cls, s_trans, copies, lane & (copies - 1)};
+  const int dead = a.dead;
+  const long long n = (long long)a.n;
+  const unsigned long long num_tiles = a.num_tiles;
 
-  // ---- load the tile ----
-  {
-    const unsigned long long avail = n > base ? n - base : 0;
-    const int tile_bytes = avail >= (unsigned long long)kLexTile ? kLexTile : (int)avail;
-    const uint8_t *src = a->in + base;
-    uint8_t *dst = reinterpret_cast<uint8_t *>(sm->bytes);
-    const bool aligned = ((reinterpret_cast<uintptr_t>(src) & 15) == 0);
-    if (aligned && tile_bytes == kLexTile) {
-      const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
-      uint4 *d4 = reinterpret_cast<uint4 *>(dst);
-      for (int i = t; i < kLexTile / 16; i += kLexThreads) d4[i] = __ldg(s4 + i);
-    } else {
-      for (int i = t; i < kLexTile; i += kLexThreads) dst[i] = i < tile_bytes ? src[i] : 0;
-    }
-  }
-  // ---- per-thread chunk geometry ----
-  const unsigned long long g0 = base + (unsigned long long)t * kLexChunk;
-  const int nb = g0 < n ? (int)((n - g0) < (unsigned long long)kLexChunk ? (n - g0) : kLexChunk) : 0;
-  sm->nbytes[t] = (uint8_t)nb;
-  __syncthreads();
+  for (;;) {
+    __syncthreads();  // tables ready / previous tile fully consumed
+    if (t == 0) sm->tile = atomicAdd(a.ticket, 1u);
+    __syncthreads();
+    const unsigned long long tile = sm->tile;
+    if (tile >= num_tiles) break;
+    const long long data0 = (long long)tile * kLexData;
+    const long long load0 = data0 - (long long)kLexHalo * kLexChunk;
 
-  const int dead = a->dead;
-  // ---- pass 1: chunk function by converging lanes ----
-  {
-    uint32_t active = 0;
-    int c0 = 0;
-    int multi_bytes = 0;
-    if (nb > 0) {
-      c0 = cls_of(c, chunk_byte(sm, t, 0));
-      const int cnt = __ldg(a->img_cnt + c0);
-      active = cnt ? ((1u << cnt) - 1u) : 0u;
-      for (int l = 0; l < cnt; l++) {
-        sm->lst[l * kLexThreads + t] = __ldg(a->img + c0 * kMaxLanes + l);
-        sm->lrm[l * kLexThreads + t] = (uint8_t)l;
-      }
-      const int nl = cnt;
-      int j = 1;
-      // several lanes: step each, drop dead ones, merge equal ones
-      while (j < nb && __popc(active) > 1) {
-        const int cl = cls_of(c, chunk_byte(sm, t, j));
-        for (uint32_t m = active; m; m &= m - 1) {
-          const int l = __ffs(m) - 1;
-          const int s2 = step(c, sm->lst[l * kLexThreads + t], cl);
-          if (s2 == dead) active &= ~(1u << l);
-          else sm->lst[l * kLexThreads + t] = (uint8_t)s2;
-        }
-        for (int l1 = 0; l1 < nl; l1++) {
-          if (!((active >> l1) & 1)) continue;
-          const int s1 = sm->lst[l1 * kLexThreads + t];
-          for (int l2 = l1 + 1; l2 < nl; l2++) {
-            if (((active >> l2) & 1) && sm->lst[l2 * kLexThreads + t] == s1) {
-              active &= ~(1u << l2);
-              for (int k = 0; k < nl; k++)
-                if (sm->lrm[k * kLexThreads + t] == l2) sm->lrm[k * kLexThreads + t] = (uint8_t)l1;
-            }
+    // ---- load halo + data ----
+    {
+      const uint8_t *in = a.in;
+      uint8_t *dst = reinterpret_cast<uint8_t *>(sm->bytes);
+      const bool aligned = ((reinterpret_cast<uintptr_t>(in) & 15) == 0);
+      for (int v = t; v < kLexLoad / 16; v += kLexThreads) {
+        const long long g = load0 + 16ll * v;
+        if (aligned && g >= 0 && g + 16 <= n) {
+          reinterpret_cast<uint4 *>(dst)[v] = __ldg(reinterpret_cast<const uint4 *>(in + g));
+        } else {
+          for (int k = 0; k < 16; ++k) {
+            const long long p = g + k;
+            dst[16 * v + k] = (p >= 0 && p < n) ? in[p] : 0;
           }
         }
-        ++j;
-        ++multi_bytes;
       }
-      // one lane: the hot loop, one lookup per byte
-      if (active && __popc(active) == 1 && j < nb) {
-        const int l = __ffs(active) - 1;
-        int s = sm->lst[l * kLexThreads + t];
-        for (; j < nb; ++j) {
-          s = step(c, s, cls_of(c, chunk_byte(sm, t, j)));
-          if (s == dead) break;
+    }
+    const long long g0 = load0 + (long long)t * kLexChunk;
+    int nb = 0;
+    if (g0 >= 0 && g0 < n) nb = (int)min((long long)kLexChunk, n - g0);
+    sm->nbytes[t] = (uint8_t)nb;
+    __syncthreads();
+
+    // ---- pass 1: lanes until they merge, then one lane recording boundaries ----
+    uint8_t *tb8 = reinterpret_cast<uint8_t *>(sm->bytes) + t * kLexChunk;
+    uint32_t active = 0;
+    unsigned long long bmask = 0;
+    int jconv = kNotConverged;
+    {
+      int c0 = 0;
+      if (nb > 0) {
+        c0 = sm->cls_id[tb8[0]];
+        const int cnt = __ldg(a.img_cnt + c0);
+        active = cnt ? ((1u << cnt) - 1u) : 0u;
+        for (int l = 0; l < cnt; l++) {
+          sm->lst[l * kLexThreads + t] = __ldg(a.img + c0 * kMaxLanes + l);
+          sm->lrm[l * kLexThreads + t] = (uint8_t)l;
         }
-        if (s == dead) active = 0;
-        else sm->lst[l * kLexThreads + t] = (uint8_t)s;
+        int j = 1;
+        while (j < nb && __popc(active) > 1) {
+          const uint32_t cp = cls_pre(tb, tb8[j]);
+          for (uint32_t m = active; m; m &= m - 1) {
+            const int l = __ffs(m) - 1;
+            const int s2 = (int)(entry(tb, cp, sm->lst[l * kLexThreads + t]) & 0x7f);
+            if (s2 == dead) active &= ~(1u << l);
+            else sm->lst[l * kLexThreads + t] = (uint8_t)s2;
+          }
+          if (__popc(active) > 1) {
+            for (uint32_t m1 = active; m1; m1 &= m1 - 1) {
+              const int l1 = __ffs(m1) - 1;
+              if (!((active >> l1) & 1)) continue;
+              const int s1 = sm->lst[l1 * kLexThreads + t];
+              for (uint32_t m2 = active & ~((2u << l1) - 1u); m2; m2 &= m2 - 1) {
+                const int l2 = __ffs(m2) - 1;
+                if (sm->lst[l2 * kLexThreads + t] == s1) {
+                  active &= ~(1u << l2);
+                  for (int k = 0; k < cnt; k++)
+                    if (sm->lrm[k * kLexThreads + t] == l2) sm->lrm[k * kLexThreads + t] = (uint8_t)l1;
+                }
+              }
+            }
+          }
+          ++j;
+        }
+        if (__popc(active) == 1) {
+          const int l = __ffs(active) - 1;
+          uint32_t s = sm->lst[l * kLexThreads + t];
+          jconv = j;
+          sm->cstate[t] = (uint8_t)s;
+          // the hot loop: one class lookup and one transition per byte
+#pragma unroll 4
+          for (; j < nb; ++j) {
+            const uint32_t e = entry(tb, cls_pre(tb, tb8[j]), s);
+            if (e & 0x80) {
+              bmask |= 1ull << j;
+              tb8[j] = (uint8_t)s;  // state of the token ending before byte j
+            }
+            s = e & 0x7f;
+            if ((int)s == dead) break;
+          }
+          if ((int)s == dead) active = 0;
+          else sm->lst[l * kLexThreads + t] = (uint8_t)s;
+        }
       }
-    }
-    sm->active[t] = (uint16_t)active;
-    sm->c0[t] = (uint8_t)c0;
-    if (a->diag) {
-      const unsigned w = __reduce_add_sync(0xffffffffu, (unsigned)multi_bytes);
-      if ((t & 31) == 0) atomicAdd(&st->scratch[3], (unsigned long long)w);
-    }
-  }
-  __syncthreads();
-
-  // ---- tile resolution: nearest constant chunk before each thread ----
-  const bool is_const = nb > 0 && __popc((uint32_t)sm->active[t]) <= 1;
-  long long ktot;
-  long long kex = block_exclusive_scan<long long>(is_const ? (long long)t : -1ll, MaxI64(), -1ll, sm->scan_tmp, &ktot);
-  sm->kconst[t] = (int)kex;
-  if (t == 0) sm->out_published = 0;
-  if (a->diag) {
-    const int nconst = __syncthreads_count(is_const);
-    if (t == 0) {
-      atomicAdd(&st->scratch[1], (unsigned long long)nconst);
-      if (ktot < 0) atomicAdd(&st->scratch[0], 1ull);
-    }
-    const unsigned chain = (unsigned)(kex >= 0 ? t - 1 - kex : t);
-    const unsigned w = __reduce_add_sync(0xffffffffu, chain);
-    if ((t & 31) == 0) atomicAdd(&st->scratch[2], (unsigned long long)w);
-  }
-  __syncthreads();
-
-  // value of a constant chunk (its single live lane, or dead)
-  auto const_value = [&](int k) -> int {
-    const uint32_t act = sm->active[k];
-    if (!act) return dead;
-    return sm->lst[(__ffs(act) - 1) * kLexThreads + k];
-  };
-  const unsigned long long num_tiles = a->num_tiles;
-  if (ktot >= 0) {
-    // outgoing state is independent of the incoming one: publish now
-    if (t == 0) {
-      int x = const_value((int)ktot);
-      for (int jj = (int)ktot + 1; jj < kLexThreads; ++jj) x = eval_chunk(c, jj, x);
-      a->st1_state[tile] = (uint8_t)(x < 0 ? 0 : x);
-      __threadfence();
-      st_release_u32(a->st1_flag + tile, 2u);
-      sm->out_published = 1;
-    }
-  } else if (tile + 1 < num_tiles) {
-    // no constant chunk: publish the tile's full transition vector
-    for (int s = t; s < a->M; s += kLexThreads) {
-      int x = s;
-      for (int jj = 0; jj < kLexThreads; ++jj) x = eval_chunk(c, jj, x);
-      a->st1_vec[tile * (unsigned long long)a->M + s] = (uint8_t)(x < 0 ? 0 : x);
+      sm->active[t] = (uint16_t)active;
+      sm->c0[t] = (uint8_t)c0;
+      if (a.diag) {
+        const unsigned w = __reduce_add_sync(0xffffffffu, (unsigned)(jconv == kNotConverged ? nb : jconv));
+        if (lane == 0) atomicAdd(&st->scratch[3], (unsigned long long)w);
+      }
     }
     __syncthreads();
-    if (t == 0) {
-      __threadfence();
-      st_release_u32(a->st1_flag + tile, 1u);
+
+    // ---- resolution: nearest constant chunk before each chunk ----
+    const bool is_const = nb > 0 && __popc(active) <= 1;
+    long long ktot;
+    const long long kex = block_exclusive_scan<long long>(is_const ? (long long)t : -1ll, MaxI64(), -1ll,
+                                                          sm->scan_tmp, &ktot);
+    sm->kconst[t] = (int)kex;
+    if (t == kLexHalo) sm->need_lookback = kex < 0 ? 1 : 0;
+    if (t == 0) sm->out_published = 0;
+    if (a.diag) {
+      const int nconst = __syncthreads_count(is_const);
+      if (t == 0) atomicAdd(&st->scratch[1], (unsigned long long)nconst);
     }
-  }
-  // ---- incoming state by look-back ----
-  if (t == 0) {
-    int s_in = a->m0;
-    if (tile > 0) {
-      long long j = (long long)tile - 1;
-      int base_state = a->m0;
-      bool have = false;
-      while (j >= 0) {
-        const unsigned f = wait_flag(a->st1_flag + j, 1u, st, kSiteLexState);
-        if (f == 0) break;  // timed out (recorded)
-        if (f >= 2) {
-          base_state = *reinterpret_cast<volatile uint8_t *>(a->st1_state + j);
-          have = true;
-          break;
+    __syncthreads();
+    if (ktot >= 0) {
+      // the outgoing state does not depend on the incoming one: publish now
+      if (t == 0) {
+        int x = const_value(a, sm, (int)ktot);
+        for (int jj = (int)ktot + 1; jj < kLexThreads; ++jj) x = eval_chunk(a, sm, jj, x);
+        a.st1_state[tile] = (uint8_t)(x < 0 ? 0 : x);
+        __threadfence();
+        st_release_u32(a.st1_flag + tile, 2u);
+        sm->out_published = 1;
+      }
+    } else if (tile + 1 < num_tiles) {
+      // no constant chunk at all: publish the data region's transition vector
+      for (int s = t; s < a.M; s += kLexThreads) {
+        int x = s;
+        for (int jj = kLexHalo; jj < kLexThreads; ++jj) x = eval_chunk(a, sm, jj, x);
+        a.st1_vec[tile * (unsigned long long)a.M + s] = (uint8_t)(x < 0 ? 0 : x);
+      }
+      __syncthreads();
+      if (t == 0) {
+        __threadfence();
+        st_release_u32(a.st1_flag + tile, 1u);
+      }
+    }
+    __syncthreads();
+    if (sm->need_lookback) {
+      if (t == 0) {
+        if (a.diag) atomicAdd(&st->scratch[0], 1ull);
+        int s_in = a.m0;
+        if (tile > 0) {
+          long long j = (long long)tile - 1;
+          int base_state = a.m0;
+          bool have = false;
+          while (j >= 0) {
+            const unsigned f = wait_flag(a.st1_flag + j, 1u, st, kSiteLexState);
+            if (f == 0) break;
+            if (f >= 2) {
+              base_state = *reinterpret_cast<volatile uint8_t *>(a.st1_state + j);
+              have = true;
+              break;
+            }
+            --j;
+          }
+          if (!have) j = -1;
+          int x = have ? base_state : a.m0;
+          for (long long jj = j + 1; jj < (long long)tile; ++jj) {
+            if (x == dead || x < 0) break;
+            x = *reinterpret_cast<volatile uint8_t *>(a.st1_vec + jj * (unsigned long long)a.M + x);
+          }
+          s_in = x;
         }
-        --j;
+        sm->s_in = s_in;
       }
-      if (!have) { j = -1; base_state = a->m0; }
-      // tiles j+1 .. tile-1 published transition vectors
-      int x = base_state;
-      for (long long jj = j + 1; jj < (long long)tile; ++jj) {
-        if (x == dead || x < 0) break;
-        x = *reinterpret_cast<volatile uint8_t *>(a->st1_vec + jj * (unsigned long long)a->M + x);
-      }
-      s_in = x;
+      __syncthreads();
     }
-    sm->s_in = s_in;
-  }
-  __syncthreads();
-  // ---- each thread's start state ----
-  {
-    const int k = sm->kconst[t];
-    int x = k < 0 ? sm->s_in : const_value(k);
-    for (int jj = k + 1; jj < t; ++jj) x = eval_chunk(c, jj, x);
-    sm->start[t] = (uint8_t)(x < 0 ? 0 : x);
-  }
-  __syncthreads();
-  if (t == 0 && !sm->out_published) {
-    int x = eval_chunk(c, kLexThreads - 1, sm->start[kLexThreads - 1]);
-    a->st1_state[tile] = (uint8_t)(x < 0 ? 0 : x);
-    __threadfence();
-    st_release_u32(a->st1_flag + tile, 2u);
-  }
+    // ---- each data chunk's start state ----
+    if (t >= kLexHalo) {
+      const int k = sm->kconst[t];
+      int x, from;
+      if (k >= 0) {
+        x = const_value(a, sm, k);
+        from = k + 1;
+      } else {
+        x = sm->s_in;
+        from = kLexHalo;
+      }
+      for (int jj = from; jj < t; ++jj) x = eval_chunk(a, sm, jj, x);
+      sm->start[t] = (uint8_t)(x < 0 ? 0 : x);
+      if (a.diag) {
+        const unsigned w = __reduce_add_sync(0xffffffffu, (unsigned)(t - from));
+        if (lane == 0) atomicAdd(&st->scratch[2], (unsigned long long)w);
+      }
+    }
+    __syncthreads();
+    if (t == 0 && !sm->out_published) {
+      const int x = eval_chunk(a, sm, kLexThreads - 1, sm->start[kLexThreads - 1]);
+      a.st1_state[tile] = (uint8_t)(x < 0 ? 0 : x);
+      __threadfence();
+      st_release_u32(a.st1_flag + tile, 2u);
+    }
 
-  // ---- pass 2a: boundaries and kept-token count from the true start ----
-  const uint8_t *sflags = a->sflags;
-  const uint8_t *sterm = a->sterm;
-  unsigned long long bmask = 0;
-  long long cnt = 0, lastb = 0;
-  int x = sm->start[t];
-  bool final_tok = false;
-  int final_term = 0;
-  {
-    uint8_t *tbytes = reinterpret_cast<uint8_t *>(sm->bytes) + t * kLexChunk;
-    bool died = false;
-    for (int j = 0; j < nb; ++j) {
-      const unsigned long long p = g0 + j;
-      const int y = step(c, x, cls_of(c, tbytes[j]));
-      if (p >= 1 && (__ldg(sflags + y) & 1)) {
-        bmask |= 1ull << j;
-        const int tm = __ldg(sterm + x);
-        tbytes[j] = (uint8_t)tm;  // terminal of the token ending at p-1
-        if (__ldg(sflags + x) & 4) ++cnt;
-        lastb = (long long)p;
+    // ---- pass 2a: re-walk the pre-merge bytes from the true start ----
+    long long cnt = 0, lastb = 0;
+    bool final_tok = false, final_kept = false;
+    int final_term = 0;
+    if (t >= kLexHalo && nb > 0) {
+      int x = sm->start[t];
+      bool died = (x == dead);
+      const int jc = jconv == kNotConverged ? nb : jconv;
+      for (int j = 0; j < jc && !died; ++j) {
+        const uint32_t e = entry(tb, cls_pre(tb, tb8[j]), (uint32_t)x);
+        if (g0 + j >= 1 && (e & 0x80)) {
+          bmask |= 1ull << j;
+          tb8[j] = (uint8_t)x;
+        }
+        x = (int)(e & 0x7f);
+        if (x == dead) died = true;
       }
-      if (y == dead) died = true;
-      x = y;
+      if (!died && jconv != kNotConverged) {
+        if (x != sm->cstate[t]) atomicCAS(&st->error, 0, -1 /* lanes disagree: internal error */);
+        if (!active) died = true;  // the merged lane died further on
+        else x = sm->lst[(__ffs(active) - 1) * kLexThreads + t];
+      }
+      if (died) record_reject(st, &st->lex_reject_reason, 1);
+      for (unsigned long long m = bmask; m; m &= m - 1) {
+        const int j = __ffsll((long long)m) - 1;
+        if (sm->sflags[tb8[j]] & 4) ++cnt;
+      }
+      if (bmask) lastb = g0 + 63 - __clzll((long long)bmask);
+      if (g0 + nb == n) {  // this chunk holds the last byte
+        final_tok = true;
+        final_term = sm->sterm[x];
+        final_kept = (sm->sflags[x] & 4) != 0;
+        if (final_kept) ++cnt;
+        if (!(sm->sflags[x] & 2) || died) record_reject(st, &st->lex_reject_reason, 2);
+      }
     }
-    if (died) record_reject(st, &st->lex_reject_reason, 1);
-    if (nb > 0 && g0 + nb == n) {  // this thread holds the last byte
-      final_tok = true;
-      final_term = __ldg(sterm + x);
-      if (__ldg(sflags + x) & 4) ++cnt;
-      if (!(__ldg(sflags + x) & 2)) record_reject(st, &st->lex_reject_reason, 2);
+    // ---- (count, last boundary) carry ----
+    long long cnt_tot, pos_tot;
+    const long long cnt_ex = block_exclusive_scan<long long>(cnt, AddI64(), 0ll, sm->scan_tmp, &cnt_tot);
+    const long long pos_ex = block_exclusive_scan<long long>(lastb, MaxI64(), 0ll, sm->scan_tmp, &pos_tot);
+    if (t == 0) {
+      const Pair64 agg{cnt_tot, pos_tot};
+      Pair64 prefix{0, 0};
+      if (tile > 0) {
+        publish_pair(a.st2, (long long)tile, agg, false);
+        prefix = lookback_pair(a.st2, (long long)tile, Pair64{0, 0}, CntPosOp(), st, kSiteLexCount);
+      }
+      const Pair64 inc = CntPosOp()(prefix, agg);
+      publish_pair(a.st2, (long long)tile, inc, true);
+      sm->cnt_prefix = prefix.a;
+      sm->pos_prefix = prefix.b;
+      if (tile + 1 == num_tiles) st->num_tokens = (unsigned long long)inc.a;
     }
-  }
-  // ---- (count, last boundary) carry: block scan then look-back ----
-  long long cnt_tot, pos_tot;
-  const long long cnt_ex = block_exclusive_scan<long long>(cnt, AddI64(), 0ll, sm->scan_tmp, &cnt_tot);
-  const long long pos_ex = block_exclusive_scan<long long>(lastb, MaxI64(), 0ll, sm->scan_tmp, &pos_tot);
-  if (t == 0) {
-    struct PairOp {
-      __device__ Pair64 operator()(Pair64 e, Pair64 l) const { return Pair64{e.a + l.a, e.b > l.b ? e.b : l.b}; }
-    };
-    Pair64 agg{cnt_tot, pos_tot};
-    Pair64 prefix{0, 0};
-    if (tile > 0) {
-      publish_pair(a->st2, (long long)tile, agg, false);
-      prefix = lookback_pair(a->st2, (long long)tile, Pair64{0, 0}, PairOp(), st, kSiteLexCount);
-    }
-    const Pair64 inc = PairOp()(prefix, agg);
-    publish_pair(a->st2, (long long)tile, inc, true);
-    sm->tile_cnt_prefix = prefix.a;
-    sm->tile_pos_prefix = prefix.b;
-    if (tile + 1 == num_tiles) st->num_tokens = (unsigned long long)inc.a;
-  }
-  __syncthreads();
+    __syncthreads();
 
-  // ---- pass 2b: write this chunk's kept tokens ----
-  {
-    unsigned long long out = (unsigned long long)(sm->tile_cnt_prefix + cnt_ex);
-    long long tok_start = sm->tile_pos_prefix > pos_ex ? sm->tile_pos_prefix : pos_ex;
-    const uint8_t *tbytes = reinterpret_cast<const uint8_t *>(sm->bytes) + t * kLexChunk;
-    const int ignore = a->ignore;
-    const unsigned long long len_max = a->len_max;
-    bool too_long = false;
-    for (unsigned long long m = bmask; m; m &= m - 1) {
-      const int j = __ffsll((long long)m) - 1;
-      const long long p = (long long)(g0 + j);
-      const int tm = tbytes[j];
-      if (tm != ignore) {
-        const unsigned long long len = (unsigned long long)(p - tok_start);
+    // ---- pass 2b: write this chunk's kept tokens ----
+    if (t >= kLexHalo && nb > 0) {
+      unsigned long long out = (unsigned long long)(sm->cnt_prefix + cnt_ex);
+      long long tok_start = sm->pos_prefix > pos_ex ? sm->pos_prefix : pos_ex;
+      const unsigned long long len_max = a.len_max;
+      bool too_long = false;
+      for (unsigned long long m = bmask; m; m &= m - 1) {
+        const int j = __ffsll((long long)m) - 1;
+        const long long p = g0 + j;
+        const int s = tb8[j];
+        if (sm->sflags[s] & 4) {
+          const unsigned long long len = (unsigned long long)(p - tok_start);
+          if (len > len_max) too_long = true;
+          store_uint(a.tok_ids, out, a.term_w, (unsigned long long)sm->sterm[s]);
+          store_uint(a.tok_starts, out, a.idx_w, (unsigned long long)tok_start);
+          store_uint(a.tok_lens, out, a.len_w, len);
+          ++out;
+        }
+        tok_start = p;
+      }
+      if (final_tok && final_kept) {
+        const unsigned long long len = (unsigned long long)(n - tok_start);
         if (len > len_max) too_long = true;
-        store_uint(a->tok_ids, out, a->term_w, (unsigned long long)tm);
-        store_uint(a->tok_starts, out, a->idx_w, (unsigned long long)tok_start);
-        store_uint(a->tok_lens, out, a->len_w, len);
-        ++out;
+        store_uint(a.tok_ids, out, a.term_w, (unsigned long long)final_term);
+        store_uint(a.tok_starts, out, a.idx_w, (unsigned long long)tok_start);
+        store_uint(a.tok_lens, out, a.len_w, len);
       }
-      tok_start = p;
+      if (too_long) record_reject(st, &st->lex_reject_reason, 3);
     }
-    if (final_tok && final_term != ignore) {
-      const unsigned long long len = n - (unsigned long long)tok_start;
-      if (len > len_max) too_long = true;
-      store_uint(a->tok_ids, out, a->term_w, (unsigned long long)final_term);
-      store_uint(a->tok_starts, out, a->idx_w, (unsigned long long)tok_start);
-      store_uint(a->tok_lens, out, a->len_w, len);
-    }
-    if (too_long) record_reject(st, &st->lex_reject_reason, 3);
   }
 }
 

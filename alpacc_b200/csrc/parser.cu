@@ -143,9 +143,11 @@ __global__ void __launch_bounds__(kPairThreads) pair_kernel(PairArgs a) {
 
 namespace {
 
+constexpr int kPseStride = kPseItems + 1;  // odd word stride: conflict-free per-thread rows
+
 struct PseSmem {
-  int32_t h[kPseTile];
-  uint32_t v[kPseTile];
+  int32_t h[kPseThreads * kPseStride];
+  uint32_t v[kPseThreads * kPseStride];
   int32_t lv[8][kPseThreads];   // lv[l][i] = min of chunk minima (i-2^l, i]
   int32_t pm[kPseThreads];      // prefix minimum of chunk minima
   long long tmp[kPseThreads / 32];
@@ -188,7 +190,7 @@ __global__ void __launch_bounds__(kPseThreads) pse_tile_kernel(PseArgs a) {
       stp = pse_step(a, v);
       if (parents) tm = __ldg(a.is_term + v) ? 1 : 0;
     }
-    sm.v[t * kPseItems + j] = v;
+    sm.v[t * kPseStride + j] = v;
     rel[j] = (int)ssum;
     ssum += stp;
     tsum += tm;
@@ -227,7 +229,7 @@ __global__ void __launch_bounds__(kPseThreads) pse_tile_kernel(PseArgs a) {
     const long long e = tile0 + (long long)t * kPseItems + j;
     const long long hv = base + sm.prefix_a + ex_s + rel[j];
     const int32_t h = (int32_t)hv;
-    sm.h[t * kPseItems + j] = h;
+    sm.h[t * kPseStride + j] = h;
     if (e < E) {
       a.h[e] = h;
       if (h < cmin) cmin = h;
@@ -253,7 +255,11 @@ __global__ void __launch_bounds__(kPseThreads) pse_tile_kernel(PseArgs a) {
     const int o = sm.lv[7][t - 128];
     if (o < sm.pm[t]) sm.pm[t] = o;
   }
-  if (t == 0) a.tile_min[tile] = sm.lv[7][kPseThreads - 1] < sm.lv[7][127] ? sm.lv[7][kPseThreads - 1] : sm.lv[7][127];
+  if (t == 0) {
+    const int32_t tm = sm.lv[7][kPseThreads - 1] < sm.lv[7][127] ? sm.lv[7][kPseThreads - 1] : sm.lv[7][127];
+    a.tile_min[tile] = tm;
+    atomicMin(a.super_min + (tile >> kPseSuperShift), tm);
+  }
   __syncthreads();
 
   // ---- queries ----
@@ -264,8 +270,8 @@ __global__ void __launch_bounds__(kPseThreads) pse_tile_kernel(PseArgs a) {
     ans[j] = INT_MIN;  // INT_MIN: no query
     const long long e = tile0 + (long long)t * kPseItems + j;
     if (e >= E) continue;
-    const uint32_t v = sm.v[t * kPseItems + j];
-    const int32_t h = sm.h[t * kPseItems + j];
+    const uint32_t v = sm.v[t * kPseStride + j];
+    const int32_t h = sm.h[t * kPseStride + j];
     int32_t qv;
     if (parents) {
       if (e == 0) {
@@ -279,7 +285,7 @@ __global__ void __launch_bounds__(kPseThreads) pse_tile_kernel(PseArgs a) {
     }
     int32_t found = -1;
     for (int jj = j - 1; jj >= 0; --jj)
-      if (sm.h[t * kPseItems + jj] <= qv) {
+      if (sm.h[t * kPseStride + jj] <= qv) {
         found = t * kPseItems + jj;
         break;
       }
@@ -288,14 +294,15 @@ __global__ void __launch_bounds__(kPseThreads) pse_tile_kernel(PseArgs a) {
       for (int l = 7; l >= 0; --l)
         if (pos - (1 << l) + 1 >= 0 && sm.lv[l][pos] > qv) pos -= 1 << l;
       for (int jj = kPseItems - 1; jj >= 0; --jj)
-        if (sm.h[pos * kPseItems + jj] <= qv) {
+        if (sm.h[pos * kPseStride + jj] <= qv) {
           found = pos * kPseItems + jj;
           break;
         }
     }
     if (found >= 0) {
       if (!parents) {
-        if ((sm.v[found] & 0x7fffffffu) != (v & 0x7fffffffu)) record_reject(st, &st->parse_reject_reason, 2);
+        const uint32_t pv = sm.v[(found / kPseItems) * kPseStride + found % kPseItems];
+        if ((pv & 0x7fffffffu) != (v & 0x7fffffffu)) record_reject(st, &st->parse_reject_reason, 2);
       }
       ans[j] = (int32_t)(tile0 + found);
     } else {
@@ -322,38 +329,63 @@ __global__ void __launch_bounds__(kPseThreads) pse_tile_kernel(PseArgs a) {
   }
 }
 
+namespace {
+
+// Latest index in [lo, hi] whose value is <= qv, or -1; one warp, 32 values
+// per step, highest index first.
+__device__ __forceinline__ long long warp_latest_le(const int32_t *arr, long long hi, long long lo, int32_t qv,
+                                                    int lane) {
+  for (long long base = hi; base >= lo; base -= 32) {
+    const long long idx = base - lane;
+    const int32_t v = idx >= lo ? arr[idx] : INT_MAX;
+    const unsigned b = __ballot_sync(0xffffffffu, v <= qv);
+    if (b) return base - (__ffs(b) - 1);
+  }
+  return -1;
+}
+
+}  // namespace
+
+// One warp per queued query: latest tile whose minimum is <= the query
+// (within the query's super-tile of 256 tiles, else via super-tile minima),
+// then the latest chunk of that tile, then the latest element of that chunk.
 __global__ void pse_resolve_kernel(PseArgs a) {
   DeviceStatus *st = a.status;
   const unsigned long long qn = *a.queue_len;
   const long long E = (long long)*a.count;
   const bool parents = a.mode == kPseParents;
-  for (unsigned long long qi = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; qi < qn && qi < a.queue_cap;
-       qi += (unsigned long long)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long warp = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long warps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+  for (unsigned long long qi = warp; qi < qn && qi < a.queue_cap; qi += warps) {
     const long long e = (long long)a.queue[qi];
     const uint32_t v = a.elems[e];
     const int32_t h = a.h[e];
     const int32_t qv = parents ? h : h - 1;
     const long long tile = e / kPseTile;
+    const long long sup0 = (tile >> kPseSuperShift) << kPseSuperShift;
+    long long tt = warp_latest_le(a.tile_min, tile - 1, sup0, qv, lane);
+    if (tt < 0 && sup0 > 0) {
+      const long long sp = warp_latest_le(a.super_min, (sup0 >> kPseSuperShift) - 1, 0, qv, lane);
+      if (sp >= 0) tt = warp_latest_le(a.tile_min, ((sp + 1) << kPseSuperShift) - 1, sp << kPseSuperShift, qv, lane);
+    }
     long long found = -1;
-    for (long long tt = tile - 1; tt >= 0 && found < 0; --tt) {
-      if (a.tile_min[tt] > qv) continue;
-      for (int c = kPseThreads - 1; c >= 0 && found < 0; --c) {
-        if (a.chunk_min[tt * kPseThreads + c] > qv) continue;
-        for (int jj = kPseItems - 1; jj >= 0; --jj) {
-          const long long idx = tt * kPseTile + (long long)c * kPseItems + jj;
-          if (idx < E && a.h[idx] <= qv) {
-            found = idx;
-            break;
-          }
-        }
+    if (tt >= 0) {
+      const long long c = warp_latest_le(a.chunk_min + tt * kPseThreads, kPseThreads - 1, 0, qv, lane);
+      if (c >= 0) {
+        const long long base = tt * kPseTile + c * kPseItems;
+        const long long hi = base + kPseItems - 1 < E - 1 ? base + kPseItems - 1 : E - 1;
+        found = warp_latest_le(a.h, hi, base, qv, lane);
       }
     }
-    if (parents) {
-      // compute_parents takes 0 when its stack is empty
-      a.answer[e] = found >= 0 ? (int32_t)found : 0;
-    } else {
-      if (found < 0) record_reject(st, &st->parse_reject_reason, 3);
-      else if ((a.elems[found] & 0x7fffffffu) != (v & 0x7fffffffu)) record_reject(st, &st->parse_reject_reason, 2);
+    if (lane == 0) {
+      if (parents) {
+        // compute_parents takes 0 when its stack is empty
+        a.answer[e] = found >= 0 ? (int32_t)found : 0;
+      } else {
+        if (found < 0) record_reject(st, &st->parse_reject_reason, 3);
+        else if ((a.elems[found] & 0x7fffffffu) != (v & 0x7fffffffu)) record_reject(st, &st->parse_reject_reason, 2);
+      }
     }
   }
 }
