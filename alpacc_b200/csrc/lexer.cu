@@ -309,6 +309,7 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
       __syncthreads();
     }
     // ---- each data chunk's start state ----
+    unsigned chain = 0;
     if (t >= kLexHalo) {
       const int k = sm->kconst[t];
       int x, from;
@@ -321,10 +322,11 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
       }
       for (int jj = from; jj < t; ++jj) x = eval_chunk(a, sm, jj, x);
       sm->start[t] = (uint8_t)(x < 0 ? 0 : x);
-      if (a.diag) {
-        const unsigned w = __reduce_add_sync(0xffffffffu, (unsigned)(t - from));
-        if (lane == 0) atomicAdd(&st->scratch[2], (unsigned long long)w);
-      }
+      chain = (unsigned)(t - from);
+    }
+    if (a.diag) {  // every lane of the warp takes part
+      const unsigned w = __reduce_add_sync(0xffffffffu, chain);
+      if (lane == 0) atomicAdd(&st->scratch[2], (unsigned long long)w);
     }
     __syncthreads();
     if (t == 0 && !sm->out_published) {
