@@ -140,6 +140,24 @@ int alpacc_gpu_parse(alpacc_gpu_grammar *g, const uint8_t *in, uint64_t n, alpac
 int alpacc_gpu_parse_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, alpacc_result *out);
 
 /*
+ * Lex device-resident bytes into caller-provided device arrays (terminal_t,
+ * index_t and length_t, room for n tokens each) without allocating anything
+ * at call time. This entry point has no counterpart in the reference. It is
+ * for callers that must not call cudaMalloc where they lex: a host framework
+ * whose caching allocator owns the device memory, or a real-time loop that
+ * cannot take the allocator's locks or wait on its synchronisation. The
+ * lexer's working memory is a fixed array inside the library, sized for
+ * inputs of at most 16 MiB (larger n returns ALPACC_E_CAPACITY). Every call
+ * shares that array, so calls must not overlap on the GPU (two streams, two
+ * threads or two handles on one device race on it); the array's address is
+ * looked up on the first call on each device, which should therefore come
+ * before any stream capture. Returns ALPACC_OK with *num_tokens set,
+ * ALPACC_REJECT, or an error.
+ */
+int alpacc_gpu_lex_noalloc(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, void *d_token_ids,
+                           void *d_token_starts, void *d_token_lengths, uint64_t *num_tokens);
+
+/*
  * Enqueue the device path for device-resident input without waiting; the
  * status and counts are written to device memory and read back later with
  * alpacc_gpu_collect. For timing loops and CUDA-graph capture.
