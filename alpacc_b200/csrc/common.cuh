@@ -157,7 +157,8 @@ struct Pair64 {
 //
 // Tile i publishes its aggregate (flag 1) as soon as it is known and its
 // inclusive prefix (flag 2) once the look-back resolved. A tile walks back
-// from i-1, combining aggregates until it meets an inclusive prefix.
+// from i-1, combining aggregates until it meets an inclusive prefix; one warp
+// examines 32 predecessors per step.
 // `tiles` holds per tile: flag (u32) in flags[i], aggregate in agg[i], inclusive
 // in inc[i] (two u64 each).
 // ---------------------------------------------------------------------------
@@ -177,25 +178,51 @@ __device__ __forceinline__ void publish_pair(PairTileState ts, long long tile, P
   unsigned long long *dst = inclusive ? ts.inc : ts.agg;
   st_relaxed_u64(dst + 2 * tile, (unsigned long long)v.a);
   st_relaxed_u64(dst + 2 * tile + 1, (unsigned long long)v.b);
-  __threadfence();
-  st_release_u32(ts.flags + tile, inclusive ? 2u : 1u);
+  st_release_u32(ts.flags + tile, inclusive ? 2u : 1u);  // orders the payload stores before the flag
 }
 
-// Exclusive prefix of tile `tile` (called by one thread). `op(earlier, later)`.
+// Exclusive prefix of tile `tile`, computed by all 32 lanes of one warp (the
+// result is returned to every lane). Each round reads the flags of the 32
+// nearest unexamined predecessors at once (lane l: tile - 1 - l - 32*round),
+// waits (bounded) until all of them have published, combines the aggregates
+// up to the nearest inclusive prefix and stops there. `op` must be
+// associative and commutative (sums and maxima here), so the lanes' values can
+// be combined in any order.
 template <typename Op>
-__device__ Pair64 lookback_pair(PairTileState ts, long long tile, Pair64 identity, Op op, DeviceStatus *st, int site) {
+__device__ Pair64 warp_lookback_pair(PairTileState ts, long long tile, Pair64 identity, Op op, DeviceStatus *st,
+                                     int site) {
+  const int lane = threadIdx.x & (kWarp - 1);
   Pair64 acc = identity;
-  long long j = tile - 1;
-  while (j >= 0) {
-    unsigned f = wait_flag(ts.flags + j, 1u, st, site);
-    if (f == 0) return acc;  // timed out: neutral continuation
-    if (f >= 2) {
-      Pair64 v{(long long)ld_relaxed_u64(ts.inc + 2 * j), (long long)ld_relaxed_u64(ts.inc + 2 * j + 1)};
-      return op(v, acc);
+  for (long long hi = tile - 1; hi >= 0; hi -= kWarp) {
+    const long long j = hi - lane;
+    unsigned f = j >= 0 ? ld_acquire_u32(ts.flags + j) : 2u;  // before tile 0: an inclusive identity
+    unsigned ns = 32;
+    unsigned it = 0;
+    while (__any_sync(0xffffffffu, f == 0u)) {
+      const bool failed = __any_sync(0xffffffffu, *reinterpret_cast<volatile int *>(&st->error) != 0);
+      if (failed || ++it >= kSpinLimit) {
+        if (!failed && lane == 0) record_timeout(st, site);
+        return acc;  // neutral continuation; the status word carries the failure
+      }
+      __nanosleep(ns);
+      if (ns < 1024) ns <<= 1;
+      if (f == 0u) f = ld_acquire_u32(ts.flags + j);
     }
-    Pair64 v{(long long)ld_relaxed_u64(ts.agg + 2 * j), (long long)ld_relaxed_u64(ts.agg + 2 * j + 1)};
+    const unsigned incl = __ballot_sync(0xffffffffu, f >= 2u);
+    const int stop = incl ? __ffs(incl) - 1 : kWarp;  // nearest predecessor holding an inclusive prefix
+    Pair64 v = identity;
+    if (j >= 0 && lane < stop) {
+      v = Pair64{(long long)ld_relaxed_u64(ts.agg + 2 * j), (long long)ld_relaxed_u64(ts.agg + 2 * j + 1)};
+    } else if (j >= 0 && lane == stop) {
+      v = Pair64{(long long)ld_relaxed_u64(ts.inc + 2 * j), (long long)ld_relaxed_u64(ts.inc + 2 * j + 1)};
+    }
+#pragma unroll
+    for (int d = kWarp / 2; d; d >>= 1) {
+      const Pair64 o{__shfl_xor_sync(0xffffffffu, v.a, d), __shfl_xor_sync(0xffffffffu, v.b, d)};
+      v = op(v, o);
+    }
     acc = op(v, acc);
-    --j;
+    if (incl) break;
   }
   return acc;
 }

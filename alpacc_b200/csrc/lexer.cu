@@ -376,18 +376,20 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
     long long cnt_tot, pos_tot;
     const long long cnt_ex = block_exclusive_scan<long long>(cnt, AddI64(), 0ll, sm->scan_tmp, &cnt_tot);
     const long long pos_ex = block_exclusive_scan<long long>(lastb, MaxI64(), 0ll, sm->scan_tmp, &pos_tot);
-    if (t == 0) {
+    if (t < kWarp) {
       const Pair64 agg{cnt_tot, pos_tot};
       Pair64 prefix{0, 0};
       if (tile > 0) {
-        publish_pair(a.st2, (long long)tile, agg, false);
-        prefix = lookback_pair(a.st2, (long long)tile, Pair64{0, 0}, CntPosOp(), st, kSiteLexCount);
+        if (t == 0) publish_pair(a.st2, (long long)tile, agg, false);
+        prefix = warp_lookback_pair(a.st2, (long long)tile, Pair64{0, 0}, CntPosOp(), st, kSiteLexCount);
       }
-      const Pair64 inc = CntPosOp()(prefix, agg);
-      publish_pair(a.st2, (long long)tile, inc, true);
-      sm->cnt_prefix = prefix.a;
-      sm->pos_prefix = prefix.b;
-      if (tile + 1 == num_tiles) st->num_tokens = (unsigned long long)inc.a;
+      if (t == 0) {
+        const Pair64 inc = CntPosOp()(prefix, agg);
+        publish_pair(a.st2, (long long)tile, inc, true);
+        sm->cnt_prefix = prefix.a;
+        sm->pos_prefix = prefix.b;
+        if (tile + 1 == num_tiles) st->num_tokens = (unsigned long long)inc.a;
+      }
     }
     __syncthreads();
 

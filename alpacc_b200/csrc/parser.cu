@@ -99,20 +99,22 @@ __global__ void __launch_bounds__(kPairThreads) pair_kernel(PairArgs a) {
   long long tb, tp;
   const long long eb = block_exclusive_scan<long long>(sb, AddI64(), 0ll, s_tmp, &tb);
   const long long ep = block_exclusive_scan<long long>(sp, AddI64(), 0ll, s_tmp, &tp);
-  if (t == 0) {
-    Pair64 agg{tb, tp};
+  if (t < kWarp) {
+    const Pair64 agg{tb, tp};
     Pair64 prefix{0, 0};
     if (tile > 0) {
-      publish_pair(a.st, (long long)tile, agg, false);
-      prefix = lookback_pair(a.st, (long long)tile, Pair64{0, 0}, AddPair(), st, kSitePairs);
+      if (t == 0) publish_pair(a.st, (long long)tile, agg, false);
+      prefix = warp_lookback_pair(a.st, (long long)tile, Pair64{0, 0}, AddPair(), st, kSitePairs);
     }
-    const Pair64 inc{prefix.a + agg.a, prefix.b + agg.b};
-    publish_pair(a.st, (long long)tile, inc, true);
-    s_prefix_b = prefix.a;
-    s_prefix_p = prefix.b;
-    if (tile0 + kPairTile >= m) {  // last data tile
-      st->num_brackets = (unsigned long long)inc.a;
-      st->num_productions = (unsigned long long)inc.b;
+    if (t == 0) {
+      const Pair64 inc{prefix.a + agg.a, prefix.b + agg.b};
+      publish_pair(a.st, (long long)tile, inc, true);
+      s_prefix_b = prefix.a;
+      s_prefix_p = prefix.b;
+      if (tile0 + kPairTile >= m) {  // last data tile
+        st->num_brackets = (unsigned long long)inc.a;
+        st->num_productions = (unsigned long long)inc.b;
+      }
     }
   }
   __syncthreads();
@@ -163,7 +165,7 @@ __device__ __forceinline__ int pse_step(const PseArgs &a, uint32_t v) {
 
 }  // namespace
 
-__global__ void __launch_bounds__(kPseThreads) pse_tile_kernel(PseArgs a) {
+__global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   __shared__ unsigned s_tile;
   __shared__ PseSmem sm;
   const int t = threadIdx.x;
@@ -199,44 +201,22 @@ __global__ void __launch_bounds__(kPseThreads) pse_tile_kernel(PseArgs a) {
   long long tot_s, tot_t;
   const long long ex_s = block_exclusive_scan<long long>(ssum, AddI64(), 0ll, sm.tmp, &tot_s);
   const long long ex_t = block_exclusive_scan<long long>(tsum, AddI64(), 0ll, sm.tmp, &tot_t);
-  if (t == 0) {
-    Pair64 agg{tot_s, tot_t};
-    Pair64 prefix{0, 0};
-    if (tile > 0) {
-      publish_pair(a.st, (long long)tile, agg, false);
-      prefix = lookback_pair(a.st, (long long)tile, Pair64{0, 0}, AddPair(), st, kSitePse);
-    }
-    const Pair64 inc{prefix.a + agg.a, prefix.b + agg.b};
-    publish_pair(a.st, (long long)tile, inc, true);
-    sm.prefix_a = prefix.a;
-    sm.prefix_b = prefix.b;
-    if (tile0 + kPseTile >= E) {  // last tile: global checks
-      if (!parents) {
-        if (inc.a != 0) record_reject(st, &st->parse_reject_reason, 3);
-      } else {
-        const long long T = (long long)st->num_tokens;
-        if (inc.b != T) record_reject(st, &st->parse_reject_reason, 4);
-        st->num_nodes = (unsigned long long)(E - inc.b);
-      }
-    }
-  }
-  __syncthreads();
-  // ---- absolute depths, chunk minima ----
-  const int base = parents ? 1 : 0;
+  // Publish the aggregate at once, so that later tiles' look-back can pass
+  // this tile while it is still searching; tile 0's aggregate is its
+  // inclusive prefix.
+  if (t == 0) publish_pair(a.st, (long long)tile, Pair64{tot_s, tot_t}, tile == 0);
+
+  // ---- depths relative to the tile start, chunk minima ----
+  // The search compares depths only with each other, so it runs on relative
+  // depths; the tile's offset is added when the results are written.
   int cmin = INT_MAX;
 #pragma unroll
   for (int j = 0; j < kPseItems; ++j) {
     const long long e = tile0 + (long long)t * kPseItems + j;
-    const long long hv = base + sm.prefix_a + ex_s + rel[j];
-    const int32_t h = (int32_t)hv;
+    const int32_t h = (int32_t)(ex_s + rel[j]);
     sm.h[t * kPseStride + j] = h;
-    if (e < E) {
-      a.h[e] = h;
-      if (h < cmin) cmin = h;
-      if (parents) a.tinc[e] = (int32_t)(sm.prefix_b + ex_t + loc_term[j]);
-    }
+    if (e < E && h < cmin) cmin = h;
   }
-  a.chunk_min[tile * kPseThreads + t] = cmin;
   sm.lv[0][t] = cmin;
   __syncthreads();
   for (int l = 1; l < 8; ++l) {
@@ -255,14 +235,9 @@ __global__ void __launch_bounds__(kPseThreads) pse_tile_kernel(PseArgs a) {
     const int o = sm.lv[7][t - 128];
     if (o < sm.pm[t]) sm.pm[t] = o;
   }
-  if (t == 0) {
-    const int32_t tm = sm.lv[7][kPseThreads - 1] < sm.lv[7][127] ? sm.lv[7][kPseThreads - 1] : sm.lv[7][127];
-    a.tile_min[tile] = tm;
-    atomicMin(a.super_min + (tile >> kPseSuperShift), tm);
-  }
   __syncthreads();
 
-  // ---- queries ----
+  // ---- queries inside the tile ----
   int pending = 0;
   int32_t ans[kPseItems];
 #pragma unroll
@@ -310,11 +285,49 @@ __global__ void __launch_bounds__(kPseThreads) pse_tile_kernel(PseArgs a) {
       ++pending;
     }
   }
-  // ---- write answers, queue the rest ----
   long long tot_p;
   const long long ex_p = block_exclusive_scan<long long>(pending, AddI64(), 0ll, sm.tmp, &tot_p);
-  if (t == 0 && tot_p > 0) sm.qbase = atomicAdd(a.queue_len, (unsigned long long)tot_p);
+
+  // ---- the tile's prefix: look-back by warp 0, now that predecessors had time ----
+  if (t < kWarp) {
+    Pair64 prefix{0, 0};
+    if (tile > 0) prefix = warp_lookback_pair(a.st, (long long)tile, Pair64{0, 0}, AddPair(), st, kSitePse);
+    if (t == 0) {
+      const Pair64 inc{prefix.a + tot_s, prefix.b + tot_t};
+      if (tile > 0) publish_pair(a.st, (long long)tile, inc, true);
+      sm.prefix_a = prefix.a;
+      sm.prefix_b = prefix.b;
+      if (tot_p > 0) sm.qbase = atomicAdd(a.queue_len, (unsigned long long)tot_p);
+      if (tile0 + kPseTile >= E) {  // last tile: global checks
+        if (!parents) {
+          if (inc.a != 0) record_reject(st, &st->parse_reject_reason, 3);
+        } else {
+          const long long T = (long long)st->num_tokens;
+          if (inc.b != T) record_reject(st, &st->parse_reject_reason, 4);
+          st->num_nodes = (unsigned long long)(E - inc.b);
+        }
+      }
+    }
+  }
   __syncthreads();
+
+  // ---- absolute depths, minima, terminal counts, answers, queue ----
+  const int32_t off = (int32_t)((parents ? 1 : 0) + sm.prefix_a);
+#pragma unroll
+  for (int j = 0; j < kPseItems; ++j) {
+    const long long e = tile0 + (long long)t * kPseItems + j;
+    if (e < E) {
+      a.h[e] = sm.h[t * kPseStride + j] + off;
+      if (parents) a.tinc[e] = (int32_t)(sm.prefix_b + ex_t + loc_term[j]);
+    }
+  }
+  a.chunk_min[tile * kPseThreads + t] = cmin == INT_MAX ? INT_MAX : cmin + off;
+  if (t == 0) {
+    const int32_t r = sm.lv[7][kPseThreads - 1] < sm.lv[7][127] ? sm.lv[7][kPseThreads - 1] : sm.lv[7][127];
+    const int32_t tm = r + off;  // the tile holds at least one element
+    a.tile_min[tile] = tm;
+    atomicMin(a.super_min + (tile >> kPseSuperShift), tm);
+  }
   unsigned long long qi = sm.qbase + (unsigned long long)ex_p;
 #pragma unroll
   for (int j = 0; j < kPseItems; ++j) {

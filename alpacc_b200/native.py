@@ -174,13 +174,15 @@ class Parser:
         self.layout = wire.Layout.of(tables)
         self._struct, self._keep = make_tables(tables)
         err = ctypes.c_int(0)
-        self._h = lib().alpacc_gpu_load(ctypes.byref(self._struct), device, max_input, ctypes.byref(err))
+        self._lib = lib()
+        self._h = self._lib.alpacc_gpu_load(ctypes.byref(self._struct), device, max_input, ctypes.byref(err))
         if not self._h:
             raise AlpaccError(err.value, lib().alpacc_strerror(err.value).decode())
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().alpacc_gpu_free(self._h)
+            # the instance's own reference: module globals may be gone at interpreter exit
+            self._lib.alpacc_gpu_free(self._h)
             self._h = None
 
     def __del__(self):

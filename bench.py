@@ -63,13 +63,19 @@ class ClockSampler:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # the timed region is short: start it only once sampling is running
+        t0 = time.time()
+        while time.time() - t0 < 10 and self.proc.poll() is None and os.path.getsize(self.path) == 0:
+            time.sleep(0.02)
 
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.06)  # one more sample at the end of the region
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -117,28 +123,40 @@ def kernel_bytes(stage, n, T, B, P, N, lay):
     return 0
 
 
-def cpu_baseline_sample(n_sample: int, seed: int):
-    """The reference C backend, single thread, on one bounded document."""
+def cpu_baseline_sample(host: bytes, n_sample: int, reps: int = 4):
+    """The reference C backend, single thread (it is sequential), on the timed
+    document itself when n_sample >= its size, otherwise on a seeded document
+    of n_sample bytes from the same generator."""
     from alpacc_b200 import workloads as W
     from oracle.ref import RefOracle, available
     import numpy as np
 
     if not available(REF_CONFIG):
         return None
-    doc = np.frombuffer(W.json_doc(n_sample, seed), dtype=np.uint8)
+    if n_sample >= len(host):
+        doc = np.frombuffer(host, dtype=np.uint8)
+        what = "the timed %d MiB document itself" % (len(host) >> 20)
+    else:
+        doc = np.frombuffer(W.json_doc(n_sample, 2), dtype=np.uint8)
+        what = "one %d MiB document of the same generator (seed 2)" % (n_sample >> 20)
     ref = RefOracle(REF_CONFIG)
     ref.pipeline(doc[: 1 << 20])  # warm
     times = []
     ok = None
-    for _ in range(3):
+    for _ in range(reps):
         t0 = time.perf_counter()
         ok = ref.pipeline(doc)
         times.append(time.perf_counter() - t0)
-    t = min(times)
-    return {"value": n_sample / t / 1e9, "unit": "GB/s", "cores": 1, "kind": "reference",
-            "sample": "one %d MiB document of the same generator (seed %d), lex_string -> parse_test -> "
-                      "compute_parents -> compact_tree in memory, best of 3 (%.2fs), accepted=%s"
-                      % (n_sample >> 20, seed, t, ok[0])}
+    t = statistics.median(times)
+    return {"value": len(doc) / t / 1e9, "unit": "GB/s", "cores": 1, "kind": "reference",
+            "sample": "%s, lex_string -> parse_test -> compute_parents -> compact_tree in memory, median of %d "
+                      "runs (%.2fs each, %.1fs of CPU work), accepted=%s" % (what, reps, t, sum(times), ok[0])}
+
+
+def workload_config(n, world):
+    return {"workload": "json_ext %d MiB single JSON document per GPU" % (n >> 20), "grammar": "json_ext.alp",
+            "bytes": n, "index": "i32", "parallelism": "replicas x%d" % world,
+            "l2": "input larger than L2 (no flush)"}
 
 
 def reference_arm(a, rank, world):
@@ -168,8 +186,9 @@ def reference_arm(a, rank, world):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": 0, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": t / a.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-        "config": {"workload": "json_ext %d MiB documents, one per host core" % (sample >> 20),
-                   "grammar": "json_ext.alp", "index": "i32"},
+        "config": dict(workload_config(a.size, a.gpus),
+                       sample="each step: %d independent %d MiB documents of the same generator, one per host "
+                              "core (the reference backend parses one document on one thread)" % (cores, sample >> 20)),
         "cpu_baseline": {"value": value, "unit": "GB/s", "cores": cores, "kind": "reference",
                          "sample": "%d independent %d MiB JSON documents per step (one per core), reference C "
                                    "backend in memory; all accepted=%s" % (cores, sample >> 20, all(oks))},
@@ -288,10 +307,7 @@ def ours(a, rank, world, local_rank, dist):
         "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic (seeded JSON generator, one document per rank)",
-        "config": {"workload": "json_ext %d MiB single document (BASELINE config 2 shape)" % (n >> 20),
-                   "grammar": "json_ext.alp", "bytes": n, "index": "i32", "tokens": T, "nodes": N,
-                   "brackets": B, "productions": P, "parallelism": "replicas x%d" % world,
-                   "l2": "input larger than L2 (no flush)"},
+        "config": dict(workload_config(n, world), tokens=T, nodes=N, brackets=B, productions=P),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                      "algorithmic_bytes": kb, "ms": mean[dom]},
@@ -305,7 +321,7 @@ def ours(a, rank, world, local_rank, dist):
         "machine": info,
     }
     if not a.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sample(a.cpu_sample, 2)
+        line["cpu_baseline"] = cpu_baseline_sample(host, a.cpu_sample)
     print(json.dumps(line))
 
 
@@ -323,11 +339,11 @@ def committed_traffic(kernel: str):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=256 << 20)
-    ap.add_argument("--cpu-sample", type=int, default=64 << 20)
+    ap.add_argument("--cpu-sample", type=int, default=256 << 20)
     ap.add_argument("--ref-sample", type=int, default=16 << 20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     a = ap.parse_args()
