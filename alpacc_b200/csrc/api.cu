@@ -55,10 +55,12 @@ int upload_tables(alpacc_gpu_grammar *g) {
       trw[i >> 2] |= e << ((i & 3) * 8);
     }
   g->trans_word_count = (int)trw.size();
-  // copies of the byte-class and transition tables in shared memory: as many
-  // as keep a CTA's tables within ~40 KB, at most one per bank
+  // copies of the byte-class and transition tables in shared memory: more
+  // copies mean fewer bank conflicts on data-dependent lookups, but fewer
+  // resident CTAs; measured on json_ext, occupancy wins - keep a CTA's tables
+  // within ~12 KB
   int copies = 32;
-  while (copies > 1 && (size_t)copies * (trw.size() * 4 + 512) > 40 * 1024) copies >>= 1;
+  while (copies > 1 && (size_t)copies * (trw.size() * 4 + 512) > 12 * 1024) copies >>= 1;
   if (const char *e = getenv("ALPACC_LEX_COPIES")) {
     int v = atoi(e);
     if (v >= 1 && v <= 32 && (v & (v - 1)) == 0) copies = v;
@@ -248,21 +250,23 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
   const uint64_t B = g->h_status->num_brackets;
   const uint64_t P = g->h_status->num_productions;
 
-  // ---------------- depth walks ----------------
+  // ---------------- depth walks (the parent walk also writes the compacted tree) ----------------
   const uint64_t Emax = std::max<uint64_t>(std::max(B, P), 1);
   const uint64_t pse_tiles_max = (Emax + kPseTile - 1) / kPseTile;
   TRY(grow(g->pse_ticket, 16));
   TRY(grow(g->pse_flags, pse_tiles_max * 4));
   TRY(grow(g->pse_agg, pse_tiles_max * 16));
   TRY(grow(g->pse_inc, pse_tiles_max * 16));
-  TRY(grow(g->h, Emax * 4));
-  TRY(grow(g->answer, std::max<uint64_t>(P, 1) * 4));
-  TRY(grow(g->tinc, std::max<uint64_t>(P, 1) * 4));
+  TRY(grow(g->ch_h0, pse_tiles_max * kPseThreads * 4));
+  TRY(grow(g->ch_tc, pse_tiles_max * kPseThreads * 4));
   TRY(grow(g->tile_min, pse_tiles_max * 4));
   TRY(grow(g->chunk_min, pse_tiles_max * kPseThreads * 4));
   TRY(grow(g->super_min, ((pse_tiles_max >> kPseSuperShift) + 1) * 4));
   TRY(grow(g->queue, Emax * 8));
   TRY(grow(g->queue_len, 16));
+  TRY(grow(g->node_prods, std::max<uint64_t>(P, 1) * prod_w));
+  TRY(grow(g->node_parents, std::max<uint64_t>(P, 1) * idx_w));
+  TRY(grow(g->token_parents, std::max<uint64_t>(T, 1) * idx_w));
   for (int mode = 0; mode < 2; ++mode) {
     const uint64_t E = mode == kPseBrackets ? B : P;
     if (E == 0) continue;
@@ -275,18 +279,23 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     a.mode = mode;
     a.elems = (const uint32_t *)(mode == kPseBrackets ? g->br.p : g->pr.p);
     a.count = mode == kPseBrackets ? &g->d_status->num_brackets : &g->d_status->num_productions;
+    a.num_tokens = &g->d_status->num_tokens;
     a.num_tiles = tiles;
     a.arity = (const int32_t *)g->arity.p;
     a.is_term = (const uint8_t *)g->is_term.p;
-    a.h = (int32_t *)g->h.p;
-    a.answer = (int32_t *)g->answer.p;
-    a.tinc = (int32_t *)g->tinc.p;
+    a.ch_h0 = (int32_t *)g->ch_h0.p;
+    a.ch_min = (int32_t *)g->chunk_min.p;
+    a.ch_tc = (int32_t *)g->ch_tc.p;
     a.tile_min = (int32_t *)g->tile_min.p;
-    a.chunk_min = (int32_t *)g->chunk_min.p;
     a.super_min = (int32_t *)g->super_min.p;
     a.queue = (unsigned long long *)g->queue.p;
     a.queue_cap = Emax;
     a.queue_len = (unsigned long long *)g->queue_len.p;
+    a.node_prods = g->node_prods.p;
+    a.node_parents = g->node_parents.p;
+    a.token_parents = g->token_parents.p;
+    a.prod_w = prod_w;
+    a.idx_w = idx_w;
     a.ticket = (unsigned *)g->pse_ticket.p;
     a.st = PairTileState{(unsigned *)g->pse_flags.p, (unsigned long long *)g->pse_agg.p,
                          (unsigned long long *)g->pse_inc.p};
@@ -301,30 +310,6 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     CK(cudaGetLastError());
   }
   if (P == 0) CK(cudaMemsetAsync(&g->d_status->num_nodes, 0, 8, g->stream));
-
-  // ---------------- compaction ----------------
-  TRY(grow(g->node_prods, std::max<uint64_t>(P, 1) * prod_w));
-  TRY(grow(g->node_parents, std::max<uint64_t>(P, 1) * idx_w));
-  TRY(grow(g->token_parents, std::max<uint64_t>(T, 1) * idx_w));
-  if (P > 0) {
-    CompactArgs a{};
-    a.prods = (const uint32_t *)g->pr.p;
-    a.count = &g->d_status->num_productions;
-    a.num_tokens = &g->d_status->num_tokens;
-    a.parent = (const int32_t *)g->answer.p;
-    a.tinc = (const int32_t *)g->tinc.p;
-    a.is_term = (const uint8_t *)g->is_term.p;
-    a.node_prods = g->node_prods.p;
-    a.node_parents = g->node_parents.p;
-    a.token_parents = g->token_parents.p;
-    a.prod_w = prod_w;
-    a.idx_w = idx_w;
-    a.status = g->d_status;
-    stage_begin(g, 6);
-    compact_kernel<<<148 * 8, 256, 0, g->stream>>>(a);
-    stage_end(g, 6);
-    CK(cudaGetLastError());
-  }
   CK(cudaEventRecord(g->ev1, g->stream));
   int rc = sync_status(g);
   if (rc) return rc;
@@ -474,7 +459,7 @@ void alpacc_gpu_free(alpacc_gpu_grammar *g) {
                     &g->arity, &g->is_term, &g->in, &g->lex_ticket, &g->st1_flag, &g->st1_state, &g->st1_vec,
                     &g->st2_flags, &g->st2_agg, &g->st2_inc, &g->tok_ids, &g->tok_starts, &g->tok_lens,
                     &g->pair_ticket, &g->pst_flags, &g->pst_agg, &g->pst_inc, &g->br, &g->pr, &g->pse_ticket,
-                    &g->pse_flags, &g->pse_agg, &g->pse_inc, &g->h, &g->answer, &g->tinc, &g->tile_min,
+                    &g->pse_flags, &g->pse_agg, &g->pse_inc, &g->ch_h0, &g->ch_tc, &g->tile_min,
                     &g->chunk_min, &g->super_min, &g->queue, &g->queue_len, &g->node_prods, &g->node_parents,
                     &g->token_parents};
   for (DevBuf *b : bufs) release(*b);

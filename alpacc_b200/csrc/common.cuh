@@ -24,7 +24,9 @@ enum TimeoutSite : int {
   kSiteLexCount = 2,
   kSitePairs = 3,
   kSitePse = 4,
-  kSiteCompact = 5,
+  kSiteLexLanes = 5,   // a loop bound below was exceeded (internal error)
+  kSitePseQuery = 6,
+  kSiteLexTiles = 7,
 };
 
 struct DeviceStatus {
@@ -172,6 +174,40 @@ struct PairTileState {
 template <typename Op>
 __device__ __forceinline__ Pair64 combine(Pair64 x, Pair64 y, Op op) {
   return op(x, y);
+}
+
+// Exclusive block-wide scan of a pair carry (one pass instead of one per
+// component); `smem` needs (blockDim.x / 32) elements.
+template <typename Op>
+__device__ __forceinline__ Pair64 block_exclusive_scan_pair(Pair64 v, Op op, Pair64 identity, Pair64 *smem,
+                                                            Pair64 *total) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  Pair64 inc = v;
+#pragma unroll
+  for (int d = 1; d < kWarp; d <<= 1) {
+    const Pair64 o{__shfl_up_sync(0xffffffffu, inc.a, d), __shfl_up_sync(0xffffffffu, inc.b, d)};
+    if (lane >= d) inc = op(o, inc);
+  }
+  if (lane == kWarp - 1) smem[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    Pair64 w = lane < nwarps ? smem[lane] : identity;
+#pragma unroll
+    for (int d = 1; d < kWarp; d <<= 1) {
+      const Pair64 o{__shfl_up_sync(0xffffffffu, w.a, d), __shfl_up_sync(0xffffffffu, w.b, d)};
+      if (lane >= d) w = op(o, w);
+    }
+    if (lane < nwarps) smem[lane] = w;
+  }
+  __syncthreads();
+  const Pair64 warp_prefix = warp == 0 ? identity : smem[warp - 1];
+  Pair64 ex{__shfl_up_sync(0xffffffffu, inc.a, 1), __shfl_up_sync(0xffffffffu, inc.b, 1)};
+  if (lane == 0) ex = identity;
+  *total = smem[nwarps - 1];
+  __syncthreads();
+  return op(warp_prefix, ex);
 }
 
 __device__ __forceinline__ void publish_pair(PairTileState ts, long long tile, Pair64 v, bool inclusive) {

@@ -80,7 +80,7 @@ struct alpacc_gpu_grammar {
   DevBuf lex_ticket, st1_flag, st1_state, st1_vec, st2_flags, st2_agg, st2_inc;
   DevBuf tok_ids, tok_starts, tok_lens;
   DevBuf pair_ticket, pst_flags, pst_agg, pst_inc, br, pr;
-  DevBuf pse_ticket, pse_flags, pse_agg, pse_inc, h, answer, tinc, tile_min, chunk_min, super_min, queue, queue_len;
+  DevBuf pse_ticket, pse_flags, pse_agg, pse_inc, ch_h0, ch_tc, tile_min, chunk_min, super_min, queue, queue_len;
   DevBuf node_prods, node_parents, token_parents;
   // pinned host result buffers kept for reuse (released results come back here)
   void *pinned_cache = nullptr;

@@ -76,6 +76,10 @@ struct PairArgs {
 __global__ void pair_kernel(PairArgs args);
 
 // ---- previous-smaller search over depth walks: 256 threads x 8 elements ----
+// A chunk is one thread's 8 consecutive elements; per chunk the walk keeps the
+// depth before its first element, its minimum depth and (parents) the
+// terminal-production count before it, so that elements' depths and counts can
+// be recomputed from at most 7 neighbours instead of being stored.
 constexpr int kPseThreads = 256;
 constexpr int kPseItems = 8;
 constexpr int kPseTile = kPseThreads * kPseItems;
@@ -86,41 +90,29 @@ enum PseMode : int { kPseBrackets = 0, kPseParents = 1 };
 
 struct PseArgs {
   int mode;
-  const uint32_t *elems;          // brackets or productions
+  const uint32_t *elems;            // brackets (bit 31 = left) or productions
   const unsigned long long *count;  // device: number of elements
+  const unsigned long long *num_tokens;
   unsigned long long num_tiles;
-  const int32_t *arity;           // parents: per production
-  const uint8_t *is_term;         // parents: terminal production flags
-  int32_t *h;                     // [E] depth before each element
-  int32_t *answer;                // [E] matched / parent position (-1 pending)
-  int32_t *tinc;                  // parents: [E] inclusive terminal-production count
-  int32_t *tile_min;              // [tiles]
-  int32_t *chunk_min;             // [tiles * kPseThreads]
-  int32_t *super_min;             // [ceil(tiles / 256)] minimum over each run of 256 tiles
-  unsigned long long *queue;      // pending (element) indices
+  const int32_t *arity;             // parents: per production
+  const uint8_t *is_term;           // parents: terminal production flags
+  int32_t *ch_h0;                   // [tiles * 256] depth before each chunk
+  int32_t *ch_min;                  // [tiles * 256] minimum depth in each chunk (INT_MAX if empty)
+  int32_t *ch_tc;                   // parents: [tiles * 256] terminal productions before each chunk
+  int32_t *tile_min;                // [tiles]
+  int32_t *super_min;               // [ceil(tiles / 256)] minimum over each run of 256 tiles
+  unsigned long long *queue;        // elements whose answer lies in an earlier tile
   unsigned long long queue_cap;
-  unsigned long long *queue_len;  // device counter
+  unsigned long long *queue_len;    // device counter
+  // parents: the compacted tree (compact_tree), written as answers are found
+  void *node_prods, *node_parents, *token_parents;
+  int prod_w, idx_w;
   unsigned *ticket;
-  PairTileState st;               // (sum of steps, terminal count)
+  PairTileState st;                 // (sum of steps, terminal count)
   DeviceStatus *status;
 };
 
 __global__ void pse_tile_kernel(PseArgs args);
 __global__ void pse_resolve_kernel(PseArgs args);
-
-// ---- tree compaction (compact_tree) ----
-struct CompactArgs {
-  const uint32_t *prods;
-  const unsigned long long *count;   // P
-  const unsigned long long *num_tokens;
-  const int32_t *parent;
-  const int32_t *tinc;
-  const uint8_t *is_term;
-  void *node_prods, *node_parents, *token_parents;
-  int prod_w, idx_w;
-  DeviceStatus *status;
-};
-
-__global__ void compact_kernel(CompactArgs args);
 
 }  // namespace alpacc

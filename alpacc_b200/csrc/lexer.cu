@@ -60,10 +60,12 @@ struct LexSmem {
   uint8_t nbytes[kLexThreads];
   uint8_t start[kLexThreads];   // true start state of data chunks
   uint8_t cstate[kLexThreads];  // lane state just before the recorded part
+  uint8_t exact[kLexThreads];   // 1: lanes tracked per start state (lst/lrm valid)
   uint8_t sterm[256];           // per machine state: terminal id
   uint8_t sflags[256];          // bit1 accept, bit2 kept
   uint8_t cls_id[256];          // byte -> class id (first byte of a chunk)
   long long scan_tmp[kLexThreads / 32];
+  Pair64 pair_tmp[kLexThreads / 32];
   int kconst[kLexThreads];
   unsigned tile;
   int s_in;
@@ -90,11 +92,15 @@ __device__ __forceinline__ uint32_t entry(const Tabs &tb, uint32_t cp, uint32_t 
   return __byte_perm(w, 0, i & 3);
 }
 
-// f_t(x): the state after chunk t when it starts in state x.
+// f_t(x): the state after chunk t when it starts in state x. A chunk walked as
+// a state set is constant: every live start ends in its one state (a start
+// whose lane died instead is caught when the chunk is re-walked from its true
+// start, which then rejects the input).
 __device__ __forceinline__ int eval_chunk(const LexArgs &a, const LexSmem *sm, int t, int x) {
   if (sm->nbytes[t] == 0) return x;
   const int dead = a.dead;
   if (x == dead) return dead;
+  if (!sm->exact[t]) return sm->active[t] ? sm->lst[t] : dead;
   const int slot = __ldg(a.lane_of + (size_t)sm->c0[t] * a.M + x);
   if (slot == 0xff) return dead;
   const int r = sm->lrm[slot * kLexThreads + t];
@@ -139,7 +145,11 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
   const long long n = (long long)a.n;
   const unsigned long long num_tiles = a.num_tiles;
 
-  for (;;) {
+  for (unsigned long long round = 0;; ++round) {
+    if (round > num_tiles) {  // every round takes a new ticket: cannot happen
+      if (t == 0) record_timeout(st, kSiteLexTiles);
+      break;
+    }
     __syncthreads();  // tables ready / previous tile fully consumed
     if (t == 0) sm->tile = atomicAdd(a.ticket, 1u);
     __syncthreads();
@@ -171,53 +181,88 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
     sm->nbytes[t] = (uint8_t)nb;
     __syncthreads();
 
-    // ---- pass 1: lanes until they merge, then one lane recording boundaries ----
+    // ---- pass 1: the set of live states until it is a single state, then
+    // one lane recording boundaries ----
+    // The set walk (machines of at most 64 states) costs one lookup per live
+    // state per byte and merges equal states for free; it gives no per-start
+    // mapping, so a chunk whose set never shrinks to one state is walked again
+    // with lanes tracked per start state (slots in lst/lrm).
     uint8_t *tb8 = reinterpret_cast<uint8_t *>(sm->bytes) + t * kLexChunk;
     uint32_t active = 0;
     unsigned long long bmask = 0;
     int jconv = kNotConverged;
     {
       int c0 = 0;
+      bool exact = a.M > 64;
       if (nb > 0) {
         c0 = sm->cls_id[tb8[0]];
         const int cnt = __ldg(a.img_cnt + c0);
-        active = cnt ? ((1u << cnt) - 1u) : 0u;
-        for (int l = 0; l < cnt; l++) {
-          sm->lst[l * kLexThreads + t] = __ldg(a.img + c0 * kMaxLanes + l);
-          sm->lrm[l * kLexThreads + t] = (uint8_t)l;
-        }
+        int lconv = -1;
+        uint32_t s = 0;
         int j = 1;
-        while (j < nb && __popc(active) > 1) {
-          const uint32_t cp = cls_pre(tb, tb8[j]);
-          for (uint32_t m = active; m; m &= m - 1) {
-            const int l = __ffs(m) - 1;
-            const int s2 = (int)(entry(tb, cp, sm->lst[l * kLexThreads + t]) & 0x7f);
-            if (s2 == dead) active &= ~(1u << l);
-            else sm->lst[l * kLexThreads + t] = (uint8_t)s2;
+        if (!exact) {
+          const unsigned long long live = dead >= 0 ? ~(1ull << dead) : ~0ull;
+          unsigned long long set = 0;
+          for (int l = 0; l < cnt; l++) set |= 1ull << __ldg(a.img + c0 * kMaxLanes + l);
+          while (j < nb && __popcll(set) > 1) {
+            const uint32_t cp = cls_pre(tb, tb8[j]);
+            unsigned long long ns = 0;
+            for (unsigned long long m = set; m; m &= m - 1)
+              ns |= 1ull << (entry(tb, cp, (uint32_t)(__ffsll((long long)m) - 1)) & 0x7f);
+            set = ns & live;
+            ++j;
           }
-          if (__popc(active) > 1) {
-            for (uint32_t m1 = active; m1; m1 &= m1 - 1) {
-              const int l1 = __ffs(m1) - 1;
-              if (!((active >> l1) & 1)) continue;
-              const int s1 = sm->lst[l1 * kLexThreads + t];
-              for (uint32_t m2 = active & ~((2u << l1) - 1u); m2; m2 &= m2 - 1) {
-                const int l2 = __ffs(m2) - 1;
-                if (sm->lst[l2 * kLexThreads + t] == s1) {
-                  active &= ~(1u << l2);
-                  for (int k = 0; k < cnt; k++)
-                    if (sm->lrm[k * kLexThreads + t] == l2) sm->lrm[k * kLexThreads + t] = (uint8_t)l1;
+          if (__popcll(set) > 1) {
+            exact = true;
+          } else if (set) {
+            lconv = 0;
+            s = (uint32_t)(__ffsll((long long)set) - 1);
+            active = 1;
+          }  // else every lane died: active = 0, not converged
+        }
+        if (exact) {
+          active = cnt ? ((1u << cnt) - 1u) : 0u;
+          for (int l = 0; l < cnt; l++) {
+            sm->lst[l * kLexThreads + t] = __ldg(a.img + c0 * kMaxLanes + l);
+            sm->lrm[l * kLexThreads + t] = (uint8_t)l;
+          }
+          j = 1;
+          while (j < nb && __popc(active) > 1) {
+            const uint32_t cp = cls_pre(tb, tb8[j]);
+            for (uint32_t m = active; m; m &= m - 1) {
+              const int l = __ffs(m) - 1;
+              const int s2 = (int)(entry(tb, cp, sm->lst[l * kLexThreads + t]) & 0x7f);
+              if (s2 == dead) active &= ~(1u << l);
+              else sm->lst[l * kLexThreads + t] = (uint8_t)s2;
+            }
+            if (__popc(active) > 1) {
+              for (uint32_t m1 = active; m1; m1 &= m1 - 1) {
+                const int l1 = __ffs(m1) - 1;
+                if (!((active >> l1) & 1)) continue;
+                const int s1 = sm->lst[l1 * kLexThreads + t];
+                for (uint32_t m2 = active & ~((2u << l1) - 1u); m2; m2 &= m2 - 1) {
+                  const int l2 = __ffs(m2) - 1;
+                  if (sm->lst[l2 * kLexThreads + t] == s1) {
+                    active &= ~(1u << l2);
+                    for (int k = 0; k < cnt; k++)
+                      if (sm->lrm[k * kLexThreads + t] == l2) sm->lrm[k * kLexThreads + t] = (uint8_t)l1;
+                  }
                 }
               }
             }
+            ++j;
           }
-          ++j;
+          if (__popc(active) == 1) {
+            lconv = __ffs(active) - 1;
+            s = sm->lst[lconv * kLexThreads + t];
+          }
         }
-        if (__popc(active) == 1) {
-          const int l = __ffs(active) - 1;
-          uint32_t s = sm->lst[l * kLexThreads + t];
+        if (lconv >= 0) {
           jconv = j;
           sm->cstate[t] = (uint8_t)s;
-          // the hot loop: one class lookup and one transition per byte
+          // the hot loop: one class lookup and one transition per byte. The
+          // dead state is absorbing and never produces, so a lane that dies
+          // records nothing further and needs no test inside the loop.
 #pragma unroll 4
           for (; j < nb; ++j) {
             const uint32_t e = entry(tb, cls_pre(tb, tb8[j]), s);
@@ -226,14 +271,14 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
               tb8[j] = (uint8_t)s;  // state of the token ending before byte j
             }
             s = e & 0x7f;
-            if ((int)s == dead) break;
           }
           if ((int)s == dead) active = 0;
-          else sm->lst[l * kLexThreads + t] = (uint8_t)s;
+          else sm->lst[lconv * kLexThreads + t] = (uint8_t)s;
         }
       }
       sm->active[t] = (uint16_t)active;
       sm->c0[t] = (uint8_t)c0;
+      sm->exact[t] = exact ? 1 : 0;
       if (a.diag) {
         const unsigned w = __reduce_add_sync(0xffffffffu, (unsigned)(jconv == kNotConverged ? nb : jconv));
         if (lane == 0) atomicAdd(&st->scratch[3], (unsigned long long)w);
@@ -373,9 +418,10 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
       }
     }
     // ---- (count, last boundary) carry ----
-    long long cnt_tot, pos_tot;
-    const long long cnt_ex = block_exclusive_scan<long long>(cnt, AddI64(), 0ll, sm->scan_tmp, &cnt_tot);
-    const long long pos_ex = block_exclusive_scan<long long>(lastb, MaxI64(), 0ll, sm->scan_tmp, &pos_tot);
+    Pair64 cp_tot;
+    const Pair64 cp_ex = block_exclusive_scan_pair(Pair64{cnt, lastb}, CntPosOp(), Pair64{0, 0}, sm->pair_tmp, &cp_tot);
+    const long long cnt_ex = cp_ex.a, pos_ex = cp_ex.b;
+    const long long cnt_tot = cp_tot.a, pos_tot = cp_tot.b;
     if (t < kWarp) {
       const Pair64 agg{cnt_tot, pos_tot};
       Pair64 prefix{0, 0};

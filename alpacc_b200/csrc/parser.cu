@@ -8,13 +8,12 @@
 // pse_tile_kernel depth walk over brackets (+1 left, -1 right) or productions
 //                 (+arity-1), with the match of each right bracket / the parent
 //                 of each production found as the previous element whose depth
-//                 is <= a query value: inside a thread's 8 elements, then in
-//                 earlier chunks of the tile via a sparse table of chunk
-//                 minima; the rest is queued (parser.c:74-87,103-118).
+//                 is <= a query value, inside the tile; parents found are
+//                 written straight into the compacted tree (compact_tree); the
+//                 rest is queued (parser.c:74-87,103-118,126-153).
 // pse_resolve     queued queries walk back over tile minima, then chunk
-//                 minima, then elements of the tile that holds the answer.
-// compact_kernel  drops terminal productions, remaps parents and writes
-//                 token_parents (parser.c:126-153).
+//                 minima, then the elements of one chunk, and emit the same
+//                 outputs.
 #include <climits>
 #include <cstdint>
 
@@ -53,10 +52,19 @@ struct AddPair {
 // Pair lookup and expansion
 // ---------------------------------------------------------------------------
 
+// The tile's terminals (with the q before and k - 1 after it) are staged in
+// shared memory once; keys are formed there with positions strided across the
+// threads (conflict-free), the per-position counts are scanned in blocked
+// order (one packed 64-bit scan of (brackets, productions)), and each thread
+// then writes the stack actions and productions of its 8 consecutive
+// positions.
 __global__ void __launch_bounds__(kPairThreads) pair_kernel(PairArgs a) {
   __shared__ unsigned s_tile;
   __shared__ long long s_tmp[kPairThreads / 32];
   __shared__ long long s_prefix_b, s_prefix_p;
+  __shared__ uint16_t s_term[kPairTile + 8];             // window of terminals; 0xffff = out of range
+  __shared__ __align__(16) uint32_t s_rec[kPairTile];    // record per position
+  __shared__ __align__(16) uint16_t s_cnt[kPairTile];    // brackets | productions << 8
   const int t = threadIdx.x;
   DeviceStatus *st = a.status;
   if (t == 0) s_tile = atomicAdd(a.ticket, 1u);
@@ -68,37 +76,59 @@ __global__ void __launch_bounds__(kPairThreads) pair_kernel(PairArgs a) {
   if (tile0 >= m) return;  // beyond the data: nobody waits on this tile
   const int L = a.q + a.k;
 
-  uint32_t rec[kPairItems];
-  long long sb = 0, sp = 0;
+  // ---- terminals of positions tile0 - q .. tile0 + kPairTile + k - 2 ----
+  for (int i = t; i < kPairTile + L - 1; i += kPairThreads) {
+    const long long pos = tile0 - a.q + i;
+    int term;
+    if (pos < 0 || pos >= m) term = a.empty_t;
+    else if (pos == 0) term = a.start_t;
+    else if (pos == m - 1) term = a.end_t;
+    else term = (int)load_uint(a.tok_ids, (unsigned long long)(pos - 1), a.term_w);
+    s_term[i] = (unsigned)term < (unsigned)a.nt ? (uint16_t)term : (uint16_t)0xffff;
+  }
+  __syncthreads();
+
+  // ---- keys and records, positions strided over the threads ----
   bool missing = false;
 #pragma unroll
   for (int j = 0; j < kPairItems; ++j) {
-    const long long i = tile0 + (long long)t * kPairItems + j;
-    rec[j] = 0xffffffffu;
-    if (i >= m) continue;
-    unsigned long long d = 0;
-    for (int x = 0; x < L; ++x) {
-      const long long pos = i - a.q + x;
-      int term;
-      if (pos < 0 || pos >= m) term = a.empty_t;
-      else if (pos == 0) term = a.start_t;
-      else if (pos == m - 1) term = a.end_t;
-      else term = (int)load_uint(a.tok_ids, (unsigned long long)(pos - 1), a.term_w);
-      d = d * (unsigned long long)a.nt + (unsigned long long)term;
+    const int li = j * kPairThreads + t;
+    uint32_t r = 0xffffffffu;
+    uint16_t c = 0;
+    if (tile0 + li < m) {
+      unsigned long long d = 0;
+      bool bad = false;
+      for (int x = 0; x < L; ++x) {
+        const unsigned term = s_term[li + x];
+        bad |= term == 0xffffu;  // keeps the table index in bounds
+        d = d * (unsigned long long)a.nt + term;
+      }
+      r = bad ? 0xffffffffu : __ldg(a.dense + d);
+      if (r == 0xffffffffu) missing = true;
+      else c = (uint16_t)(__ldg(a.rec_nb + r) | (__ldg(a.rec_np + r) << 8));
     }
-    const uint32_t r = __ldg(a.dense + d);
-    rec[j] = r;
-    if (r == 0xffffffffu) {
-      missing = true;
-      continue;
-    }
-    sb += __ldg(a.rec_nb + r);
-    sp += __ldg(a.rec_np + r);
+    s_rec[li] = r;
+    s_cnt[li] = c;
   }
   if (missing) record_reject(st, &st->parse_reject_reason, 1);
-  long long tb, tp;
-  const long long eb = block_exclusive_scan<long long>(sb, AddI64(), 0ll, s_tmp, &tb);
-  const long long ep = block_exclusive_scan<long long>(sp, AddI64(), 0ll, s_tmp, &tp);
+  __syncthreads();
+
+  // ---- blocked counts: thread t owns positions t*8 .. t*8+7 ----
+  uint16_t cnt[kPairItems];
+  {
+    const uint4 cv = reinterpret_cast<const uint4 *>(s_cnt)[t];
+    cnt[0] = cv.x & 0xffff; cnt[1] = cv.x >> 16; cnt[2] = cv.y & 0xffff; cnt[3] = cv.y >> 16;
+    cnt[4] = cv.z & 0xffff; cnt[5] = cv.z >> 16; cnt[6] = cv.w & 0xffff; cnt[7] = cv.w >> 16;
+  }
+  long long sb = 0, sp = 0;
+#pragma unroll
+  for (int j = 0; j < kPairItems; ++j) {
+    sb += cnt[j] & 0xff;
+    sp += cnt[j] >> 8;
+  }
+  long long tot;
+  const long long ex = block_exclusive_scan<long long>((sb << 32) + sp, AddI64(), 0ll, s_tmp, &tot);
+  const long long tb = tot >> 32, tp = tot & 0xffffffffll;
   if (t < kWarp) {
     const Pair64 agg{tb, tp};
     Pair64 prefix{0, 0};
@@ -118,19 +148,19 @@ __global__ void __launch_bounds__(kPairThreads) pair_kernel(PairArgs a) {
     }
   }
   __syncthreads();
-  unsigned long long ob = (unsigned long long)(s_prefix_b + eb);
-  unsigned long long op = (unsigned long long)(s_prefix_p + ep);
+  unsigned long long ob = (unsigned long long)(s_prefix_b + (ex >> 32));
+  unsigned long long op = (unsigned long long)(s_prefix_p + (ex & 0xffffffffll));
   bool overflow = false;
 #pragma unroll
   for (int j = 0; j < kPairItems; ++j) {
-    const uint32_t r = rec[j];
+    const uint32_t r = s_rec[t * kPairItems + j];
     if (r == 0xffffffffu) continue;
-    const int nb = __ldg(a.rec_nb + r), np = __ldg(a.rec_np + r);
-    const uint32_t ss = __ldg(a.rec_ss + r), ps = __ldg(a.rec_ps + r);
+    const int nb = cnt[j] & 0xff, np = cnt[j] >> 8;
     if (ob + nb > a.br_cap || op + np > a.pr_cap) {
       overflow = true;
       break;
     }
+    const uint32_t ss = __ldg(a.rec_ss + r), ps = __ldg(a.rec_ps + r);
     for (int x = 0; x < nb; ++x) a.br_out[ob + x] = __ldg(a.stacks + ss + x);
     for (int x = 0; x < np; ++x) a.pr_out[op + x] = __ldg(a.prods + ps + x);
     ob += nb;
@@ -146,29 +176,55 @@ __global__ void __launch_bounds__(kPairThreads) pair_kernel(PairArgs a) {
 namespace {
 
 constexpr int kPseStride = kPseItems + 1;  // odd word stride: conflict-free per-thread rows
+constexpr int kPseWarps = kPseThreads / kWarp;
+constexpr long long kPack = 1ll << 32;     // (step sum, terminal count) packed in one scan value
 
 struct PseSmem {
-  int32_t h[kPseThreads * kPseStride];
   uint32_t v[kPseThreads * kPseStride];
-  int32_t lv[8][kPseThreads];   // lv[l][i] = min of chunk minima (i-2^l, i]
-  int32_t pm[kPseThreads];      // prefix minimum of chunk minima
-  long long tmp[kPseThreads / 32];
+  int32_t h[kPseThreads * kPseStride];   // depth before each element, relative to the tile start
+  int32_t tc[kPseThreads * kPseStride];  // parents: inclusive terminal count, relative to the tile start
+  int32_t lv[5][kPseThreads];            // lv[k][i]: minimum of chunk minima over (i - 2^k, i] within i's warp
+  int32_t wmin[kPseWarps];               // minimum of each warp's chunk minima
+  long long tmp[kPseWarps];
   long long prefix_a, prefix_b;
-  unsigned long long qbase;
 };
 
-// step of an element and whether it carries a query
 __device__ __forceinline__ int pse_step(const PseArgs &a, uint32_t v) {
   if (a.mode == kPseBrackets) return (v >> 31) ? 1 : -1;
   return __ldg(a.arity + v) - 1;
 }
 
+// compact_tree's output for production e (parser.c:126-153): terminal
+// productions give their token's parent, the others a tree node; parents are
+// renumbered by subtracting the terminal productions before them.
+__device__ __forceinline__ void emit_node(const PseArgs &a, uint32_t prod, long long e, long long tinc_e,
+                                          long long p_new, long long T) {
+  if (__ldg(a.is_term + prod)) {
+    if (tinc_e >= 1 && tinc_e <= T)
+      store_uint(a.token_parents, (unsigned long long)(tinc_e - 1), a.idx_w, (unsigned long long)p_new);
+  } else {
+    const long long o = e - tinc_e;
+    if (o >= 0) {
+      store_uint(a.node_prods, (unsigned long long)o, a.prod_w, prod);
+      store_uint(a.node_parents, (unsigned long long)o, a.idx_w, (unsigned long long)p_new);
+    }
+  }
+}
+
 }  // namespace
 
+// One tile of 2048 elements: depth walk, then each query (a right bracket's
+// match, a production's parent) searched as the latest earlier element whose
+// depth is <= the query value - first in the thread's own chunk, then in
+// earlier chunks of the warp (binary descent over shuffled window minima),
+// then in earlier warps; what the tile cannot answer is queued. Parents found
+// here are emitted straight into the compacted tree.
 __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   __shared__ unsigned s_tile;
   __shared__ PseSmem sm;
   const int t = threadIdx.x;
+  const int lane = t & (kWarp - 1);
+  const int warp = t >> 5;
   DeviceStatus *st = a.status;
   if (t == 0) s_tile = atomicAdd(a.ticket, 1u);
   __syncthreads();
@@ -177,116 +233,168 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   const long long tile0 = (long long)tile * kPseTile;
   if (tile0 >= E) return;
   const bool parents = a.mode == kPseParents;
+  const long long c0 = tile0 + (long long)t * kPseItems;  // first element of this thread's chunk
 
-  // ---- load, local steps ----
-  int rel[kPseItems];
-  int loc_term[kPseItems];
-  long long ssum = 0, tsum = 0;
+  // ---- load ----
+  uint32_t v[kPseItems];
+  if (c0 + kPseItems <= E) {
+    const uint4 x0 = __ldg(reinterpret_cast<const uint4 *>(a.elems + c0));
+    const uint4 x1 = __ldg(reinterpret_cast<const uint4 *>(a.elems + c0) + 1);
+    v[0] = x0.x; v[1] = x0.y; v[2] = x0.z; v[3] = x0.w;
+    v[4] = x1.x; v[5] = x1.y; v[6] = x1.z; v[7] = x1.w;
+  } else {
+#pragma unroll
+    for (int j = 0; j < kPseItems; ++j) v[j] = c0 + j < E ? a.elems[c0 + j] : 0u;
+  }
+
+  // ---- local steps, one packed scan ----
+  int hr[kPseItems], tcr[kPseItems];
+  int ssum = 0, tsum = 0;
 #pragma unroll
   for (int j = 0; j < kPseItems; ++j) {
-    const long long e = tile0 + (long long)t * kPseItems + j;
-    uint32_t v = 0;
-    int stp = 0, tm = 0;
-    if (e < E) {
-      v = a.elems[e];
-      stp = pse_step(a, v);
-      if (parents) tm = __ldg(a.is_term + v) ? 1 : 0;
+    hr[j] = ssum;
+    if (c0 + j < E) {
+      ssum += pse_step(a, v[j]);
+      if (parents) tsum += __ldg(a.is_term + v[j]) ? 1 : 0;
     }
-    sm.v[t * kPseStride + j] = v;
-    rel[j] = (int)ssum;
-    ssum += stp;
-    tsum += tm;
-    loc_term[j] = (int)tsum;
+    tcr[j] = tsum;
   }
-  long long tot_s, tot_t;
-  const long long ex_s = block_exclusive_scan<long long>(ssum, AddI64(), 0ll, sm.tmp, &tot_s);
-  const long long ex_t = block_exclusive_scan<long long>(tsum, AddI64(), 0ll, sm.tmp, &tot_t);
-  // Publish the aggregate at once, so that later tiles' look-back can pass
-  // this tile while it is still searching; tile 0's aggregate is its
-  // inclusive prefix.
+  long long tot;
+  const long long ex = block_exclusive_scan<long long>((long long)ssum * kPack + tsum, AddI64(), 0ll, sm.tmp, &tot);
+  const int ex_t = (int)(ex & 0xffffffffll);
+  const int ex_s = (int)((ex - ex_t) >> 32);
+  const long long tot_t = tot & 0xffffffffll;
+  const long long tot_s = (tot - tot_t) >> 32;
+  // publish the aggregate at once; tile 0's aggregate is its inclusive prefix
   if (t == 0) publish_pair(a.st, (long long)tile, Pair64{tot_s, tot_t}, tile == 0);
 
-  // ---- depths relative to the tile start, chunk minima ----
-  // The search compares depths only with each other, so it runs on relative
-  // depths; the tile's offset is added when the results are written.
+  // ---- relative depths, chunk minimum, warp windows ----
   int cmin = INT_MAX;
 #pragma unroll
   for (int j = 0; j < kPseItems; ++j) {
-    const long long e = tile0 + (long long)t * kPseItems + j;
-    const int32_t h = (int32_t)(ex_s + rel[j]);
-    sm.h[t * kPseStride + j] = h;
-    if (e < E && h < cmin) cmin = h;
+    hr[j] += ex_s;
+    if (c0 + j < E && hr[j] < cmin) cmin = hr[j];
+    sm.v[t * kPseStride + j] = v[j];
+    sm.h[t * kPseStride + j] = hr[j];
+    if (parents) sm.tc[t * kPseStride + j] = ex_t + tcr[j];
   }
-  sm.lv[0][t] = cmin;
-  __syncthreads();
-  for (int l = 1; l < 8; ++l) {
-    const int w = 1 << (l - 1);
-    int v = sm.lv[l - 1][t];
-    if (t >= w) {
-      const int o = sm.lv[l - 1][t - w];
-      v = o < v ? o : v;
-    }
-    sm.lv[l][t] = v;
-    __syncthreads();
+  int L[6];
+  L[0] = cmin;
+#pragma unroll
+  for (int k = 1; k < 6; ++k) {
+    const int o = __shfl_up_sync(0xffffffffu, L[k - 1], 1 << (k - 1));
+    L[k] = (lane >= (1 << (k - 1)) && o < L[k - 1]) ? o : L[k - 1];
   }
-  sm.pm[t] = sm.lv[7][t];  // covers (t-128, t]; complete with a second window below
-  __syncthreads();
-  if (t >= 128) {
-    const int o = sm.lv[7][t - 128];
-    if (o < sm.pm[t]) sm.pm[t] = o;
-  }
+#pragma unroll
+  for (int k = 0; k < 5; ++k) sm.lv[k][t] = L[k];
+  if (lane == kWarp - 1) sm.wmin[warp] = L[5];
   __syncthreads();
 
-  // ---- queries inside the tile ----
-  int pending = 0;
-  int32_t ans[kPseItems];
+  // ---- queries: own chunk ----
+  // ans: local index of the answer; -1 pending; -2 no query; -3 the root
+  int ans[kPseItems];
+  unsigned need = 0;
 #pragma unroll
   for (int j = 0; j < kPseItems; ++j) {
-    ans[j] = INT_MIN;  // INT_MIN: no query
-    const long long e = tile0 + (long long)t * kPseItems + j;
+    ans[j] = -2;
+    const long long e = c0 + j;
     if (e >= E) continue;
-    const uint32_t v = sm.v[t * kPseStride + j];
-    const int32_t h = sm.h[t * kPseStride + j];
-    int32_t qv;
+    int qv;
     if (parents) {
       if (e == 0) {
-        ans[j] = 0;
+        ans[j] = -3;
         continue;
       }
-      qv = h;
+      qv = hr[j];
     } else {
-      if (v >> 31) continue;  // left bracket: no query
-      qv = h - 1;
+      if (v[j] >> 31) continue;  // left bracket: no query
+      qv = hr[j] - 1;
     }
-    int32_t found = -1;
-    for (int jj = j - 1; jj >= 0; --jj)
-      if (sm.h[t * kPseStride + jj] <= qv) {
-        found = t * kPseItems + jj;
-        break;
+    int f = -1;
+    uint32_t pv = 0;
+#pragma unroll
+    for (int jj = 0; jj < j; ++jj)
+      if (hr[jj] <= qv) {
+        f = jj;
+        pv = v[jj];
       }
-    if (found < 0 && t > 0 && sm.pm[t - 1] <= qv) {
-      int pos = t - 1;
-      for (int l = 7; l >= 0; --l)
-        if (pos - (1 << l) + 1 >= 0 && sm.lv[l][pos] > qv) pos -= 1 << l;
-      for (int jj = kPseItems - 1; jj >= 0; --jj)
-        if (sm.h[pos * kPseStride + jj] <= qv) {
-          found = pos * kPseItems + jj;
-          break;
-        }
-    }
-    if (found >= 0) {
-      if (!parents) {
-        const uint32_t pv = sm.v[(found / kPseItems) * kPseStride + found % kPseItems];
-        if ((pv & 0x7fffffffu) != (v & 0x7fffffffu)) record_reject(st, &st->parse_reject_reason, 2);
-      }
-      ans[j] = (int32_t)(tile0 + found);
+    if (f >= 0) {
+      ans[j] = t * kPseItems + f;
+      if (!parents && ((pv ^ v[j]) & 0x7fffffffu)) record_reject(st, &st->parse_reject_reason, 2);
     } else {
       ans[j] = -1;
-      ++pending;
+      need |= 1u << j;
     }
   }
-  long long tot_p;
-  const long long ex_p = block_exclusive_scan<long long>(pending, AddI64(), 0ll, sm.tmp, &tot_p);
+  // ---- earlier chunks of the tile: one query per lane per round ----
+  for (int guard = 0; __any_sync(0xffffffffu, need != 0u); ++guard) {
+    if (guard > kPseItems) {  // one item per round: cannot happen
+      if (lane == 0) record_timeout(st, kSitePseQuery);
+      break;
+    }
+    const bool act = need != 0u;
+    const int j = act ? __ffs(need) - 1 : 0;
+    const int qv = act ? sm.h[t * kPseStride + j] - (parents ? 0 : 1) : INT_MIN;
+    int pos = lane > 0 ? lane - 1 : 0;
+    const int pm = __shfl_sync(0xffffffffu, L[5], pos);  // prefix minimum of the warp up to pos
+    const bool inwarp = act && lane > 0 && pm <= qv;
+#pragma unroll
+    for (int k = 4; k >= 0; --k) {
+      const int w = __shfl_sync(0xffffffffu, L[k], pos);
+      if (inwarp && w > qv && pos >= (1 << k)) pos -= 1 << k;
+    }
+    int found = -1;
+    if (inwarp) {
+      const int pl = warp * kWarp + pos;
+#pragma unroll
+      for (int jj = kPseItems - 1; jj >= 0; --jj)
+        if (found < 0 && sm.h[pl * kPseStride + jj] <= qv) found = pl * kPseItems + jj;
+    } else if (act) {
+      for (int w = warp - 1; w >= 0 && found < 0; --w) {
+        if (sm.wmin[w] > qv) continue;
+        int p = w * kWarp + kWarp - 1;
+#pragma unroll
+        for (int k = 4; k >= 0; --k)
+          if (sm.lv[k][p] > qv && p - (1 << k) >= w * kWarp) p -= 1 << k;
+#pragma unroll
+        for (int jj = kPseItems - 1; jj >= 0; --jj)
+          if (found < 0 && sm.h[p * kPseStride + jj] <= qv) found = p * kPseItems + jj;
+      }
+    }
+    if (act) {
+      if (found >= 0) {
+        if (!parents) {
+          const uint32_t pv = sm.v[(found / kPseItems) * kPseStride + found % kPseItems];
+          if ((pv & 0x7fffffffu) != (sm.v[t * kPseStride + j] & 0x7fffffffu))
+            record_reject(st, &st->parse_reject_reason, 2);
+        }
+#pragma unroll
+        for (int jj = 0; jj < kPseItems; ++jj)
+          if (jj == j) ans[jj] = found;
+      }
+      need &= need - 1u;
+    }
+  }
+  // ---- queue what the tile could not answer (warp-aggregated) ----
+  {
+    int pending = 0;
+#pragma unroll
+    for (int j = 0; j < kPseItems; ++j) pending += ans[j] == -1 ? 1 : 0;
+    if (__any_sync(0xffffffffu, pending != 0)) {
+      const int incl = warp_inclusive_scan(pending, [](int x, int y) { return x + y; });
+      unsigned long long base = 0;
+      if (lane == kWarp - 1) base = atomicAdd(a.queue_len, (unsigned long long)incl);
+      base = __shfl_sync(0xffffffffu, base, kWarp - 1);
+      unsigned long long qi = base + (unsigned long long)(incl - pending);
+#pragma unroll
+      for (int j = 0; j < kPseItems; ++j)
+        if (ans[j] == -1) {
+          if (qi < a.queue_cap) a.queue[qi] = (unsigned long long)(c0 + j);
+          else atomicCAS(&st->error, 0, -4 /* ALPACC_E_CAPACITY */);
+          ++qi;
+        }
+    }
+  }
 
   // ---- the tile's prefix: look-back by warp 0, now that predecessors had time ----
   if (t < kWarp) {
@@ -297,12 +405,11 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
       if (tile > 0) publish_pair(a.st, (long long)tile, inc, true);
       sm.prefix_a = prefix.a;
       sm.prefix_b = prefix.b;
-      if (tot_p > 0) sm.qbase = atomicAdd(a.queue_len, (unsigned long long)tot_p);
       if (tile0 + kPseTile >= E) {  // last tile: global checks
         if (!parents) {
           if (inc.a != 0) record_reject(st, &st->parse_reject_reason, 3);
         } else {
-          const long long T = (long long)st->num_tokens;
+          const long long T = (long long)*a.num_tokens;
           if (inc.b != T) record_reject(st, &st->parse_reject_reason, 4);
           st->num_nodes = (unsigned long long)(E - inc.b);
         }
@@ -311,33 +418,33 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   }
   __syncthreads();
 
-  // ---- absolute depths, minima, terminal counts, answers, queue ----
+  // ---- chunk state, tile minimum, tree nodes ----
   const int32_t off = (int32_t)((parents ? 1 : 0) + sm.prefix_a);
-#pragma unroll
-  for (int j = 0; j < kPseItems; ++j) {
-    const long long e = tile0 + (long long)t * kPseItems + j;
-    if (e < E) {
-      a.h[e] = sm.h[t * kPseStride + j] + off;
-      if (parents) a.tinc[e] = (int32_t)(sm.prefix_b + ex_t + loc_term[j]);
-    }
-  }
-  a.chunk_min[tile * kPseThreads + t] = cmin == INT_MAX ? INT_MAX : cmin + off;
+  const long long pb = sm.prefix_b;
+  const unsigned long long ci = tile * kPseThreads + t;
+  a.ch_h0[ci] = off + ex_s;
+  a.ch_min[ci] = cmin == INT_MAX ? INT_MAX : cmin + off;
+  if (parents) a.ch_tc[ci] = (int32_t)(pb + ex_t);
   if (t == 0) {
-    const int32_t r = sm.lv[7][kPseThreads - 1] < sm.lv[7][127] ? sm.lv[7][kPseThreads - 1] : sm.lv[7][127];
+    int32_t r = sm.wmin[0];
+#pragma unroll
+    for (int w = 1; w < kPseWarps; ++w) r = sm.wmin[w] < r ? sm.wmin[w] : r;
     const int32_t tm = r + off;  // the tile holds at least one element
     a.tile_min[tile] = tm;
     atomicMin(a.super_min + (tile >> kPseSuperShift), tm);
   }
-  unsigned long long qi = sm.qbase + (unsigned long long)ex_p;
+  if (parents) {
+    const long long T = (long long)*a.num_tokens;
 #pragma unroll
-  for (int j = 0; j < kPseItems; ++j) {
-    const long long e = tile0 + (long long)t * kPseItems + j;
-    if (e >= E || ans[j] == INT_MIN) continue;
-    if (parents) a.answer[e] = ans[j];
-    if (ans[j] == -1) {
-      if (qi < a.queue_cap) a.queue[qi] = (unsigned long long)e;
-      else atomicCAS(&st->error, 0, -4 /* ALPACC_E_CAPACITY */);
-      ++qi;
+    for (int j = 0; j < kPseItems; ++j) {
+      const int an = ans[j];
+      if (an == -3) {  // the root: compute_parents gives it parent 0
+        emit_node(a, v[j], c0 + j, pb + ex_t + tcr[j], 0 - (pb + sm.tc[0]), T);
+      } else if (an >= 0) {
+        const long long p = tile0 + an;
+        const long long tinc_p = pb + sm.tc[(an / kPseItems) * kPseStride + an % kPseItems];
+        emit_node(a, v[j], c0 + j, pb + ex_t + tcr[j], p - tinc_p, T);
+      }
     }
   }
 }
@@ -357,11 +464,36 @@ __device__ __forceinline__ long long warp_latest_le(const int32_t *arr, long lon
   return -1;
 }
 
+// Depth before each element of chunk c, for lanes 0..7 (lane l: element
+// c * 8 + l); other lanes and elements past the end get INT_MAX.
+__device__ __forceinline__ int32_t chunk_depth(const PseArgs &a, long long c, long long E, int lane) {
+  const long long e = c * kPseItems + lane;
+  const bool ok = lane < kPseItems && e < E;
+  int stp = ok ? pse_step(a, a.elems[e]) : 0;
+  const int32_t h0 = a.ch_h0[c];
+#pragma unroll
+  for (int d = 1; d < kPseItems; d <<= 1) {
+    const int o = __shfl_up_sync(0xffffffffu, stp, d);
+    if (lane >= d) stp += o;
+  }
+  const int excl = __shfl_up_sync(0xffffffffu, stp, 1);
+  return ok ? h0 + (lane > 0 ? excl : 0) : INT_MAX;
+}
+
+// Inclusive terminal-production count up to element x (warp-wide call).
+__device__ __forceinline__ long long terminal_count(const PseArgs &a, long long x, int lane) {
+  const long long c = x / kPseItems;
+  const long long e = c * kPseItems + lane;
+  const bool t = lane <= (int)(x - c * kPseItems) && __ldg(a.is_term + a.elems[e < x ? e : x]);
+  return (long long)a.ch_tc[c] + __popc(__ballot_sync(0xffffffffu, t));
+}
+
 }  // namespace
 
 // One warp per queued query: latest tile whose minimum is <= the query
 // (within the query's super-tile of 256 tiles, else via super-tile minima),
-// then the latest chunk of that tile, then the latest element of that chunk.
+// then the latest chunk of that tile, then the latest element of that chunk
+// (depths recomputed from the chunk's start depth).
 __global__ void pse_resolve_kernel(PseArgs a) {
   DeviceStatus *st = a.status;
   const unsigned long long qn = *a.queue_len;
@@ -373,8 +505,9 @@ __global__ void pse_resolve_kernel(PseArgs a) {
   for (unsigned long long qi = warp; qi < qn && qi < a.queue_cap; qi += warps) {
     const long long e = (long long)a.queue[qi];
     const uint32_t v = a.elems[e];
-    const int32_t h = a.h[e];
-    const int32_t qv = parents ? h : h - 1;
+    const long long ce = e / kPseItems;
+    const int32_t he = __shfl_sync(0xffffffffu, chunk_depth(a, ce, E, lane), (int)(e - ce * kPseItems));
+    const int32_t qv = parents ? he : he - 1;
     const long long tile = e / kPseTile;
     const long long sup0 = (tile >> kPseSuperShift) << kPseSuperShift;
     long long tt = warp_latest_le(a.tile_min, tile - 1, sup0, qv, lane);
@@ -384,48 +517,22 @@ __global__ void pse_resolve_kernel(PseArgs a) {
     }
     long long found = -1;
     if (tt >= 0) {
-      const long long c = warp_latest_le(a.chunk_min + tt * kPseThreads, kPseThreads - 1, 0, qv, lane);
+      const long long c = warp_latest_le(a.ch_min + tt * kPseThreads, kPseThreads - 1, 0, qv, lane);
       if (c >= 0) {
-        const long long base = tt * kPseTile + c * kPseItems;
-        const long long hi = base + kPseItems - 1 < E - 1 ? base + kPseItems - 1 : E - 1;
-        found = warp_latest_le(a.h, hi, base, qv, lane);
+        const long long cc = tt * kPseThreads + c;
+        const unsigned b = __ballot_sync(0xffffffffu, chunk_depth(a, cc, E, lane) <= qv);
+        if (b) found = cc * kPseItems + (31 - __clz(b));
       }
     }
-    if (lane == 0) {
-      if (parents) {
-        // compute_parents takes 0 when its stack is empty
-        a.answer[e] = found >= 0 ? (int32_t)found : 0;
-      } else {
-        if (found < 0) record_reject(st, &st->parse_reject_reason, 3);
-        else if ((a.elems[found] & 0x7fffffffu) != (v & 0x7fffffffu)) record_reject(st, &st->parse_reject_reason, 2);
-      }
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Compaction (compact_tree)
-// ---------------------------------------------------------------------------
-
-__global__ void compact_kernel(CompactArgs a) {
-  const unsigned long long P = *a.count;
-  const long long T = (long long)*a.num_tokens;
-  for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; e < P;
-       e += (unsigned long long)gridDim.x * blockDim.x) {
-    const uint32_t prod = a.prods[e];
-    long long p = e == 0 ? 0 : a.parent[e];
-    if (p < 0 || (unsigned long long)p >= P) p = 0;  // only after a recorded reject or error
-    const long long p_new = p - (long long)a.tinc[p];
-    const long long ti = a.tinc[e];
-    if (__ldg(a.is_term + prod)) {
-      if (ti >= 1 && ti <= T)
-        store_uint(a.token_parents, (unsigned long long)(ti - 1), a.idx_w, (unsigned long long)p_new);
-    } else {
-      const long long o = (long long)e - ti;
-      if (o >= 0) {
-        store_uint(a.node_prods, (unsigned long long)o, a.prod_w, prod);
-        store_uint(a.node_parents, (unsigned long long)o, a.idx_w, (unsigned long long)p_new);
-      }
+    if (parents) {
+      // compute_parents takes 0 when its stack is empty
+      const long long p = found >= 0 ? found : 0;
+      const long long tinc_p = terminal_count(a, p, lane);
+      const long long tinc_e = terminal_count(a, e, lane);
+      if (lane == 0) emit_node(a, v, e, tinc_e, p - tinc_p, (long long)*a.num_tokens);
+    } else if (lane == 0) {
+      if (found < 0) record_reject(st, &st->parse_reject_reason, 3);
+      else if ((a.elems[found] & 0x7fffffffu) != (v & 0x7fffffffu)) record_reject(st, &st->parse_reject_reason, 2);
     }
   }
 }

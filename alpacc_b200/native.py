@@ -282,7 +282,7 @@ class Parser:
     def last_ms(self) -> float:
         return lib().alpacc_gpu_last_ms(self._h)
 
-    STAGES = ("lex", "pairs", "bracket_walk", "bracket_resolve", "parent_walk", "parent_resolve", "compact")
+    STAGES = ("lex", "pairs", "bracket_walk", "bracket_resolve", "parent_walk", "parent_resolve")
 
     def stage_ms(self) -> dict:
         vals = (ctypes.c_double * 8)()

@@ -108,18 +108,16 @@ def algorithmic_bytes(n, T, N, lay):
 
 
 def kernel_bytes(stage, n, T, B, P, N, lay):
-    """Algorithmic bytes of one launch of each kernel (its compulsory inputs and
-    outputs; the intermediate arrays count where they are the kernel's contract)."""
+    """Algorithmic bytes of one launch of each kernel: its compulsory inputs
+    and outputs (brackets and productions are u32 on the device)."""
     if stage == "lex":
         return n + T * (lay.terminal + lay.index + lay.length)
     if stage == "pairs":
         return T * lay.terminal + 4 * (B + P)
     if stage == "bracket_walk":
-        return 4 * B + 4 * B
+        return 4 * B
     if stage == "parent_walk":
-        return 4 * P + 4 * P + 4 * P + 4 * P
-    if stage == "compact":
-        return 4 * P * 3 + N * (lay.production + lay.index) + T * lay.index
+        return 4 * P + N * (lay.production + lay.index) + T * lay.index
     return 0
 
 
@@ -151,6 +149,22 @@ def cpu_baseline_sample(host: bytes, n_sample: int, reps: int = 4):
     return {"value": len(doc) / t / 1e9, "unit": "GB/s", "cores": 1, "kind": "reference",
             "sample": "%s, lex_string -> parse_test -> compute_parents -> compact_tree in memory, median of %d "
                       "runs (%.2fs each, %.1fs of CPU work), accepted=%s" % (what, reps, t, sum(times), ok[0])}
+
+
+def max_over_ranks(dist, ms, device=None):
+    """The largest of every rank's value: the job takes as long as its slowest rank."""
+    if not dist:
+        return ms
+    import torch
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world, n, steps, ms_total):
+    """Whole-job input GB/s: each of `world` ranks parsed its own n-byte document per step."""
+    return world * n * steps / (ms_total / 1e3) / 1e9
 
 
 def workload_config(n, world):
@@ -260,12 +274,9 @@ def ours(a, rank, world, local_rank, dist):
     torch.cuda.synchronize()
     ms_total = e0.elapsed_time(e1)
     clk = clocks.stop()
-    if dist:
-        t = torch.tensor([ms_total], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = max_over_ranks(dist, ms_total, dev)
     ms_step = ms_total / a.steps
-    value = world * n * a.steps / (ms_total / 1e3) / 1e9
+    value = job_throughput(world, n, a.steps, ms_total)
 
     # ---- end to end: pinned host input, host results ----
     pin = torch.empty(n, dtype=torch.uint8, pin_memory=True)
@@ -285,17 +296,15 @@ def ours(a, rank, world, local_rank, dist):
     f1.record(ext)
     torch.cuda.synchronize()
     e2e_ms = f0.elapsed_time(f1)
-    if dist:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = world * n * a.steps / (e2e_ms / 1e3) / 1e9
+    e2e_ms = max_over_ranks(dist, e2e_ms, dev)
+    e2e = job_throughput(world, n, a.steps, e2e_ms)
     d2h = T * (lay.terminal + lay.index + lay.length) + N * (lay.production + lay.index) + T * lay.index
 
     if rank != 0:
         return
     peak, peak_kind = peaks()
     mean = {k: (sum(v) / len(v) if v else 0.0) for k, v in stages.items()}
+    launches_per_call = sum(1 for v in mean.values() if v > 0)  # one kernel launch per timed stage
     dom = max(mean, key=lambda k: mean[k])
     st = parser.counts()
     B, P = st.get("B", 0), st.get("P", 0)
@@ -316,7 +325,7 @@ def ours(a, rank, world, local_rank, dist):
         "stage_ms": mean,
         "e2e": {"value": e2e, "unit": "GB/s", "h2d_bytes_per_step": n, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_ms / a.steps},
-        "gpu_launches": 7 * a.steps,
+        "gpu_launches": launches_per_call * a.steps,
         "clocks": clk,
         "machine": info,
     }
