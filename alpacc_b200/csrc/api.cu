@@ -71,14 +71,18 @@ int upload_tables(alpacc_gpu_grammar *g) {
   TRY(upload(g->lane_of, lm.lane_of));
   TRY(upload(g->img, lm.img));
   TRY(upload(g->img_cnt, lm.img_cnt));
+  if (!lm.img2.empty()) TRY(upload(g->img2, lm.img2));
   TRY(upload(g->sterm, lm.term));
   TRY(upload(g->sflags, lm.flags));
   const PairTable &pt = g->hg.pairs;
   TRY(upload(g->dense, pt.dense));
-  TRY(upload(g->rec_ss, pt.rec_ss));
-  TRY(upload(g->rec_ps, pt.rec_ps));
-  TRY(upload(g->rec_nb, pt.rec_nb));
-  TRY(upload(g->rec_np, pt.rec_np));
+  // records packed as ss | ps << 24 | nb << 48 | np << 56 (spans checked < 2^24 on load)
+  std::vector<unsigned long long> rec(pt.rec_ss.size());
+  for (size_t i = 0; i < rec.size(); i++)
+    rec[i] = (unsigned long long)pt.rec_ss[i] | ((unsigned long long)pt.rec_ps[i] << 24) |
+             ((unsigned long long)pt.rec_nb[i] << 48) | ((unsigned long long)pt.rec_np[i] << 56);
+  TRY(upload(g->rec, rec));
+
   TRY(upload(g->stacks, pt.stacks));
   TRY(upload(g->prods, pt.prods));
   TRY(upload(g->arity, pt.arity));
@@ -123,6 +127,118 @@ int ensure_lex_smem(size_t bytes) {
   return ALPACC_OK;
 }
 
+// Header of a pinned host result block; the arrays follow it. A result owns
+// two blocks: the token arrays (copied while the parser runs) and the tree
+// arrays (`second`).
+struct PinnedBlock {
+  alpacc_gpu_grammar *owner;
+  size_t size;
+  PinnedBlock *second;
+  size_t pad[5];
+};
+
+constexpr uint64_t kPieceTiles = 1128;  // tiles per host-to-device piece (~16 MiB)
+
+// A pinned block of at least `total` bytes, from the handle's cache when it
+// is large enough.
+PinnedBlock *acquire_block(alpacc_gpu_grammar *g, void **cache, size_t *cache_size, size_t total) {
+  void *host = nullptr;
+  if (*cache && *cache_size >= total) {
+    host = *cache;
+    *cache = nullptr;
+  } else {
+    if (*cache) cudaFreeHost(*cache);
+    *cache = nullptr;
+    const size_t want = total + total / 8;
+    if (cudaMallocHost(&host, want) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    reinterpret_cast<PinnedBlock *>(host)->size = want;
+  }
+  PinnedBlock *b = reinterpret_cast<PinnedBlock *>(host);
+  b->owner = g;
+  b->second = nullptr;
+  return b;
+}
+
+void release_block(alpacc_gpu_grammar *g, PinnedBlock *b, bool tree) {
+  if (!b) return;
+  void **cache = tree ? &g->pinned_cache2 : &g->pinned_cache;
+  size_t *size = tree ? &g->pinned_cache2_size : &g->pinned_cache_size;
+  if (!*cache) {
+    *cache = b;
+    *size = b->size;
+  } else {
+    cudaFreeHost(b);
+  }
+}
+
+// Token arrays of the current host call: copied on cstream once the lexer
+// finished, overlapping the parser's kernels.
+int start_token_copy(alpacc_gpu_grammar *g, uint64_t T) {
+  const alpacc_tables &tb = g->hg.t;
+  const size_t sz[3] = {T * tb.terminal_size, T * tb.index_size, T * tb.length_size};
+  size_t total = sizeof(PinnedBlock);
+  for (int i = 0; i < 3; i++) {
+    g->tok_off[i] = total;
+    total += (sz[i] + 15) & ~(size_t)15;
+  }
+  PinnedBlock *b = acquire_block(g, &g->pinned_cache, &g->pinned_cache_size, total);
+  if (!b) return ALPACC_E_NOMEM;
+  g->tok_block = b;
+  CK(cudaStreamWaitEvent(g->cstream, g->lex_done, 0));
+  const void *src[3] = {g->tok_ids.p, g->tok_starts.p, g->tok_lens.p};
+  for (int i = 0; i < 3; i++)
+    if (sz[i]) CK(cudaMemcpyAsync((char *)b + g->tok_off[i], src[i], sz[i], cudaMemcpyDeviceToHost, g->cstream));
+  return ALPACC_OK;
+}
+
+// Drop the current call's token block (after a reject or an error).
+void abandon_host_result(alpacc_gpu_grammar *g) {
+  if (!g->tok_block) return;
+  cudaStreamSynchronize(g->cstream);
+  release_block(g, reinterpret_cast<PinnedBlock *>(g->tok_block), false);
+  g->tok_block = nullptr;
+}
+
+// Tree arrays of the current host call, then the whole result.
+int finish_host_result(alpacc_gpu_grammar *g, alpacc_result *out) {
+  const alpacc_tables &tb = g->hg.t;
+  const uint64_t T = g->last_T, N = g->last_N;
+  const size_t sz[3] = {N * tb.production_size, N * tb.index_size, T * tb.index_size};
+  size_t off[3], total = sizeof(PinnedBlock);
+  for (int i = 0; i < 3; i++) {
+    off[i] = total;
+    total += (sz[i] + 15) & ~(size_t)15;
+  }
+  PinnedBlock *tree = acquire_block(g, &g->pinned_cache2, &g->pinned_cache2_size, total);
+  if (!tree) {
+    abandon_host_result(g);
+    return ALPACC_E_NOMEM;
+  }
+  const void *src[3] = {g->node_prods.p, g->node_parents.p, g->token_parents.p};
+  for (int i = 0; i < 3; i++)
+    if (sz[i]) CK(cudaMemcpyAsync((char *)tree + off[i], src[i], sz[i], cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  CK(cudaStreamSynchronize(g->cstream));
+  PinnedBlock *toks = reinterpret_cast<PinnedBlock *>(g->tok_block);
+  g->tok_block = nullptr;
+  toks->second = tree;
+  std::memset(out, 0, sizeof(*out));
+  out->valid = 1;
+  out->num_tokens = T;
+  out->num_nodes = N;
+  out->token_ids = (char *)toks + g->tok_off[0];
+  out->token_starts = (char *)toks + g->tok_off[1];
+  out->token_lengths = (char *)toks + g->tok_off[2];
+  out->node_productions = (char *)tree + off[0];
+  out->node_parents = (char *)tree + off[1];
+  out->token_parents = (char *)tree + off[2];
+  out->internal = toks;
+  return ALPACC_OK;
+}
+
 // The whole device path for d_in[0..n). Leaves counts in g->last_T / last_N.
 int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
   const HostGrammar &hg = g->hg;
@@ -133,6 +249,7 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
   const int prod_w = (int)tb.production_size;
   if (n > (1ull << 31) - 1) return ALPACC_E_CAPACITY;
   CK(cudaMemsetAsync(g->d_status, 0, sizeof(DeviceStatus), g->stream));
+  g->launches = 0;
   for (int k = 0; k < alpacc_gpu_grammar::kStages; k++) g->stage_used[k] = false;
   CK(cudaEventRecord(g->ev0, g->stream));
 
@@ -140,7 +257,17 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
   uint64_t T = 0;
   if (n > 0) {
     const uint64_t tiles = (n + kLexData - 1) / kLexData;
-    TRY(grow(g->lex_ticket, 16));
+    // host input: copied in pieces of ~16 MiB, each piece's tiles lexed as soon as it arrived
+    uint64_t piece_tiles = tiles, pieces = 1;
+    if (g->h_in) {
+      piece_tiles = kPieceTiles;
+      pieces = (tiles + piece_tiles - 1) / piece_tiles;
+      if (pieces > (uint64_t)alpacc_gpu_grammar::kMaxPieces) {
+        piece_tiles = (tiles + alpacc_gpu_grammar::kMaxPieces - 1) / alpacc_gpu_grammar::kMaxPieces;
+        pieces = (tiles + piece_tiles - 1) / piece_tiles;
+      }
+    }
+    TRY(grow(g->lex_ticket, 16 + pieces * 4));
     TRY(grow(g->st1_flag, tiles * 4));
     TRY(grow(g->st1_state, tiles));
     TRY(grow(g->st1_vec, tiles * (uint64_t)lm.M));
@@ -150,7 +277,16 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     TRY(grow(g->tok_ids, n * term_w));
     TRY(grow(g->tok_starts, n * idx_w));
     TRY(grow(g->tok_lens, n * len_w));
-    CK(cudaMemsetAsync(g->lex_ticket.p, 0, 16, g->stream));
+    // staged tokens: at most one per data byte of a tile, plus the final token of the last tile
+    const uint64_t cap = tiles * (uint64_t)kLexData + 16;
+    TRY(grow(g->stage_ids, cap));
+    TRY(grow(g->stage_starts, cap * 4));
+    TRY(grow(g->stage_ends, cap * 4));
+    TRY(grow(g->tile_cnt, tiles * 4));
+    TRY(grow(g->tile_pos, tiles * 4));
+    TRY(grow(g->tile_off, tiles * 8));
+    TRY(grow(g->tile_prev, tiles * 4));
+    CK(cudaMemsetAsync(g->lex_ticket.p, 0, 16 + pieces * 4, g->stream));
     CK(cudaMemsetAsync(g->st1_flag.p, 0, tiles * 4, g->stream));
     CK(cudaMemsetAsync(g->st2_flags.p, 0, tiles * 4, g->stream));
     LexArgs a{};
@@ -164,6 +300,7 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     a.lane_of = (const uint8_t *)g->lane_of.p;
     a.img = (const uint8_t *)g->img.p;
     a.img_cnt = (const uint8_t *)g->img_cnt.p;
+    a.img2 = lm.img2.empty() ? nullptr : (const unsigned long long *)g->img2.p;
     a.sterm = (const uint8_t *)g->sterm.p;
     a.sflags = (const uint8_t *)g->sflags.p;
     a.M = lm.M;
@@ -186,15 +323,59 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
                           (unsigned long long *)g->st2_inc.p};
     a.status = g->d_status;
     a.diag = g->diag;
+    a.stage_ids = (uint8_t *)g->stage_ids.p;
+    a.stage_starts = (uint32_t *)g->stage_starts.p;
+    a.stage_ends = (uint32_t *)g->stage_ends.p;
+    a.tile_cnt = (uint32_t *)g->tile_cnt.p;
+    a.tile_pos = (uint32_t *)g->tile_pos.p;
+    LexPlaceArgs pa{};
+    pa.num_tiles = tiles;
+    pa.n = n;
+    pa.tile_cnt = a.tile_cnt;
+    pa.tile_pos = a.tile_pos;
+    pa.tile_off = (unsigned long long *)g->tile_off.p;
+    pa.tile_prev = (uint32_t *)g->tile_prev.p;
+    pa.stage_ids = a.stage_ids;
+    pa.stage_starts = a.stage_starts;
+    pa.stage_ends = a.stage_ends;
+    pa.tok_ids = a.tok_ids;
+    pa.tok_starts = a.tok_starts;
+    pa.tok_lens = a.tok_lens;
+    pa.term_w = term_w;
+    pa.idx_w = idx_w;
+    pa.len_w = len_w;
+    pa.len_max = hg.len_max;
+    pa.status = g->d_status;
     stage_begin(g, 0);
-    const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)g->lex_grid);
-    lex_kernel<<<grid, kLexThreads, lex_smem_bytes(g), g->stream>>>(a);
+    for (uint64_t k = 0; k < pieces; ++k) {
+      const uint64_t tb = k * piece_tiles, te = std::min(tiles, tb + piece_tiles);
+      if (g->h_in) {
+        const uint64_t b0 = tb * kLexData, b1 = std::min<uint64_t>(n, te * kLexData);
+        CK(cudaMemcpyAsync((uint8_t *)d_in + b0, g->h_in + b0, b1 - b0, cudaMemcpyHostToDevice, g->cstream));
+        CK(cudaEventRecord(g->piece_ev[k], g->cstream));
+        CK(cudaStreamWaitEvent(g->stream, g->piece_ev[k], 0));
+      }
+      a.tile_begin = tb;
+      a.tile_end = te;
+      a.ticket = (unsigned *)g->lex_ticket.p + 4 + k;
+      const unsigned grid = (unsigned)std::min<uint64_t>(te - tb, (uint64_t)g->lex_grid);
+      lex_kernel<<<grid, kLexThreads, lex_smem_bytes(g), g->stream>>>(a);
+    ++g->launches;
+      CK(cudaGetLastError());
+    }
+    lex_scan_kernel<<<1, kLexScanThreads, 0, g->stream>>>(pa);
+    ++g->launches;
+    CK(cudaGetLastError());
+    lex_place_kernel<<<(unsigned)std::min<uint64_t>(tiles, 148 * 8), 256, 0, g->stream>>>(pa);
+    ++g->launches;
     stage_end(g, 0);
     CK(cudaGetLastError());
+    if (g->host_out) CK(cudaEventRecord(g->lex_done, g->stream));
     int rc = sync_status(g);
     if (rc) return rc;
     if (g->h_status->reject) return ALPACC_REJECT;
     T = g->h_status->num_tokens;
+    if (g->host_out) TRY(start_token_copy(g, T));
   }
 
   // ---------------- pair lookup ----------------
@@ -225,10 +406,7 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     a.start_t = (int)tb.start_terminal;
     a.end_t = (int)tb.end_terminal;
     a.dense = (const uint32_t *)g->dense.p;
-    a.rec_ss = (const uint32_t *)g->rec_ss.p;
-    a.rec_ps = (const uint32_t *)g->rec_ps.p;
-    a.rec_nb = (const uint8_t *)g->rec_nb.p;
-    a.rec_np = (const uint8_t *)g->rec_np.p;
+    a.rec = (const unsigned long long *)g->rec.p;
     a.stacks = (const uint32_t *)g->stacks.p;
     a.prods = (const uint32_t *)g->prods.p;
     a.br_out = (uint32_t *)g->br.p;
@@ -241,6 +419,7 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     a.status = g->d_status;
     stage_begin(g, 1);
     pair_kernel<<<(unsigned)tiles, kPairThreads, 0, g->stream>>>(a);
+    ++g->launches;
     stage_end(g, 1);
     CK(cudaGetLastError());
     int rc = sync_status(g);
@@ -283,6 +462,7 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     a.num_tiles = tiles;
     a.arity = (const int32_t *)g->arity.p;
     a.is_term = (const uint8_t *)g->is_term.p;
+    a.num_prods = (int)pt.arity.size();
     a.ch_h0 = (int32_t *)g->ch_h0.p;
     a.ch_min = (int32_t *)g->chunk_min.p;
     a.ch_tc = (int32_t *)g->ch_tc.p;
@@ -302,10 +482,12 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     a.status = g->d_status;
     stage_begin(g, 2 + 2 * mode);
     pse_tile_kernel<<<(unsigned)tiles, kPseThreads, 0, g->stream>>>(a);
+    ++g->launches;
     stage_end(g, 2 + 2 * mode);
     CK(cudaGetLastError());
     stage_begin(g, 3 + 2 * mode);
-    pse_resolve_kernel<<<148 * 4, 256, 0, g->stream>>>(a);
+    pse_resolve_kernel<<<148 * 8, 256, 0, g->stream>>>(a);
+    ++g->launches;
     stage_end(g, 3 + 2 * mode);
     CK(cudaGetLastError());
   }
@@ -338,59 +520,6 @@ void fill_device_result(alpacc_gpu_grammar *g, alpacc_result *out, int status) {
   out->token_parents = g->token_parents.p;
 }
 
-// Header of a pinned host result block; the arrays follow it.
-struct PinnedBlock {
-  alpacc_gpu_grammar *owner;
-  size_t size;
-  size_t pad[6];
-};
-
-// Copy a device result to one pinned host block (reused across calls once the
-// caller frees the previous result).
-int copy_result_to_host(alpacc_gpu_grammar *g, alpacc_result *out) {
-  const alpacc_tables &tb = g->hg.t;
-  const uint64_t T = g->last_T, N = g->last_N;
-  const size_t sz[6] = {T * tb.terminal_size, T * tb.index_size, T * tb.length_size,
-                        N * tb.production_size, N * tb.index_size, T * tb.index_size};
-  size_t off[6], total = sizeof(PinnedBlock);
-  for (int i = 0; i < 6; i++) {
-    off[i] = total;
-    total += (sz[i] + 15) & ~(size_t)15;
-  }
-  void *host = nullptr;
-  if (g->pinned_cache && g->pinned_cache_size >= total) {
-    host = g->pinned_cache;
-    g->pinned_cache = nullptr;
-  } else {
-    if (g->pinned_cache) cudaFreeHost(g->pinned_cache);
-    g->pinned_cache = nullptr;
-    size_t want = total + total / 8;
-    if (cudaMallocHost(&host, want) != cudaSuccess) {
-      cudaGetLastError();
-      return ALPACC_E_NOMEM;
-    }
-    reinterpret_cast<PinnedBlock *>(host)->size = want;
-  }
-  reinterpret_cast<PinnedBlock *>(host)->owner = g;
-  const void *src[6] = {g->tok_ids.p, g->tok_starts.p, g->tok_lens.p, g->node_prods.p, g->node_parents.p,
-                        g->token_parents.p};
-  for (int i = 0; i < 6; i++)
-    if (sz[i]) CK(cudaMemcpyAsync((char *)host + off[i], src[i], sz[i], cudaMemcpyDeviceToHost, g->stream));
-  CK(cudaStreamSynchronize(g->stream));
-  std::memset(out, 0, sizeof(*out));
-  out->valid = 1;
-  out->num_tokens = T;
-  out->num_nodes = N;
-  out->token_ids = (char *)host + off[0];
-  out->token_starts = (char *)host + off[1];
-  out->token_lengths = (char *)host + off[2];
-  out->node_productions = (char *)host + off[3];
-  out->node_parents = (char *)host + off[4];
-  out->token_parents = (char *)host + off[5];
-  out->internal = host;
-  return ALPACC_OK;
-}
-
 }  // namespace
 
 extern "C" {
@@ -417,6 +546,13 @@ alpacc_gpu_grammar *alpacc_gpu_load(const alpacc_tables *tables, int device, uin
       [&] {
         for (auto &e : g->sev)
           if (cudaEventCreate(&e) != cudaSuccess) return true;
+        return false;
+      }() ||
+      cudaStreamCreateWithFlags(&g->cstream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&g->lex_done, cudaEventDisableTiming) != cudaSuccess ||
+      [&] {
+        for (auto &e : g->piece_ev)
+          if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return true;
         return false;
       }() ||
       cudaMalloc(&g->d_status, sizeof(DeviceStatus)) != cudaSuccess ||
@@ -454,16 +590,24 @@ void alpacc_gpu_free(alpacc_gpu_grammar *g) {
   if (!g) return;
   cudaSetDevice(g->device);
   if (g->stream) cudaStreamSynchronize(g->stream);
-  DevBuf *bufs[] = {&g->cls_id, &g->trans_words, &g->lane_of, &g->img, &g->img_cnt, &g->sterm, &g->sflags,
-                    &g->dense, &g->rec_ss, &g->rec_ps, &g->rec_nb, &g->rec_np, &g->stacks, &g->prods,
+  DevBuf *bufs[] = {&g->cls_id, &g->trans_words, &g->lane_of, &g->img, &g->img_cnt, &g->img2, &g->sterm, &g->sflags,
+                    &g->dense, &g->rec, &g->stacks, &g->prods,
                     &g->arity, &g->is_term, &g->in, &g->lex_ticket, &g->st1_flag, &g->st1_state, &g->st1_vec,
                     &g->st2_flags, &g->st2_agg, &g->st2_inc, &g->tok_ids, &g->tok_starts, &g->tok_lens,
                     &g->pair_ticket, &g->pst_flags, &g->pst_agg, &g->pst_inc, &g->br, &g->pr, &g->pse_ticket,
                     &g->pse_flags, &g->pse_agg, &g->pse_inc, &g->ch_h0, &g->ch_tc, &g->tile_min,
                     &g->chunk_min, &g->super_min, &g->queue, &g->queue_len, &g->node_prods, &g->node_parents,
-                    &g->token_parents};
+                    &g->token_parents, &g->stage_ids, &g->stage_starts, &g->stage_ends, &g->tile_cnt,
+                    &g->tile_pos, &g->tile_off, &g->tile_prev};
   for (DevBuf *b : bufs) release(*b);
+  if (g->cstream) cudaStreamSynchronize(g->cstream);
   if (g->pinned_cache) cudaFreeHost(g->pinned_cache);
+  if (g->pinned_cache2) cudaFreeHost(g->pinned_cache2);
+  if (g->tok_block) cudaFreeHost(g->tok_block);
+  if (g->lex_done) cudaEventDestroy(g->lex_done);
+  for (auto &e : g->piece_ev)
+    if (e) cudaEventDestroy(e);
+  if (g->cstream) cudaStreamDestroy(g->cstream);
   if (g->d_status) cudaFree(g->d_status);
   if (g->h_status) cudaFreeHost(g->h_status);
   if (g->ev0) cudaEventDestroy(g->ev0);
@@ -503,12 +647,19 @@ int alpacc_gpu_parse(alpacc_gpu_grammar *g, const uint8_t *in, uint64_t n, alpac
   if (cudaSetDevice(g->device) != cudaSuccess) return ALPACC_E_CUDA;
   int rc = grow(g->in, n + 16);
   if (rc) return rc;
-  if (n > 0 && cudaMemcpyAsync(g->in.p, in, n, cudaMemcpyHostToDevice, g->stream) != cudaSuccess)
-    return ALPACC_E_CUDA;
+  g->h_in = in;
+  g->host_out = true;
   rc = run_device(g, (const uint8_t *)g->in.p, n);
+  g->h_in = nullptr;
+  g->host_out = false;
   g->last_status = rc;
-  if (rc != ALPACC_OK) return rc;
-  return copy_result_to_host(g, out);
+  if (rc == ALPACC_OK && !g->tok_block) rc = start_token_copy(g, g->last_T);  // empty input: no lexer ran
+  if (rc != ALPACC_OK) {
+    cudaStreamSynchronize(g->cstream);  // no piece copy may still read the caller's buffer
+    abandon_host_result(g);
+    return rc;
+  }
+  return finish_host_result(g, out);
 }
 
 int alpacc_gpu_parse_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offsets, uint32_t count,
@@ -528,12 +679,14 @@ void alpacc_result_free(alpacc_result *r) {
   if (!r) return;
   if (r->internal) {
     PinnedBlock *b = reinterpret_cast<PinnedBlock *>(r->internal);
+    PinnedBlock *tree = b->second;
     alpacc_gpu_grammar *g = b->owner;
-    if (g && !g->pinned_cache) {
-      g->pinned_cache = b;
-      g->pinned_cache_size = b->size;
+    if (g) {
+      release_block(g, b, false);
+      release_block(g, tree, true);
     } else {
       cudaFreeHost(b);
+      if (tree) cudaFreeHost(tree);
     }
   }
   std::memset(r, 0, sizeof(*r));
@@ -604,12 +757,13 @@ const char *alpacc_gpu_last_error(const alpacc_gpu_grammar *g) { return g ? g->l
 
 int alpacc_gpu_counts(const alpacc_gpu_grammar *g, int64_t *vals, int n) {
   if (!g || !vals || !g->h_status) return ALPACC_E_INVALID;
-  const int64_t v[8] = {(int64_t)g->h_status->num_tokens, (int64_t)g->h_status->num_brackets,
+  const int64_t v[9] = {(int64_t)g->h_status->num_tokens, (int64_t)g->h_status->num_brackets,
                         (int64_t)g->h_status->num_productions, (int64_t)g->h_status->num_nodes,
                         (int64_t)g->h_status->scratch[0], (int64_t)g->h_status->scratch[1],
-                        (int64_t)g->h_status->scratch[2], (int64_t)g->h_status->scratch[3]};
-  for (int i = 0; i < n && i < 8; i++) vals[i] = v[i];
-  return 8;
+                        (int64_t)g->h_status->scratch[2], (int64_t)g->h_status->scratch[3],
+                        (int64_t)g->launches};
+  for (int i = 0; i < n && i < 9; i++) vals[i] = v[i];
+  return 9;
 }
 
 void alpacc_gpu_set_diagnostics(alpacc_gpu_grammar *g, int on) {

@@ -178,6 +178,18 @@ static int build_lexer(const alpacc_tables *t, int ignore, LexerMachine *lm, std
     lm->img_cnt[c] = (uint8_t)targets.size();
     for (size_t i = 0; i < targets.size(); i++) lm->img[(size_t)c * kMaxLanes + i] = (uint8_t)targets[i];
   }
+  if (M <= 64 && (size_t)C * C <= 65536) {
+    lm->img2.assign((size_t)C * C, 0);
+    for (int c0 = 0; c0 < C; c0++)
+      for (int c1 = 0; c1 < C; c1++) {
+        unsigned long long mask = 0;
+        for (int i = 0; i < lm->img_cnt[c0]; i++) {
+          const int u = uniq[c1][lm->img[(size_t)c0 * kMaxLanes + i]];
+          if (u != lm->dead) mask |= 1ull << u;
+        }
+        lm->img2[(size_t)c0 * C + c1] = mask;
+      }
+  }
   return ALPACC_OK;
 }
 
@@ -225,6 +237,7 @@ static int build_pairs(const alpacc_tables *t, PairTable *pt, std::string *why) 
       return ALPACC_E_INVALID;
     }
     if (se - ss > 255 || pe - ps > 255) { *why = "more than 255 brackets or productions per pair"; return ALPACC_E_UNSUPPORTED; }
+    if (ss >= (1 << 24) || ps >= (1 << 24)) { *why = "stack or production table too large"; return ALPACC_E_UNSUPPORTED; }
     uint64_t d = 0;
     for (int j = 0; j < L; j++) d = d * (uint64_t)nt + key[j];
     if (pt->dense[d] != 0xffffffffu) continue;

@@ -32,6 +32,9 @@ struct LexerMachine {
   std::vector<uint8_t> img;       // [C*kMaxLanes] distinct live targets of each class
   std::vector<uint8_t> img_cnt;   // [C]
   std::vector<uint8_t> lane_of;   // [C*M] slot of trans[s][c] in img[c] or 0xff (dead)
+  // [C*C] (machines of at most 64 states): bit s set when some live state
+  // reaches live state s on a byte of class c0 followed by one of class c1
+  std::vector<unsigned long long> img2;
 };
 
 // LLP pair table as a dense array indexed by the key's terminals in base NT

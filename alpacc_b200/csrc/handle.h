@@ -67,10 +67,11 @@ struct alpacc_gpu_grammar {
   bool stage_used[kStages] = {};
   double stage_ms[kStages] = {};
   // tables
-  DevBuf cls_id, trans_words, lane_of, img, img_cnt, sterm, sflags;
-  DevBuf dense, rec_ss, rec_ps, rec_nb, rec_np, stacks, prods, arity, is_term;
+  DevBuf cls_id, trans_words, lane_of, img, img_cnt, img2, sterm, sflags;
+  DevBuf dense, rec, stacks, prods, arity, is_term;
   int trans_word_count = 0, trans_rep = 32;
   int lex_grid = 0;
+  int launches = 0;  // kernel launches of the last call
   int diag = 0;
   // status
   DeviceStatus *d_status = nullptr;
@@ -78,13 +79,28 @@ struct alpacc_gpu_grammar {
   // scratch
   DevBuf in;                                   // device copy of host input
   DevBuf lex_ticket, st1_flag, st1_state, st1_vec, st2_flags, st2_agg, st2_inc;
+  DevBuf stage_ids, stage_starts, stage_ends, tile_cnt, tile_pos, tile_off, tile_prev;
   DevBuf tok_ids, tok_starts, tok_lens;
   DevBuf pair_ticket, pst_flags, pst_agg, pst_inc, br, pr;
   DevBuf pse_ticket, pse_flags, pse_agg, pse_inc, ch_h0, ch_tc, tile_min, chunk_min, super_min, queue, queue_len;
   DevBuf node_prods, node_parents, token_parents;
-  // pinned host result buffers kept for reuse (released results come back here)
+  // pinned host result buffers kept for reuse (released results come back
+  // here): the token arrays' block and the tree arrays' block
   void *pinned_cache = nullptr;
   size_t pinned_cache_size = 0;
+  void *pinned_cache2 = nullptr;
+  size_t pinned_cache2_size = 0;
+  // host-buffer calls (alpacc_gpu_parse): the input is copied in pieces on
+  // cstream, each piece's lexer launch waits for its copy; the token arrays
+  // are copied back on cstream while the parser runs
+  cudaStream_t cstream = nullptr;
+  static constexpr int kMaxPieces = 64;
+  cudaEvent_t piece_ev[kMaxPieces] = {};
+  cudaEvent_t lex_done = nullptr;
+  const uint8_t *h_in = nullptr;  // host input of the current call, or null
+  bool host_out = false;          // copy the tokens back as soon as they exist
+  void *tok_block = nullptr;      // pinned block receiving the tokens of the current call
+  size_t tok_off[3] = {};
   // last result (device)
   uint64_t last_T = 0, last_N = 0;
   int last_status = ALPACC_E_INVALID;

@@ -29,6 +29,7 @@ struct LexArgs {
   const uint8_t *lane_of;           // [C*M]
   const uint8_t *img;               // [C*kMaxLanes]
   const uint8_t *img_cnt;           // [C]
+  const unsigned long long *img2;   // [C*C] live states after two bytes, or null
   const uint8_t *sterm;             // [M]
   const uint8_t *sflags;            // [M] bit0 produce, bit1 accept, bit2 kept
   int M, C, dead, m0, ignore;
@@ -41,17 +42,46 @@ struct LexArgs {
   unsigned *st1_flag;   // [tiles] 1 = transition vector published, 2 = outgoing state published
   uint8_t *st1_state;   // [tiles]
   uint8_t *st1_vec;     // [tiles * M]
+  unsigned long long tile_begin, tile_end;  // this launch's tiles (tile_end 0: all num_tiles)
   PairTileState st2;    // (kept-token count, last boundary position)
   DeviceStatus *status;
   int diag;             // 1: accumulate diagnostic counters in status->scratch
+  // Staged output (when stage_ids is set): tile i writes its kept tokens at
+  // i * kLexData + k with their start (0 when the start lies before the tile)
+  // and end positions, and its (count, last boundary) to tile_cnt / tile_pos;
+  // lex_scan_kernel and lex_place_kernel then place them. No tile waits for
+  // another tile's count. Without staging, the tiles chain their counts by
+  // decoupled look-back (st2) and write the final arrays directly.
+  uint8_t *stage_ids;
+  uint32_t *stage_starts, *stage_ends;
+  uint32_t *tile_cnt, *tile_pos;
 };
 
 __global__ void lex_kernel(LexArgs args);
+
+struct LexPlaceArgs {
+  unsigned long long num_tiles;
+  unsigned long long n;
+  const uint32_t *tile_cnt, *tile_pos;
+  unsigned long long *tile_off;  // exclusive prefix of tile_cnt
+  uint32_t *tile_prev;           // last boundary before each tile (0: none)
+  const uint8_t *stage_ids;
+  const uint32_t *stage_starts, *stage_ends;
+  void *tok_ids, *tok_starts, *tok_lens;
+  int term_w, idx_w, len_w;
+  unsigned long long len_max;
+  DeviceStatus *status;
+};
+
+constexpr int kLexScanThreads = 1024;
+__global__ void lex_scan_kernel(LexPlaceArgs args);   // one CTA
+__global__ void lex_place_kernel(LexPlaceArgs args);  // CTAs over tiles
 
 // ---- pair lookup / stack-action expansion: 256 threads x 8 positions ----
 constexpr int kPairThreads = 256;
 constexpr int kPairItems = 8;
 constexpr int kPairTile = kPairThreads * kPairItems;
+constexpr int kPairOut = 6144;  // output window of pair_kernel (elements)
 
 struct PairArgs {
   const void *tok_ids;      // lexer output, terminal ids (term_w bytes each)
@@ -61,8 +91,7 @@ struct PairArgs {
   int q, k, nt;
   int empty_t, start_t, end_t;
   const uint32_t *dense;    // [nt^(q+k)] record index or 0xffffffff
-  const uint32_t *rec_ss, *rec_ps;
-  const uint8_t *rec_nb, *rec_np;
+  const unsigned long long *rec;  // ss | ps << 24 | nb << 48 | np << 56
   const uint32_t *stacks;   // bit31 left
   const uint32_t *prods;
   uint32_t *br_out;         // brackets (capacity br_cap)
@@ -96,6 +125,7 @@ struct PseArgs {
   unsigned long long num_tiles;
   const int32_t *arity;             // parents: per production
   const uint8_t *is_term;           // parents: terminal production flags
+  int num_prods;                    // entries of arity / is_term
   int32_t *ch_h0;                   // [tiles * 256] depth before each chunk
   int32_t *ch_min;                  // [tiles * 256] minimum depth in each chunk (INT_MAX if empty)
   int32_t *ch_tc;                   // parents: [tiles * 256] terminal productions before each chunk

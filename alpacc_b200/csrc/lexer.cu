@@ -144,17 +144,18 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
   const int dead = a.dead;
   const long long n = (long long)a.n;
   const unsigned long long num_tiles = a.num_tiles;
+  const unsigned long long tile_end = a.tile_end ? a.tile_end : num_tiles;
 
   for (unsigned long long round = 0;; ++round) {
-    if (round > num_tiles) {  // every round takes a new ticket: cannot happen
+    if (round > tile_end - a.tile_begin) {  // every round takes a new ticket: cannot happen
       if (t == 0) record_timeout(st, kSiteLexTiles);
       break;
     }
     __syncthreads();  // tables ready / previous tile fully consumed
     if (t == 0) sm->tile = atomicAdd(a.ticket, 1u);
     __syncthreads();
-    const unsigned long long tile = sm->tile;
-    if (tile >= num_tiles) break;
+    const unsigned long long tile = a.tile_begin + sm->tile;
+    if (tile >= tile_end) break;
     const long long data0 = (long long)tile * kLexData;
     const long long load0 = data0 - (long long)kLexHalo * kLexChunk;
 
@@ -203,7 +204,12 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
         if (!exact) {
           const unsigned long long live = dead >= 0 ? ~(1ull << dead) : ~0ull;
           unsigned long long set = 0;
-          for (int l = 0; l < cnt; l++) set |= 1ull << __ldg(a.img + c0 * kMaxLanes + l);
+          if (a.img2 && nb >= 2) {  // the first two bytes at once
+            set = __ldg(a.img2 + c0 * a.C + sm->cls_id[tb8[1]]);
+            j = 2;
+          } else {
+            for (int l = 0; l < cnt; l++) set |= 1ull << __ldg(a.img + c0 * kMaxLanes + l);
+          }
           while (j < nb && __popcll(set) > 1) {
             const uint32_t cp = cls_pre(tb, tb8[j]);
             unsigned long long ns = 0;
@@ -422,6 +428,35 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
     const Pair64 cp_ex = block_exclusive_scan_pair(Pair64{cnt, lastb}, CntPosOp(), Pair64{0, 0}, sm->pair_tmp, &cp_tot);
     const long long cnt_ex = cp_ex.a, pos_ex = cp_ex.b;
     const long long cnt_tot = cp_tot.a, pos_tot = cp_tot.b;
+    if (a.stage_ids) {
+      // ---- staged: tile-local offsets, no wait on other tiles ----
+      if (t == 0) {
+        a.tile_cnt[tile] = (uint32_t)cnt_tot;
+        a.tile_pos[tile] = (uint32_t)pos_tot;
+      }
+      if (t >= kLexHalo && nb > 0) {
+        unsigned long long out = tile * (unsigned long long)kLexData + (unsigned long long)cnt_ex;
+        long long tok_start = pos_ex;  // 0: the token starts before this tile
+        for (unsigned long long m = bmask; m; m &= m - 1) {
+          const int j = __ffsll((long long)m) - 1;
+          const long long p = g0 + j;
+          const int s = tb8[j];
+          if (sm->sflags[s] & 4) {
+            a.stage_ids[out] = sm->sterm[s];
+            a.stage_starts[out] = (uint32_t)tok_start;
+            a.stage_ends[out] = (uint32_t)p;
+            ++out;
+          }
+          tok_start = p;
+        }
+        if (final_tok && final_kept) {
+          a.stage_ids[out] = (uint8_t)final_term;
+          a.stage_starts[out] = (uint32_t)tok_start;
+          a.stage_ends[out] = (uint32_t)n;
+        }
+      }
+      continue;
+    }
     if (t < kWarp) {
       const Pair64 agg{cnt_tot, pos_tot};
       Pair64 prefix{0, 0};
@@ -469,6 +504,68 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
       if (too_long) record_reject(st, &st->lex_reject_reason, 3);
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// Placement of staged tokens
+// ---------------------------------------------------------------------------
+
+// Exclusive (count, last boundary) prefix over the tiles, by one CTA; also the
+// total token count.
+__global__ void __launch_bounds__(kLexScanThreads) lex_scan_kernel(LexPlaceArgs a) {
+  __shared__ Pair64 tmp[kLexScanThreads / 32];
+  const int t = threadIdx.x;
+  constexpr int kPer = 4;
+  Pair64 carry{0, 0};
+  for (unsigned long long base = 0; base < a.num_tiles; base += (unsigned long long)kLexScanThreads * kPer) {
+    const unsigned long long i0 = base + (unsigned long long)t * kPer;
+    long long c[kPer], p[kPer];
+    Pair64 loc{0, 0};
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const bool ok = i0 + k < a.num_tiles;
+      c[k] = ok ? a.tile_cnt[i0 + k] : 0;
+      p[k] = ok ? a.tile_pos[i0 + k] : 0;
+      loc = CntPosOp()(loc, Pair64{c[k], p[k]});
+    }
+    Pair64 tot;
+    const Pair64 ex = block_exclusive_scan_pair(loc, CntPosOp(), Pair64{0, 0}, tmp, &tot);
+    Pair64 run = CntPosOp()(carry, ex);
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      if (i0 + k < a.num_tiles) {
+        a.tile_off[i0 + k] = (unsigned long long)run.a;
+        a.tile_prev[i0 + k] = (uint32_t)run.b;
+      }
+      run = CntPosOp()(run, Pair64{c[k], p[k]});
+    }
+    carry = CntPosOp()(carry, tot);
+  }
+  if (t == 0) a.status->num_tokens = (unsigned long long)carry.a;
+}
+
+// Each CTA copies whole tiles' staged tokens to their final places; a token
+// whose start lies before its tile takes the last boundary before the tile.
+__global__ void __launch_bounds__(256) lex_place_kernel(LexPlaceArgs a) {
+  DeviceStatus *st = a.status;
+  bool too_long = false;
+  for (unsigned long long tile = blockIdx.x; tile < a.num_tiles; tile += gridDim.x) {
+    const unsigned c = a.tile_cnt[tile];
+    const unsigned long long off = a.tile_off[tile];
+    const uint32_t prev = a.tile_prev[tile];
+    const unsigned long long base = tile * (unsigned long long)kLexData;
+    for (unsigned i = threadIdx.x; i < c; i += blockDim.x) {
+      const uint32_t s0 = a.stage_starts[base + i];
+      const uint32_t start = s0 > prev ? s0 : prev;
+      const uint32_t end = a.stage_ends[base + i];
+      const unsigned long long len = end - start;
+      if (len > a.len_max) too_long = true;
+      store_uint(a.tok_ids, off + i, a.term_w, a.stage_ids[base + i]);
+      store_uint(a.tok_starts, off + i, a.idx_w, start);
+      store_uint(a.tok_lens, off + i, a.len_w, len);
+    }
+  }
+  if (too_long) record_reject(st, &st->lex_reject_reason, 3);
 }
 
 }  // namespace alpacc

@@ -55,16 +55,18 @@ struct AddPair {
 // The tile's terminals (with the q before and k - 1 after it) are staged in
 // shared memory once; keys are formed there with positions strided across the
 // threads (conflict-free), the per-position counts are scanned in blocked
-// order (one packed 64-bit scan of (brackets, productions)), and each thread
-// then writes the stack actions and productions of its 8 consecutive
-// positions.
-__global__ void __launch_bounds__(kPairThreads) pair_kernel(PairArgs a) {
+// order (one packed 64-bit scan of (brackets, productions)), and the tile's
+// stack actions, then its productions, are assembled in a shared-memory
+// window and written with consecutive threads (a thread's own runs would
+// cost one memory transaction per element).
+__global__ void __launch_bounds__(kPairThreads, 5) pair_kernel(PairArgs a) {
   __shared__ unsigned s_tile;
   __shared__ long long s_tmp[kPairThreads / 32];
   __shared__ long long s_prefix_b, s_prefix_p;
   __shared__ uint16_t s_term[kPairTile + 8];             // window of terminals; 0xffff = out of range
   __shared__ __align__(16) uint32_t s_rec[kPairTile];    // record per position
   __shared__ __align__(16) uint16_t s_cnt[kPairTile];    // brackets | productions << 8
+  __shared__ __align__(16) uint32_t s_out[kPairOut];     // output window
   const int t = threadIdx.x;
   DeviceStatus *st = a.status;
   if (t == 0) s_tile = atomicAdd(a.ticket, 1u);
@@ -94,7 +96,6 @@ __global__ void __launch_bounds__(kPairThreads) pair_kernel(PairArgs a) {
   for (int j = 0; j < kPairItems; ++j) {
     const int li = j * kPairThreads + t;
     uint32_t r = 0xffffffffu;
-    uint16_t c = 0;
     if (tile0 + li < m) {
       unsigned long long d = 0;
       bool bad = false;
@@ -105,10 +106,9 @@ __global__ void __launch_bounds__(kPairThreads) pair_kernel(PairArgs a) {
       }
       r = bad ? 0xffffffffu : __ldg(a.dense + d);
       if (r == 0xffffffffu) missing = true;
-      else c = (uint16_t)(__ldg(a.rec_nb + r) | (__ldg(a.rec_np + r) << 8));
     }
     s_rec[li] = r;
-    s_cnt[li] = c;
+    s_cnt[li] = r == 0xffffffffu ? (uint16_t)0 : (uint16_t)(__ldg(a.rec + r) >> 48);
   }
   if (missing) record_reject(st, &st->parse_reject_reason, 1);
   __syncthreads();
@@ -148,25 +148,37 @@ __global__ void __launch_bounds__(kPairThreads) pair_kernel(PairArgs a) {
     }
   }
   __syncthreads();
-  unsigned long long ob = (unsigned long long)(s_prefix_b + (ex >> 32));
-  unsigned long long op = (unsigned long long)(s_prefix_p + (ex & 0xffffffffll));
-  bool overflow = false;
-#pragma unroll
-  for (int j = 0; j < kPairItems; ++j) {
-    const uint32_t r = s_rec[t * kPairItems + j];
-    if (r == 0xffffffffu) continue;
-    const int nb = cnt[j] & 0xff, np = cnt[j] >> 8;
-    if (ob + nb > a.br_cap || op + np > a.pr_cap) {
-      overflow = true;
-      break;
-    }
-    const uint32_t ss = __ldg(a.rec_ss + r), ps = __ldg(a.rec_ps + r);
-    for (int x = 0; x < nb; ++x) a.br_out[ob + x] = __ldg(a.stacks + ss + x);
-    for (int x = 0; x < np; ++x) a.pr_out[op + x] = __ldg(a.prods + ps + x);
-    ob += nb;
-    op += np;
+  const long long pre_b = s_prefix_b, pre_p = s_prefix_p;
+  if ((unsigned long long)(pre_b + tb) > a.br_cap || (unsigned long long)(pre_p + tp) > a.pr_cap) {
+    if (t == 0) atomicCAS(&st->error, 0, -4 /* ALPACC_E_CAPACITY */);
+    return;
   }
-  if (overflow) atomicCAS(&st->error, 0, -4 /* ALPACC_E_CAPACITY */);
+  // ---- brackets (pass 0) and productions (pass 1) through the output window ----
+  for (int pass = 0; pass < 2; ++pass) {
+    const long long total = pass == 0 ? tb : tp;
+    const long long base = pass == 0 ? (ex >> 32) : (ex & 0xffffffffll);
+    const uint32_t *src = pass == 0 ? a.stacks : a.prods;
+    uint32_t *dst = pass == 0 ? a.br_out + pre_b : a.pr_out + pre_p;
+    for (long long w0 = 0; w0 < total; w0 += kPairOut) {
+      long long o = base;
+#pragma unroll
+      for (int j = 0; j < kPairItems; ++j) {
+        const int c = pass == 0 ? (cnt[j] & 0xff) : (cnt[j] >> 8);
+        if (c == 0) continue;
+        const unsigned long long rc = __ldg(a.rec + s_rec[t * kPairItems + j]);
+        const uint32_t sidx = (uint32_t)((pass == 0 ? rc : rc >> 24) & 0xffffffu);
+        for (int x = 0; x < c; ++x) {
+          const long long q = o + x - w0;
+          if (q >= 0 && q < kPairOut) s_out[q] = __ldg(src + sidx + x);
+        }
+        o += c;
+      }
+      __syncthreads();
+      const int wn = (int)(total - w0 < kPairOut ? total - w0 : kPairOut);
+      for (int i = t; i < wn; i += kPairThreads) dst[w0 + i] = s_out[i];
+      __syncthreads();
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -194,12 +206,14 @@ __device__ __forceinline__ int pse_step(const PseArgs &a, uint32_t v) {
   return __ldg(a.arity + v) - 1;
 }
 
+constexpr int kPseSmemProds = 1024;  // production tables copied to shared memory up to this size
+
 // compact_tree's output for production e (parser.c:126-153): terminal
 // productions give their token's parent, the others a tree node; parents are
 // renumbered by subtracting the terminal productions before them.
-__device__ __forceinline__ void emit_node(const PseArgs &a, uint32_t prod, long long e, long long tinc_e,
+__device__ __forceinline__ void emit_node(const PseArgs &a, uint32_t prod, bool term, long long e, long long tinc_e,
                                           long long p_new, long long T) {
-  if (__ldg(a.is_term + prod)) {
+  if (term) {
     if (tinc_e >= 1 && tinc_e <= T)
       store_uint(a.token_parents, (unsigned long long)(tinc_e - 1), a.idx_w, (unsigned long long)p_new);
   } else {
@@ -222,17 +236,25 @@ __device__ __forceinline__ void emit_node(const PseArgs &a, uint32_t prod, long 
 __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   __shared__ unsigned s_tile;
   __shared__ PseSmem sm;
+  __shared__ int32_t s_arity[kPseSmemProds];
+  __shared__ uint8_t s_is_term[kPseSmemProds];
   const int t = threadIdx.x;
   const int lane = t & (kWarp - 1);
   const int warp = t >> 5;
   DeviceStatus *st = a.status;
   if (t == 0) s_tile = atomicAdd(a.ticket, 1u);
+  const bool parents = a.mode == kPseParents;
+  const bool prod_smem = parents && a.num_prods <= kPseSmemProds;
+  if (prod_smem)
+    for (int i = t; i < a.num_prods; i += kPseThreads) {
+      s_arity[i] = __ldg(a.arity + i);
+      s_is_term[i] = __ldg(a.is_term + i);
+    }
   __syncthreads();
   const unsigned long long tile = s_tile;
   const long long E = (long long)*a.count;
   const long long tile0 = (long long)tile * kPseTile;
   if (tile0 >= E) return;
-  const bool parents = a.mode == kPseParents;
   const long long c0 = tile0 + (long long)t * kPseItems;  // first element of this thread's chunk
 
   // ---- load ----
@@ -254,8 +276,15 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   for (int j = 0; j < kPseItems; ++j) {
     hr[j] = ssum;
     if (c0 + j < E) {
-      ssum += pse_step(a, v[j]);
-      if (parents) tsum += __ldg(a.is_term + v[j]) ? 1 : 0;
+      if (!parents) {
+        ssum += (v[j] >> 31) ? 1 : -1;
+      } else if (prod_smem && v[j] < kPseSmemProds) {
+        ssum += s_arity[v[j]] - 1;
+        tsum += s_is_term[v[j]];
+      } else {
+        ssum += __ldg(a.arity + v[j]) - 1;
+        tsum += __ldg(a.is_term + v[j]) ? 1 : 0;
+      }
     }
     tcr[j] = tsum;
   }
@@ -290,10 +319,11 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   if (lane == kWarp - 1) sm.wmin[warp] = L[5];
   __syncthreads();
 
-  // ---- queries: own chunk ----
+  // ---- queries: own chunk, then the previous chunk ----
   // ans: local index of the answer; -1 pending; -2 no query; -3 the root
   int ans[kPseItems];
   unsigned need = 0;
+  const int prev_min = t > 0 ? sm.lv[0][t - 1] : INT_MAX;  // minimum depth of the previous chunk
 #pragma unroll
   for (int j = 0; j < kPseItems; ++j) {
     ans[j] = -2;
@@ -310,15 +340,26 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
       if (v[j] >> 31) continue;  // left bracket: no query
       qv = hr[j] - 1;
     }
-    int f = -1;
+    int f = 0;
+    bool got = false;
     uint32_t pv = 0;
 #pragma unroll
     for (int jj = 0; jj < j; ++jj)
       if (hr[jj] <= qv) {
         f = jj;
         pv = v[jj];
+        got = true;
       }
-    if (f >= 0) {
+    if (!got && prev_min <= qv) {  // the latest candidate lies in the previous chunk
+#pragma unroll
+      for (int jj = kPseItems - 1; jj >= 0; --jj)
+        if (!got && sm.h[(t - 1) * kPseStride + jj] <= qv) {
+          f = jj - kPseItems;
+          pv = sm.v[(t - 1) * kPseStride + jj];
+          got = true;
+        }
+    }
+    if (got) {
       ans[j] = t * kPseItems + f;
       if (!parents && ((pv ^ v[j]) & 0x7fffffffu)) record_reject(st, &st->parse_reject_reason, 2);
     } else {
@@ -438,12 +479,13 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
 #pragma unroll
     for (int j = 0; j < kPseItems; ++j) {
       const int an = ans[j];
+      const bool term = tcr[j] != (j > 0 ? tcr[j - 1] : 0);
       if (an == -3) {  // the root: compute_parents gives it parent 0
-        emit_node(a, v[j], c0 + j, pb + ex_t + tcr[j], 0 - (pb + sm.tc[0]), T);
+        emit_node(a, v[j], term, c0 + j, pb + ex_t + tcr[j], 0 - (pb + sm.tc[0]), T);
       } else if (an >= 0) {
         const long long p = tile0 + an;
         const long long tinc_p = pb + sm.tc[(an / kPseItems) * kPseStride + an % kPseItems];
-        emit_node(a, v[j], c0 + j, pb + ex_t + tcr[j], p - tinc_p, T);
+        emit_node(a, v[j], term, c0 + j, pb + ex_t + tcr[j], p - tinc_p, T);
       }
     }
   }
@@ -529,7 +571,7 @@ __global__ void pse_resolve_kernel(PseArgs a) {
       const long long p = found >= 0 ? found : 0;
       const long long tinc_p = terminal_count(a, p, lane);
       const long long tinc_e = terminal_count(a, e, lane);
-      if (lane == 0) emit_node(a, v, e, tinc_e, p - tinc_p, (long long)*a.num_tokens);
+      if (lane == 0) emit_node(a, v, __ldg(a.is_term + v) != 0, e, tinc_e, p - tinc_p, (long long)*a.num_tokens);
     } else if (lane == 0) {
       if (found < 0) record_reject(st, &st->parse_reject_reason, 3);
       else if ((a.elems[found] & 0x7fffffffu) != (v & 0x7fffffffu)) record_reject(st, &st->parse_reject_reason, 2);

@@ -256,10 +256,10 @@ class Parser:
 
     def counts(self) -> dict:
         """Tokens, brackets, productions, nodes of the last call."""
-        vals = (ctypes.c_int64 * 8)()
-        lib().alpacc_gpu_counts(self._h, vals, 8)
+        vals = (ctypes.c_int64 * 9)()
+        lib().alpacc_gpu_counts(self._h, vals, 9)
         return {"T": vals[0], "B": vals[1], "P": vals[2], "N": vals[3], "vector_tiles": vals[4],
-                "const_chunks": vals[5], "chain_evals": vals[6], "multi_lane_bytes": vals[7]}
+                "const_chunks": vals[5], "chain_evals": vals[6], "multi_lane_bytes": vals[7], "launches": vals[8]}
 
     def set_diagnostics(self, on: bool):
         lib().alpacc_gpu_set_diagnostics(self._h, 1 if on else 0)

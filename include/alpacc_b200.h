@@ -128,7 +128,9 @@ void alpacc_gpu_free(alpacc_gpu_grammar *g);
 
 /*
  * Parse host bytes: H2D copy, the device path, D2H copy of the result into
- * pinned memory owned by *out. Returns ALPACC_OK, ALPACC_REJECT or an error.
+ * pinned memory owned by *out. The input is copied in pieces of ~16 MiB and
+ * each piece is lexed as soon as it has arrived; the token arrays are copied
+ * back while the parser runs. Returns ALPACC_OK, ALPACC_REJECT or an error.
  */
 int alpacc_gpu_parse(alpacc_gpu_grammar *g, const uint8_t *in, uint64_t n, alpacc_result *out);
 
@@ -158,9 +160,9 @@ int alpacc_gpu_lex_noalloc(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t 
                            void *d_token_starts, void *d_token_lengths, uint64_t *num_tokens);
 
 /*
- * Enqueue the device path for device-resident input without waiting; the
- * status and counts are written to device memory and read back later with
- * alpacc_gpu_collect. For timing loops and CUDA-graph capture.
+ * Run the device path for device-resident input (as alpacc_gpu_parse_device,
+ * which also waits for the status) and keep the outcome in the handle;
+ * alpacc_gpu_collect then returns that status and the device result arrays.
  */
 int alpacc_gpu_enqueue(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n);
 int alpacc_gpu_collect(alpacc_gpu_grammar *g, alpacc_result *out);
@@ -214,7 +216,8 @@ const char *alpacc_gpu_last_error(const alpacc_gpu_grammar *g);
 int alpacc_gpu_stage_ms(const alpacc_gpu_grammar *g, double *out, int n);
 /* Tokens, brackets, productions and tree nodes of the last call, then four
    lexer diagnostic counters (collected when diagnostics are on): tiles without
-   a constant chunk, constant chunks, chain evaluations, multi-lane bytes. */
+   a constant chunk, constant chunks, chain evaluations, multi-lane bytes; then
+   the number of kernels the call launched. */
 int alpacc_gpu_counts(const alpacc_gpu_grammar *g, int64_t *vals, int n);
 void alpacc_gpu_set_diagnostics(alpacc_gpu_grammar *g, int on);
 
