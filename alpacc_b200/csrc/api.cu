@@ -137,7 +137,7 @@ struct PinnedBlock {
   size_t pad[5];
 };
 
-constexpr uint64_t kPieceTiles = 1128;  // tiles per host-to-device piece (~16 MiB)
+constexpr uint64_t kPieceTiles = (16u << 20) / kLexData;  // tiles per host-to-device piece (~16 MiB)
 
 // A pinned block of at least `total` bytes, from the handle's cache when it
 // is large enough.
@@ -330,6 +330,7 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     a.tile_pos = (uint32_t *)g->tile_pos.p;
     LexPlaceArgs pa{};
     pa.num_tiles = tiles;
+    pa.tile_data = kLexData;
     pa.n = n;
     pa.tile_cnt = a.tile_cnt;
     pa.tile_pos = a.tile_pos;

@@ -70,7 +70,7 @@ struct alpacc_gpu_grammar {
   DevBuf cls_id, trans_words, lane_of, img, img_cnt, img2, sterm, sflags;
   DevBuf dense, rec, stacks, prods, arity, is_term;
   int trans_word_count = 0, trans_rep = 32;
-  int lex_grid = 0;
+  int lex_grid = 0;  // persistent grid of lex_kernel
   int launches = 0;  // kernel launches of the last call
   int diag = 0;
   // status

@@ -61,6 +61,7 @@ __global__ void lex_kernel(LexArgs args);
 
 struct LexPlaceArgs {
   unsigned long long num_tiles;
+  unsigned long long tile_data;  // data bytes per tile (staging stride)
   unsigned long long n;
   const uint32_t *tile_cnt, *tile_pos;
   unsigned long long *tile_off;  // exclusive prefix of tile_cnt

@@ -515,29 +515,20 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
 __global__ void __launch_bounds__(kLexScanThreads) lex_scan_kernel(LexPlaceArgs a) {
   __shared__ Pair64 tmp[kLexScanThreads / 32];
   const int t = threadIdx.x;
-  constexpr int kPer = 4;
+  constexpr int kPer = 16;
   Pair64 carry{0, 0};
   for (unsigned long long base = 0; base < a.num_tiles; base += (unsigned long long)kLexScanThreads * kPer) {
     const unsigned long long i0 = base + (unsigned long long)t * kPer;
-    long long c[kPer], p[kPer];
     Pair64 loc{0, 0};
-#pragma unroll
-    for (int k = 0; k < kPer; ++k) {
-      const bool ok = i0 + k < a.num_tiles;
-      c[k] = ok ? a.tile_cnt[i0 + k] : 0;
-      p[k] = ok ? a.tile_pos[i0 + k] : 0;
-      loc = CntPosOp()(loc, Pair64{c[k], p[k]});
-    }
+    for (int k = 0; k < kPer && i0 + k < a.num_tiles; ++k)
+      loc = CntPosOp()(loc, Pair64{(long long)a.tile_cnt[i0 + k], (long long)a.tile_pos[i0 + k]});
     Pair64 tot;
     const Pair64 ex = block_exclusive_scan_pair(loc, CntPosOp(), Pair64{0, 0}, tmp, &tot);
     Pair64 run = CntPosOp()(carry, ex);
-#pragma unroll
-    for (int k = 0; k < kPer; ++k) {
-      if (i0 + k < a.num_tiles) {
-        a.tile_off[i0 + k] = (unsigned long long)run.a;
-        a.tile_prev[i0 + k] = (uint32_t)run.b;
-      }
-      run = CntPosOp()(run, Pair64{c[k], p[k]});
+    for (int k = 0; k < kPer && i0 + k < a.num_tiles; ++k) {
+      a.tile_off[i0 + k] = (unsigned long long)run.a;
+      a.tile_prev[i0 + k] = (uint32_t)run.b;
+      run = CntPosOp()(run, Pair64{(long long)a.tile_cnt[i0 + k], (long long)a.tile_pos[i0 + k]});
     }
     carry = CntPosOp()(carry, tot);
   }
@@ -553,7 +544,7 @@ __global__ void __launch_bounds__(256) lex_place_kernel(LexPlaceArgs a) {
     const unsigned c = a.tile_cnt[tile];
     const unsigned long long off = a.tile_off[tile];
     const uint32_t prev = a.tile_prev[tile];
-    const unsigned long long base = tile * (unsigned long long)kLexData;
+    const unsigned long long base = tile * (unsigned long long)a.tile_data;
     for (unsigned i = threadIdx.x; i < c; i += blockDim.x) {
       const uint32_t s0 = a.stage_starts[base + i];
       const uint32_t start = s0 > prev ? s0 : prev;

@@ -36,6 +36,25 @@ METRIC = "input GB/s lex+parse at 1 B200 (% HBM peak); serve p99 ms vs per-input
 GRAMMAR = os.path.join(REPO, "grammars", "json_ext.alp")
 REF_CONFIG = "json_ext_i32"
 
+# Workloads (the default is the headline one). Each: grammar, index width,
+# reference configuration, default size, document generator (n, seed), and
+# whether the document is meant to be rejected.
+WORKLOADS = {
+    "json": dict(grammar="json_ext.alp", index32=True, ref="json_ext_i32", size=256 << 20, reject=False,
+                 desc="json_ext %d MiB single JSON document per GPU"),
+    "sexp": dict(grammar="sexp.alp", index32=False, ref="sexp_i64", size=1 << 30, reject=False,
+                 desc="sexp %d MiB single s-expression document per GPU (nesting up to 10000)"),
+    "sexp_unbalanced": dict(grammar="sexp.alp", index32=False, ref="sexp_i64", size=1 << 30, reject=True,
+                            desc="sexp %d MiB document with 5%% of forms carrying an extra ')' (rejected)"),
+}
+
+
+def make_doc(workload, n, seed):
+    from alpacc_b200 import workloads as W
+    if workload == "json":
+        return W.json_doc(n, seed)
+    return W.sexp_doc(n, seed + 1, unbalanced_frac=0.05 if workload == "sexp_unbalanced" else 0.0, max_depth=10000)
+
 
 def peaks():
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
@@ -121,23 +140,23 @@ def kernel_bytes(stage, n, T, B, P, N, lay):
     return 0
 
 
-def cpu_baseline_sample(host: bytes, n_sample: int, reps: int = 4):
+def cpu_baseline_sample(host: bytes, n_sample: int, ref_config: str = REF_CONFIG, workload: str = "json",
+                        reps: int = 4):
     """The reference C backend, single thread (it is sequential), on the timed
     document itself when n_sample >= its size, otherwise on a seeded document
     of n_sample bytes from the same generator."""
-    from alpacc_b200 import workloads as W
     from oracle.ref import RefOracle, available
     import numpy as np
 
-    if not available(REF_CONFIG):
+    if not available(ref_config):
         return None
     if n_sample >= len(host):
         doc = np.frombuffer(host, dtype=np.uint8)
         what = "the timed %d MiB document itself" % (len(host) >> 20)
     else:
-        doc = np.frombuffer(W.json_doc(n_sample, 2), dtype=np.uint8)
+        doc = np.frombuffer(make_doc(workload, n_sample, 2), dtype=np.uint8)
         what = "one %d MiB document of the same generator (seed 2)" % (n_sample >> 20)
-    ref = RefOracle(REF_CONFIG)
+    ref = RefOracle(ref_config)
     ref.pipeline(doc[: 1 << 20])  # warm
     times = []
     ok = None
@@ -167,9 +186,10 @@ def job_throughput(world, n, steps, ms_total):
     return world * n * steps / (ms_total / 1e3) / 1e9
 
 
-def workload_config(n, world):
-    return {"workload": "json_ext %d MiB single JSON document per GPU" % (n >> 20), "grammar": "json_ext.alp",
-            "bytes": n, "index": "i32", "parallelism": "replicas x%d" % world,
+def workload_config(n, world, workload="json"):
+    wl = WORKLOADS[workload]
+    return {"workload": wl["desc"] % (n >> 20), "grammar": wl["grammar"], "bytes": n,
+            "index": "i32" if wl["index32"] else "i64", "parallelism": "replicas x%d" % world,
             "l2": "input larger than L2 (no flush)"}
 
 
@@ -180,13 +200,14 @@ def reference_arm(a, rank, world):
 
     from oracle.ref import available
 
-    if not available(REF_CONFIG):
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/lib%s.so is not built" % REF_CONFIG}))
+    wl = WORKLOADS[a.workload]
+    if not available(wl["ref"]):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/lib%s.so is not built" % wl["ref"]}))
         return
     cores = os.cpu_count() or 1
     sample = a.ref_sample
     ctx = mp.get_context("spawn")
-    with ctx.Pool(cores, initializer=_pool_init, initargs=(sample,)) as pool:
+    with ctx.Pool(cores, initializer=_pool_init, initargs=(sample, a.workload)) as pool:
         pool.map(_pool_step, range(cores))  # load
         for _ in range(a.warmup):
             pool.map(_pool_step, range(cores))
@@ -200,7 +221,7 @@ def reference_arm(a, rank, world):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": 0, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": t / a.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-        "config": dict(workload_config(a.size, a.gpus),
+        "config": dict(workload_config(a.size or wl["size"], a.gpus, a.workload),
                        sample="each step: %d independent %d MiB documents of the same generator, one per host "
                               "core (the reference backend parses one document on one thread)" % (cores, sample >> 20)),
         "cpu_baseline": {"value": value, "unit": "GB/s", "cores": cores, "kind": "reference",
@@ -214,14 +235,13 @@ def reference_arm(a, rank, world):
 _POOL = {}
 
 
-def _pool_init(sample):
-    from alpacc_b200 import workloads as W
+def _pool_init(sample, workload="json"):
     from oracle.ref import RefOracle
     import numpy as np
 
     pid = os.getpid()
-    _POOL["doc"] = np.frombuffer(W.json_doc(sample, 2 + (pid % 97)), dtype=np.uint8)
-    _POOL["ref"] = RefOracle(REF_CONFIG)
+    _POOL["doc"] = np.frombuffer(make_doc(workload, sample, 2 + (pid % 97)), dtype=np.uint8)
+    _POOL["ref"] = RefOracle(WORKLOADS[workload]["ref"])
 
 
 def _pool_step(_):
@@ -238,10 +258,11 @@ def ours(a, rank, world, local_rank, dist):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    n = a.size
-    tables = load_tables(GRAMMAR, index32=True)
+    wl = WORKLOADS[a.workload]
+    n = a.size if a.size else wl["size"]
+    tables = load_tables(os.path.join(REPO, "grammars", wl["grammar"]), index32=wl["index32"])
     lay = wire.Layout.of(tables)
-    host = W.json_doc(n, 2 + rank)
+    host = make_doc(a.workload, n, 2 + rank)
     parser = Parser(tables, device=local_rank, max_input=n)
     d_in = torch.frombuffer(bytearray(host), dtype=torch.uint8).to(dev)
     ext = torch.cuda.ExternalStream(parser.stream_handle(), device=dev)
@@ -253,8 +274,8 @@ def ours(a, rank, world, local_rank, dist):
 
     for _ in range(a.warmup):
         rc, r = step()
-    if rc != 0:
-        raise SystemExit("warm-up parse did not accept the document (status %d)" % rc)
+    if rc != (1 if wl["reject"] else 0):
+        raise SystemExit("warm-up parse returned status %d on the %s workload" % (rc, a.workload))
     T, N = r.num_tokens, r.num_nodes
     info = parser.info()
     # ---- device-resident timing ----
@@ -316,7 +337,7 @@ def ours(a, rank, world, local_rank, dist):
         "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic (seeded JSON generator, one document per rank)",
-        "config": dict(workload_config(n, world), tokens=T, nodes=N, brackets=B, productions=P),
+        "config": dict(workload_config(n, world, a.workload), tokens=T, nodes=N, brackets=B, productions=P),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                      "algorithmic_bytes": kb, "ms": mean[dom]},
@@ -330,7 +351,8 @@ def ours(a, rank, world, local_rank, dist):
         "machine": info,
     }
     if not a.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sample(host, a.cpu_sample)
+        line["cpu_baseline"] = cpu_baseline_sample(host, a.cpu_sample, wl["ref"], a.workload,
+                                                   reps=2 if n > (512 << 20) else 4)
     print(json.dumps(line))
 
 
@@ -351,7 +373,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--size", type=int, default=256 << 20)
+    ap.add_argument("--size", type=int, default=0, help="input bytes (default: the workload's size)")
+    ap.add_argument("--workload", default="json", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-sample", type=int, default=256 << 20)
     ap.add_argument("--ref-sample", type=int, default=16 << 20)
     ap.add_argument("--no-cpu-baseline", action="store_true")

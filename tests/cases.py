@@ -131,7 +131,12 @@ def simple_json(n: int, seed: int) -> bytes:
     return doc + b" " * (n - len(doc))
 
 
-def case_inputs(config: str, sizes=(1, 7, 64, 1000, 15359, 15360, 15361, 40000), seeds=(0, 1)):
+# sizes around the lexer's tile geometry: tiles of 14880 new bytes after a
+# 480-byte halo, chunks of 60 bytes
+TILE_SIZES = (1, 7, 60, 61, 64, 1000, 14879, 14880, 14881, 15359, 15360, 15361, 29760, 29761, 40000)
+
+
+def case_inputs(config: str, sizes=TILE_SIZES, seeds=(0, 1)):
     """Fixed cases, generated documents of several sizes, and mutations."""
     f = family(config)
     out = list(FIXED[f])

@@ -60,10 +60,11 @@ def test_parity_golden_records(gpu, config):
 
 
 @pytest.mark.parametrize("config,n", [("json_ext_i32", 8 << 20), ("json_ext_i64", 3 << 20),
-                                      ("sexp_i64", 4 << 20), ("arithmetic_i32", 2 << 20)])
+                                      ("sexp_i64", 4 << 20), ("arithmetic_i32", 2 << 20),
+                                      ("json_ext_i32", 40 << 20)])
 def test_parity_large_vs_port(gpu, config, n):
-    """Multi-tile inputs (hundreds of lexer tiles, deep nesting) against the C
-    restatement oracle."""
+    """Multi-tile inputs (thousands of lexer tiles, deep nesting; 40 MiB spans
+    three host-to-device pieces) against the C restatement oracle."""
     from oracle.port import PortOracle
     data = cases.generated(config, n, 99)
     if config.startswith("sexp"):

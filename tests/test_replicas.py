@@ -71,6 +71,7 @@ def test_reference_arm_prints_only_on_rank_zero(capsys):
         steps = 1
         warmup = 0
         ref_sample = 1 << 20
+        workload = "json"
 
     bench.reference_arm(A, 1, 2)
     assert capsys.readouterr().out == ""
