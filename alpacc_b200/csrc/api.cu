@@ -23,6 +23,7 @@
 using namespace alpacc;
 
 #include "handle.h"
+#include "pipeline.h"
 
 namespace {
 
@@ -127,52 +128,7 @@ int ensure_lex_smem(size_t bytes) {
   return ALPACC_OK;
 }
 
-// Header of a pinned host result block; the arrays follow it. A result owns
-// two blocks: the token arrays (copied while the parser runs) and the tree
-// arrays (`second`).
-struct PinnedBlock {
-  alpacc_gpu_grammar *owner;
-  size_t size;
-  PinnedBlock *second;
-  size_t pad[5];
-};
-
 constexpr uint64_t kPieceTiles = (16u << 20) / kLexData;  // tiles per host-to-device piece (~16 MiB)
-
-// A pinned block of at least `total` bytes, from the handle's cache when it
-// is large enough.
-PinnedBlock *acquire_block(alpacc_gpu_grammar *g, void **cache, size_t *cache_size, size_t total) {
-  void *host = nullptr;
-  if (*cache && *cache_size >= total) {
-    host = *cache;
-    *cache = nullptr;
-  } else {
-    if (*cache) cudaFreeHost(*cache);
-    *cache = nullptr;
-    const size_t want = total + total / 8;
-    if (cudaMallocHost(&host, want) != cudaSuccess) {
-      cudaGetLastError();
-      return nullptr;
-    }
-    reinterpret_cast<PinnedBlock *>(host)->size = want;
-  }
-  PinnedBlock *b = reinterpret_cast<PinnedBlock *>(host);
-  b->owner = g;
-  b->second = nullptr;
-  return b;
-}
-
-void release_block(alpacc_gpu_grammar *g, PinnedBlock *b, bool tree) {
-  if (!b) return;
-  void **cache = tree ? &g->pinned_cache2 : &g->pinned_cache;
-  size_t *size = tree ? &g->pinned_cache2_size : &g->pinned_cache_size;
-  if (!*cache) {
-    *cache = b;
-    *size = b->size;
-  } else {
-    cudaFreeHost(b);
-  }
-}
 
 // Token arrays of the current host call: copied on cstream once the lexer
 // finished, overlapping the parser's kernels.
@@ -289,64 +245,8 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     CK(cudaMemsetAsync(g->lex_ticket.p, 0, 16 + pieces * 4, g->stream));
     CK(cudaMemsetAsync(g->st1_flag.p, 0, tiles * 4, g->stream));
     CK(cudaMemsetAsync(g->st2_flags.p, 0, tiles * 4, g->stream));
-    LexArgs a{};
-    a.in = d_in;
-    a.n = n;
-    a.num_tiles = tiles;
-    a.cls_id = (const uint8_t *)g->cls_id.p;
-    a.trans_words_ptr = (const uint32_t *)g->trans_words.p;
-    a.trans_words = g->trans_word_count;
-    a.copies = g->trans_rep;
-    a.lane_of = (const uint8_t *)g->lane_of.p;
-    a.img = (const uint8_t *)g->img.p;
-    a.img_cnt = (const uint8_t *)g->img_cnt.p;
-    a.img2 = lm.img2.empty() ? nullptr : (const unsigned long long *)g->img2.p;
-    a.sterm = (const uint8_t *)g->sterm.p;
-    a.sflags = (const uint8_t *)g->sflags.p;
-    a.M = lm.M;
-    a.C = lm.C;
-    a.dead = lm.dead;
-    a.m0 = lm.m0;
-    a.ignore = hg.ignore;
-    a.len_max = hg.len_max;
-    a.tok_ids = g->tok_ids.p;
-    a.tok_starts = g->tok_starts.p;
-    a.tok_lens = g->tok_lens.p;
-    a.term_w = term_w;
-    a.idx_w = idx_w;
-    a.len_w = len_w;
-    a.ticket = (unsigned *)g->lex_ticket.p;
-    a.st1_flag = (unsigned *)g->st1_flag.p;
-    a.st1_state = (uint8_t *)g->st1_state.p;
-    a.st1_vec = (uint8_t *)g->st1_vec.p;
-    a.st2 = PairTileState{(unsigned *)g->st2_flags.p, (unsigned long long *)g->st2_agg.p,
-                          (unsigned long long *)g->st2_inc.p};
-    a.status = g->d_status;
-    a.diag = g->diag;
-    a.stage_ids = (uint8_t *)g->stage_ids.p;
-    a.stage_starts = (uint32_t *)g->stage_starts.p;
-    a.stage_ends = (uint32_t *)g->stage_ends.p;
-    a.tile_cnt = (uint32_t *)g->tile_cnt.p;
-    a.tile_pos = (uint32_t *)g->tile_pos.p;
-    LexPlaceArgs pa{};
-    pa.num_tiles = tiles;
-    pa.tile_data = kLexData;
-    pa.n = n;
-    pa.tile_cnt = a.tile_cnt;
-    pa.tile_pos = a.tile_pos;
-    pa.tile_off = (unsigned long long *)g->tile_off.p;
-    pa.tile_prev = (uint32_t *)g->tile_prev.p;
-    pa.stage_ids = a.stage_ids;
-    pa.stage_starts = a.stage_starts;
-    pa.stage_ends = a.stage_ends;
-    pa.tok_ids = a.tok_ids;
-    pa.tok_starts = a.tok_starts;
-    pa.tok_lens = a.tok_lens;
-    pa.term_w = term_w;
-    pa.idx_w = idx_w;
-    pa.len_w = len_w;
-    pa.len_max = hg.len_max;
-    pa.status = g->d_status;
+    LexArgs a = lex_args(g, d_in, n, tiles);
+    const LexPlaceArgs pa = lex_place_args(g, a, tiles);
     stage_begin(g, 0);
     for (uint64_t k = 0; k < pieces; ++k) {
       const uint64_t tb = k * piece_tiles, te = std::min(tiles, tb + piece_tiles);
@@ -395,29 +295,10 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     CK(cudaMemsetAsync(g->pair_ticket.p, 0, 16, g->stream));
     CK(cudaMemsetAsync(g->pst_flags.p, 0, tiles * 4, g->stream));
     if (n == 0) CK(cudaMemsetAsync(&g->d_status->num_tokens, 0, 8, g->stream));
-    PairArgs a{};
-    a.tok_ids = g->tok_ids.p;
-    a.term_w = term_w;
-    a.num_tokens = &g->d_status->num_tokens;
+    PairArgs a = pair_args(g);
     a.num_tiles = tiles;
-    a.q = pt.q;
-    a.k = pt.k;
-    a.nt = pt.nt;
-    a.empty_t = (int)tb.empty_terminal;
-    a.start_t = (int)tb.start_terminal;
-    a.end_t = (int)tb.end_terminal;
-    a.dense = (const uint32_t *)g->dense.p;
-    a.rec = (const unsigned long long *)g->rec.p;
-    a.stacks = (const uint32_t *)g->stacks.p;
-    a.prods = (const uint32_t *)g->prods.p;
-    a.br_out = (uint32_t *)g->br.p;
-    a.pr_out = (uint32_t *)g->pr.p;
     a.br_cap = br_cap;
     a.pr_cap = pr_cap;
-    a.ticket = (unsigned *)g->pair_ticket.p;
-    a.st = PairTileState{(unsigned *)g->pst_flags.p, (unsigned long long *)g->pst_agg.p,
-                         (unsigned long long *)g->pst_inc.p};
-    a.status = g->d_status;
     stage_begin(g, 1);
     pair_kernel<<<(unsigned)tiles, kPairThreads, 0, g->stream>>>(a);
     ++g->launches;
@@ -455,32 +336,8 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     CK(cudaMemsetAsync(g->pse_flags.p, 0, tiles * 4, g->stream));
     CK(cudaMemsetAsync(g->queue_len.p, 0, 16, g->stream));
     CK(cudaMemsetAsync(g->super_min.p, 0x7f, ((tiles >> kPseSuperShift) + 1) * 4, g->stream));
-    PseArgs a{};
-    a.mode = mode;
-    a.elems = (const uint32_t *)(mode == kPseBrackets ? g->br.p : g->pr.p);
-    a.count = mode == kPseBrackets ? &g->d_status->num_brackets : &g->d_status->num_productions;
-    a.num_tokens = &g->d_status->num_tokens;
+    PseArgs a = pse_args(g, mode, Emax);
     a.num_tiles = tiles;
-    a.arity = (const int32_t *)g->arity.p;
-    a.is_term = (const uint8_t *)g->is_term.p;
-    a.num_prods = (int)pt.arity.size();
-    a.ch_h0 = (int32_t *)g->ch_h0.p;
-    a.ch_min = (int32_t *)g->chunk_min.p;
-    a.ch_tc = (int32_t *)g->ch_tc.p;
-    a.tile_min = (int32_t *)g->tile_min.p;
-    a.super_min = (int32_t *)g->super_min.p;
-    a.queue = (unsigned long long *)g->queue.p;
-    a.queue_cap = Emax;
-    a.queue_len = (unsigned long long *)g->queue_len.p;
-    a.node_prods = g->node_prods.p;
-    a.node_parents = g->node_parents.p;
-    a.token_parents = g->token_parents.p;
-    a.prod_w = prod_w;
-    a.idx_w = idx_w;
-    a.ticket = (unsigned *)g->pse_ticket.p;
-    a.st = PairTileState{(unsigned *)g->pse_flags.p, (unsigned long long *)g->pse_agg.p,
-                         (unsigned long long *)g->pse_inc.p};
-    a.status = g->d_status;
     stage_begin(g, 2 + 2 * mode);
     pse_tile_kernel<<<(unsigned)tiles, kPseThreads, 0, g->stream>>>(a);
     ++g->launches;
@@ -599,7 +456,8 @@ void alpacc_gpu_free(alpacc_gpu_grammar *g) {
                     &g->pse_flags, &g->pse_agg, &g->pse_inc, &g->ch_h0, &g->ch_tc, &g->tile_min,
                     &g->chunk_min, &g->super_min, &g->queue, &g->queue_len, &g->node_prods, &g->node_parents,
                     &g->token_parents, &g->stage_ids, &g->stage_starts, &g->stage_ends, &g->tile_cnt,
-                    &g->tile_pos, &g->tile_off, &g->tile_prev};
+                    &g->tile_pos, &g->tile_off, &g->tile_prev, &g->b_arrays, &g->b_desc, &g->b_status,
+                    &g->b_pack, &g->b_packed};
   for (DevBuf *b : bufs) release(*b);
   if (g->cstream) cudaStreamSynchronize(g->cstream);
   if (g->pinned_cache) cudaFreeHost(g->pinned_cache);
@@ -663,31 +521,20 @@ int alpacc_gpu_parse(alpacc_gpu_grammar *g, const uint8_t *in, uint64_t n, alpac
   return finish_host_result(g, out);
 }
 
-int alpacc_gpu_parse_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offsets, uint32_t count,
-                           alpacc_result *outs) {
-  if (!g || !offsets || !outs) return ALPACC_E_INVALID;
-  for (uint32_t i = 0; i < count; i++) {
-    const int64_t a = offsets[i], b = offsets[i + 1];
-    if (b < a) return ALPACC_E_INVALID;
-    int rc = alpacc_gpu_parse(g, bytes + a, (uint64_t)(b - a), &outs[i]);
-    if (rc < 0) return rc;
-    outs[i].valid = rc == ALPACC_OK ? 1 : 0;
-  }
-  return ALPACC_OK;
-}
-
 void alpacc_result_free(alpacc_result *r) {
   if (!r) return;
   if (r->internal) {
     PinnedBlock *b = reinterpret_cast<PinnedBlock *>(r->internal);
-    PinnedBlock *tree = b->second;
-    alpacc_gpu_grammar *g = b->owner;
-    if (g) {
-      release_block(g, b, false);
-      release_block(g, tree, true);
-    } else {
-      cudaFreeHost(b);
-      if (tree) cudaFreeHost(tree);
+    if (__atomic_sub_fetch(&b->refs, 1, __ATOMIC_ACQ_REL) <= 0) {  // the last result sharing this block
+      PinnedBlock *tree = b->second;
+      alpacc_gpu_grammar *g = b->owner;
+      if (g) {
+        release_block(g, b, false);
+        release_block(g, tree, true);
+      } else {
+        cudaFreeHost(b);
+        if (tree) cudaFreeHost(tree);
+      }
     }
   }
   std::memset(r, 0, sizeof(*r));
@@ -738,6 +585,51 @@ const char *alpacc_strerror(int status) {
 }
 
 double alpacc_gpu_last_ms(alpacc_gpu_grammar *g) { return g ? g->last_ms : -1.0; }
+
+int alpacc_gpu_autotune(alpacc_gpu_grammar *g, const uint8_t *d_sample, uint64_t n, int *choice) {
+  if (!g || (n > 0 && !d_sample)) return ALPACC_E_INVALID;
+  if (cudaSetDevice(g->device) != cudaSuccess) return ALPACC_E_CUDA;
+  const int keep = g->trans_rep;
+  const size_t per_copy = (size_t)g->trans_word_count * 4 + 512;
+  int best = keep;
+  double best_ms = -1.0;
+  for (int c = 1; c <= 32; c <<= 1) {
+    if ((size_t)c * per_copy > 64 * 1024) break;  // shared memory per CTA stays modest
+    g->trans_rep = c;
+    int per_sm = 0, sms = 0;
+    if (ensure_lex_smem(lex_smem_bytes(g)) != ALPACC_OK ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lex_kernel, kLexThreads, lex_smem_bytes(g)) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device) != cudaSuccess || per_sm < 1) {
+      cudaGetLastError();
+      continue;
+    }
+    g->lex_grid = per_sm * sms;
+    double ms = 0;
+    int ok = 1;
+    for (int rep = 0; rep < 3 && ok; ++rep) {  // first run warms up
+      const int rc = run_device(g, d_sample, n);
+      if (rc < 0) ok = 0;
+      else if (rep > 0) ms += g->stage_ms[0];
+    }
+    if (ok && (best_ms < 0 || ms < best_ms)) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  g->trans_rep = best;
+  int per_sm = 0, sms = 0;
+  if (ensure_lex_smem(lex_smem_bytes(g)) != ALPACC_OK ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lex_kernel, kLexThreads, lex_smem_bytes(g)) !=
+          cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device) != cudaSuccess || per_sm < 1) {
+    cudaGetLastError();
+    return ALPACC_E_CUDA;
+  }
+  g->lex_grid = per_sm * sms;
+  if (choice) *choice = best;
+  return best_ms < 0 ? ALPACC_E_CUDA : ALPACC_OK;
+}
 
 void *alpacc_gpu_stream(alpacc_gpu_grammar *g) { return g ? (void *)g->stream : nullptr; }
 

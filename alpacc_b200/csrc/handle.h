@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -84,8 +85,11 @@ struct alpacc_gpu_grammar {
   DevBuf pair_ticket, pst_flags, pst_agg, pst_inc, br, pr;
   DevBuf pse_ticket, pse_flags, pse_agg, pse_inc, ch_h0, ch_tc, tile_min, chunk_min, super_min, queue, queue_len;
   DevBuf node_prods, node_parents, token_parents;
+  // batches: descriptor arrays, per-document statuses, packing ranges, packed results
+  DevBuf b_arrays, b_desc, b_status, b_pack, b_packed;
   // pinned host result buffers kept for reuse (released results come back
   // here): the token arrays' block and the tree arrays' block
+  std::mutex cache_mu;  // results may be released from other threads than the one parsing
   void *pinned_cache = nullptr;
   size_t pinned_cache_size = 0;
   void *pinned_cache2 = nullptr;
@@ -106,6 +110,61 @@ struct alpacc_gpu_grammar {
   int last_status = ALPACC_E_INVALID;
   std::string last_error;
 };
+
+// Header of a pinned host result block; the arrays follow it. A single
+// document's result owns two blocks (the token arrays, copied while the parser
+// runs, and the tree arrays in `second`); the results of a batch share one
+// block, released when the last of them is (`refs`).
+struct PinnedBlock {
+  alpacc_gpu_grammar *owner;
+  size_t size;
+  PinnedBlock *second;
+  int refs;
+  int pad0;
+  size_t pad[4];
+};
+
+// A pinned block of at least `total` bytes, from the handle's cache when it
+// is large enough.
+inline PinnedBlock *acquire_block(alpacc_gpu_grammar *g, void **cache, size_t *cache_size, size_t total) {
+  void *host = nullptr;
+  void *stale = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g->cache_mu);
+    if (*cache && *cache_size >= total) host = *cache;
+    else stale = *cache;
+    *cache = nullptr;
+  }
+  if (!host) {
+    if (stale) cudaFreeHost(stale);
+    const size_t want = total + total / 8;
+    if (cudaMallocHost(&host, want) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    reinterpret_cast<PinnedBlock *>(host)->size = want;
+  }
+  PinnedBlock *b = reinterpret_cast<PinnedBlock *>(host);
+  b->owner = g;
+  b->second = nullptr;
+  b->refs = 1;
+  return b;
+}
+
+inline void release_block(alpacc_gpu_grammar *g, PinnedBlock *b, bool tree) {
+  if (!b) return;
+  void **cache = tree ? &g->pinned_cache2 : &g->pinned_cache;
+  size_t *size = tree ? &g->pinned_cache2_size : &g->pinned_cache_size;
+  {
+    std::lock_guard<std::mutex> lock(g->cache_mu);
+    if (!*cache) {
+      *cache = b;
+      *size = b->size;
+      return;
+    }
+  }
+  cudaFreeHost(b);
+}
 
 // Dynamic shared memory of lex_kernel for this handle's tables.
 inline size_t lex_dyn_smem(const alpacc_gpu_grammar *g) {

@@ -8,6 +8,44 @@
 
 namespace alpacc {
 
+// ---- batches: many independent documents through one launch per stage ----
+// Each stage's tiles form one virtual tile space in which document d owns
+// tiles [tile0[d], tile0[d+1]); a ticketed tile is mapped to (document, local
+// tile) by binary search. Per-document data lives in per-document regions of
+// every array and each document has its own status, so documents never see
+// each other: each behaves exactly as if it had been parsed alone.
+struct BatchDesc {
+  int docs;
+  const unsigned long long *in_off;   // [docs] byte offset of document d in the input
+  const unsigned long long *n;        // [docs] bytes of document d
+  const unsigned long long *tok_off;  // [docs+1] token region (capacity n_d + 1)
+  const unsigned long long *br_off;   // [docs+1] bracket region (capacity (n_d + 3) * max brackets per position)
+  const unsigned long long *pr_off;   // [docs+1] production and tree-node region
+  const unsigned long long *lex_tile0;  // [docs+1] lexer tiles (host: from n_d)
+  unsigned long long *pair_tile0;       // [docs+1] pair tiles (planned on the device from T_d)
+  unsigned long long *br_tile0;         // [docs+1] bracket-walk tiles (from B_d)
+  unsigned long long *pr_tile0;         // [docs+1] parent-walk tiles (from P_d)
+  DeviceStatus *status;                 // [docs]
+};
+
+// Document owning virtual tile vt: the last d with tile0[d] <= vt (documents
+// without tiles share their successor's tile0 and are skipped by the search).
+__device__ __forceinline__ int batch_doc(const unsigned long long *tile0, int docs, unsigned long long vt) {
+  int lo = 0, hi = docs;  // answer in [lo, hi)
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (tile0[mid] <= vt) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Per-document tile counts of the next stage from the counts the previous
+// stage left in each document's status (one CTA): tile0[d] = sum over earlier
+// documents of ceil((count_d + extra) / tile).
+enum PlanKind : int { kPlanPairs = 0, kPlanBrackets = 1, kPlanParents = 2 };
+__global__ void batch_plan_kernel(BatchDesc b, int kind, unsigned long long *tile0, unsigned long long tile);
+
 // ---- lexer tiles: 256 chunks x 15 words (60 bytes); the first 8 chunks are
 // a halo repeating the end of the previous tile ----
 constexpr int kLexThreads = 256;
@@ -55,6 +93,7 @@ struct LexArgs {
   uint8_t *stage_ids;
   uint32_t *stage_starts, *stage_ends;
   uint32_t *tile_cnt, *tile_pos;
+  const BatchDesc *batch;  // null: one document (in, n, status); else tiles are virtual (lex_tile0)
 };
 
 __global__ void lex_kernel(LexArgs args);
@@ -72,6 +111,7 @@ struct LexPlaceArgs {
   int term_w, idx_w, len_w;
   unsigned long long len_max;
   DeviceStatus *status;
+  const BatchDesc *batch;  // null: one document; else counts restart at each document's first tile
 };
 
 constexpr int kLexScanThreads = 1024;
@@ -101,6 +141,7 @@ struct PairArgs {
   unsigned *ticket;
   PairTileState st;         // (brackets, productions)
   DeviceStatus *status;
+  const BatchDesc *batch;   // null: one document; else virtual tiles (pair_tile0) and per-document regions
 };
 
 __global__ void pair_kernel(PairArgs args);
@@ -141,6 +182,7 @@ struct PseArgs {
   unsigned *ticket;
   PairTileState st;                 // (sum of steps, terminal count)
   DeviceStatus *status;
+  const BatchDesc *batch;           // null: one document; else virtual tiles (br_tile0 / pr_tile0)
 };
 
 __global__ void pse_tile_kernel(PseArgs args);

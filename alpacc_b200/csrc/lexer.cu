@@ -120,14 +120,13 @@ struct CntPosOp {
 
 }  // namespace
 
-__global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
+__global__ void __launch_bounds__(kLexThreads, 6) lex_kernel(LexArgs args) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   __shared__ __align__(16) LexSmem sm_static;
   LexSmem *sm = &sm_static;
   const LexArgs &a = args;
   const int t = threadIdx.x;
   const int lane = t & 31;
-  DeviceStatus *st = a.status;
   const int copies = a.copies;
 
   // ---- tables, once per CTA ----
@@ -142,13 +141,12 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
   }
   const Tabs tb{s_cls, s_trans, copies, lane & (copies - 1)};
   const int dead = a.dead;
-  const long long n = (long long)a.n;
   const unsigned long long num_tiles = a.num_tiles;
   const unsigned long long tile_end = a.tile_end ? a.tile_end : num_tiles;
 
   for (unsigned long long round = 0;; ++round) {
     if (round > tile_end - a.tile_begin) {  // every round takes a new ticket: cannot happen
-      if (t == 0) record_timeout(st, kSiteLexTiles);
+      if (t == 0) record_timeout(a.status, kSiteLexTiles);
       break;
     }
     __syncthreads();  // tables ready / previous tile fully consumed
@@ -156,12 +154,27 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
     __syncthreads();
     const unsigned long long tile = a.tile_begin + sm->tile;
     if (tile >= tile_end) break;
-    const long long data0 = (long long)tile * kLexData;
+    // this tile's document: the whole input, or one document of a batch
+    // (virtual tile `tile` is local tile `lt` of `tiles_t`)
+    const uint8_t *in_base = a.in;
+    long long n = (long long)a.n;
+    unsigned long long lt = tile, tiles_t = num_tiles;
+    DeviceStatus *st = a.status;
+    if (a.batch) {
+      const BatchDesc &b = *a.batch;
+      const int d = batch_doc(b.lex_tile0, b.docs, tile);
+      lt = tile - b.lex_tile0[d];
+      tiles_t = b.lex_tile0[d + 1] - b.lex_tile0[d];
+      in_base = a.in + b.in_off[d];
+      n = (long long)b.n[d];
+      st = b.status + d;
+    }
+    const long long data0 = (long long)lt * kLexData;
     const long long load0 = data0 - (long long)kLexHalo * kLexChunk;
 
     // ---- load halo + data ----
     {
-      const uint8_t *in = a.in;
+      const uint8_t *in = in_base;
       uint8_t *dst = reinterpret_cast<uint8_t *>(sm->bytes);
       const bool aligned = ((reinterpret_cast<uintptr_t>(in) & 15) == 0);
       for (int v = t; v < kLexLoad / 16; v += kLexThreads) {
@@ -315,7 +328,7 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
         st_release_u32(a.st1_flag + tile, 2u);
         sm->out_published = 1;
       }
-    } else if (tile + 1 < num_tiles) {
+    } else if (lt + 1 < tiles_t) {
       // no constant chunk at all: publish the data region's transition vector
       for (int s = t; s < a.M; s += kLexThreads) {
         int x = s;
@@ -333,11 +346,12 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
       if (t == 0) {
         if (a.diag) atomicAdd(&st->scratch[0], 1ull);
         int s_in = a.m0;
-        if (tile > 0) {
+        if (lt > 0) {
           long long j = (long long)tile - 1;
+          const long long jfirst = (long long)(tile - lt);  // the document's first tile
           int base_state = a.m0;
           bool have = false;
-          while (j >= 0) {
+          while (j >= jfirst) {
             const unsigned f = wait_flag(a.st1_flag + j, 1u, st, kSiteLexState);
             if (f == 0) break;
             if (f >= 2) {
@@ -347,7 +361,7 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
             }
             --j;
           }
-          if (!have) j = -1;
+          if (!have) j = jfirst - 1;
           int x = have ? base_state : a.m0;
           for (long long jj = j + 1; jj < (long long)tile; ++jj) {
             if (x == dead || x < 0) break;
@@ -460,7 +474,7 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
     if (t < kWarp) {
       const Pair64 agg{cnt_tot, pos_tot};
       Pair64 prefix{0, 0};
-      if (tile > 0) {
+      if (lt > 0) {
         if (t == 0) publish_pair(a.st2, (long long)tile, agg, false);
         prefix = warp_lookback_pair(a.st2, (long long)tile, Pair64{0, 0}, CntPosOp(), st, kSiteLexCount);
       }
@@ -469,7 +483,7 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
         publish_pair(a.st2, (long long)tile, inc, true);
         sm->cnt_prefix = prefix.a;
         sm->pos_prefix = prefix.b;
-        if (tile + 1 == num_tiles) st->num_tokens = (unsigned long long)inc.a;
+        if (lt + 1 == tiles_t) st->num_tokens = (unsigned long long)inc.a;
       }
     }
     __syncthreads();
@@ -511,36 +525,76 @@ __global__ void __launch_bounds__(kLexThreads) lex_kernel(LexArgs args) {
 // ---------------------------------------------------------------------------
 
 // Exclusive (count, last boundary) prefix over the tiles, by one CTA; also the
-// total token count.
+// total token count. In a batch the prefix restarts at each document's first
+// tile (a segmented scan: the flag bit kSeg marks a segment start) and the
+// offsets are placed in the document's token region.
+constexpr long long kSeg = 1ll << 62;
+
+struct SegCntPosOp {
+  __device__ Pair64 operator()(Pair64 l, Pair64 r) const {
+    if (r.b & kSeg) return r;
+    const long long lp = l.b & ~kSeg;
+    return Pair64{l.a + r.a, (lp > r.b ? lp : r.b) | (l.b & kSeg)};
+  }
+};
+
 __global__ void __launch_bounds__(kLexScanThreads) lex_scan_kernel(LexPlaceArgs a) {
   __shared__ Pair64 tmp[kLexScanThreads / 32];
   const int t = threadIdx.x;
   constexpr int kPer = 16;
+  const BatchDesc *bd = a.batch;
+  // segment start of tile i (a batch document's first tile) and its document
+  auto seg_doc = [&](unsigned long long i, bool *start) -> int {
+    if (!bd) {
+      *start = i == 0;
+      return 0;
+    }
+    const int d = batch_doc(bd->lex_tile0, bd->docs, i);
+    *start = bd->lex_tile0[d] == i;
+    return d;
+  };
   Pair64 carry{0, 0};
   for (unsigned long long base = 0; base < a.num_tiles; base += (unsigned long long)kLexScanThreads * kPer) {
     const unsigned long long i0 = base + (unsigned long long)t * kPer;
     Pair64 loc{0, 0};
-    for (int k = 0; k < kPer && i0 + k < a.num_tiles; ++k)
-      loc = CntPosOp()(loc, Pair64{(long long)a.tile_cnt[i0 + k], (long long)a.tile_pos[i0 + k]});
-    Pair64 tot;
-    const Pair64 ex = block_exclusive_scan_pair(loc, CntPosOp(), Pair64{0, 0}, tmp, &tot);
-    Pair64 run = CntPosOp()(carry, ex);
     for (int k = 0; k < kPer && i0 + k < a.num_tiles; ++k) {
-      a.tile_off[i0 + k] = (unsigned long long)run.a;
-      a.tile_prev[i0 + k] = (uint32_t)run.b;
-      run = CntPosOp()(run, Pair64{(long long)a.tile_cnt[i0 + k], (long long)a.tile_pos[i0 + k]});
+      bool start;
+      seg_doc(i0 + k, &start);
+      const Pair64 v{(long long)a.tile_cnt[i0 + k], (long long)a.tile_pos[i0 + k] | (start ? kSeg : 0)};
+      loc = SegCntPosOp()(loc, v);
     }
-    carry = CntPosOp()(carry, tot);
+    Pair64 tot;
+    const Pair64 ex = block_exclusive_scan_pair(loc, SegCntPosOp(), Pair64{0, 0}, tmp, &tot);
+    Pair64 run = SegCntPosOp()(carry, ex);
+    for (int k = 0; k < kPer && i0 + k < a.num_tiles; ++k) {
+      bool start;
+      const int d = seg_doc(i0 + k, &start);
+      if (start) run = Pair64{0, 0};
+      const unsigned long long region = bd ? bd->tok_off[d] : 0;
+      a.tile_off[i0 + k] = region + (unsigned long long)run.a;
+      a.tile_prev[i0 + k] = (uint32_t)(run.b & ~kSeg);
+      run = Pair64{run.a + (long long)a.tile_cnt[i0 + k],
+                   ((run.b & ~kSeg) > (long long)a.tile_pos[i0 + k] ? (run.b & ~kSeg) : (long long)a.tile_pos[i0 + k])};
+      // the document's token count, at its last tile
+      if (bd && i0 + k + 1 == bd->lex_tile0[d + 1]) bd->status[d].num_tokens = (unsigned long long)run.a;
+    }
+    carry = SegCntPosOp()(carry, tot);
   }
-  if (t == 0) a.status->num_tokens = (unsigned long long)carry.a;
+  if (t == 0 && !bd) a.status->num_tokens = (unsigned long long)(carry.a);
 }
 
 // Each CTA copies whole tiles' staged tokens to their final places; a token
 // whose start lies before its tile takes the last boundary before the tile.
 __global__ void __launch_bounds__(256) lex_place_kernel(LexPlaceArgs a) {
-  DeviceStatus *st = a.status;
   bool too_long = false;
+  DeviceStatus *st = a.status;
   for (unsigned long long tile = blockIdx.x; tile < a.num_tiles; tile += gridDim.x) {
+    DeviceStatus *sd = a.batch ? a.batch->status + batch_doc(a.batch->lex_tile0, a.batch->docs, tile) : a.status;
+    if (sd != st) {
+      if (too_long) record_reject(st, &st->lex_reject_reason, 3);
+      too_long = false;
+      st = sd;
+    }
     const unsigned c = a.tile_cnt[tile];
     const unsigned long long off = a.tile_off[tile];
     const uint32_t prev = a.tile_prev[tile];

@@ -68,15 +68,38 @@ __global__ void __launch_bounds__(kPairThreads, 5) pair_kernel(PairArgs a) {
   __shared__ __align__(16) uint16_t s_cnt[kPairTile];    // brackets | productions << 8
   __shared__ __align__(16) uint32_t s_out[kPairOut];     // output window
   const int t = threadIdx.x;
-  DeviceStatus *st = a.status;
+  const int L = a.q + a.k;
+  for (;;) {
+  __syncthreads();  // the previous tile's shared data is consumed
   if (t == 0) s_tile = atomicAdd(a.ticket, 1u);
   __syncthreads();
-  const unsigned long long tile = s_tile;
-  const long long T = (long long)*a.num_tokens;
+  const unsigned long long tile = s_tile;  // virtual tile in a batch
+  const unsigned long long total = a.batch ? a.batch->pair_tile0[a.batch->docs] : a.num_tiles;
+  if (tile >= total) break;
+  // this tile's document
+  unsigned long long lt = tile;
+  const void *tok_ids = a.tok_ids;
+  uint32_t *br_base = a.br_out, *pr_base = a.pr_out;
+  unsigned long long br_cap = a.br_cap, pr_cap = a.pr_cap;
+  DeviceStatus *st = a.status;
+  long long T;
+  if (a.batch) {
+    const BatchDesc &b = *a.batch;
+    const int d = batch_doc(b.pair_tile0, b.docs, tile);
+    lt = tile - b.pair_tile0[d];
+    st = b.status + d;
+    T = (long long)st->num_tokens;
+    tok_ids = static_cast<const uint8_t *>(a.tok_ids) + b.tok_off[d] * (unsigned long long)a.term_w;
+    br_base = a.br_out + b.br_off[d];
+    pr_base = a.pr_out + b.pr_off[d];
+    br_cap = b.br_off[d + 1] - b.br_off[d];
+    pr_cap = b.pr_off[d + 1] - b.pr_off[d];
+  } else {
+    T = (long long)*a.num_tokens;
+  }
   const long long m = T + 2;
-  const long long tile0 = (long long)tile * kPairTile;
-  if (tile0 >= m) return;  // beyond the data: nobody waits on this tile
-  const int L = a.q + a.k;
+  const long long tile0 = (long long)lt * kPairTile;
+  if (tile0 >= m) continue;  // beyond the data: nobody waits on this tile
 
   // ---- terminals of positions tile0 - q .. tile0 + kPairTile + k - 2 ----
   for (int i = t; i < kPairTile + L - 1; i += kPairThreads) {
@@ -85,7 +108,7 @@ __global__ void __launch_bounds__(kPairThreads, 5) pair_kernel(PairArgs a) {
     if (pos < 0 || pos >= m) term = a.empty_t;
     else if (pos == 0) term = a.start_t;
     else if (pos == m - 1) term = a.end_t;
-    else term = (int)load_uint(a.tok_ids, (unsigned long long)(pos - 1), a.term_w);
+    else term = (int)load_uint(tok_ids, (unsigned long long)(pos - 1), a.term_w);
     s_term[i] = (unsigned)term < (unsigned)a.nt ? (uint16_t)term : (uint16_t)0xffff;
   }
   __syncthreads();
@@ -132,7 +155,7 @@ __global__ void __launch_bounds__(kPairThreads, 5) pair_kernel(PairArgs a) {
   if (t < kWarp) {
     const Pair64 agg{tb, tp};
     Pair64 prefix{0, 0};
-    if (tile > 0) {
+    if (lt > 0) {
       if (t == 0) publish_pair(a.st, (long long)tile, agg, false);
       prefix = warp_lookback_pair(a.st, (long long)tile, Pair64{0, 0}, AddPair(), st, kSitePairs);
     }
@@ -149,16 +172,16 @@ __global__ void __launch_bounds__(kPairThreads, 5) pair_kernel(PairArgs a) {
   }
   __syncthreads();
   const long long pre_b = s_prefix_b, pre_p = s_prefix_p;
-  if ((unsigned long long)(pre_b + tb) > a.br_cap || (unsigned long long)(pre_p + tp) > a.pr_cap) {
+  if ((unsigned long long)(pre_b + tb) > br_cap || (unsigned long long)(pre_p + tp) > pr_cap) {
     if (t == 0) atomicCAS(&st->error, 0, -4 /* ALPACC_E_CAPACITY */);
-    return;
+    continue;
   }
   // ---- brackets (pass 0) and productions (pass 1) through the output window ----
   for (int pass = 0; pass < 2; ++pass) {
     const long long total = pass == 0 ? tb : tp;
     const long long base = pass == 0 ? (ex >> 32) : (ex & 0xffffffffll);
     const uint32_t *src = pass == 0 ? a.stacks : a.prods;
-    uint32_t *dst = pass == 0 ? a.br_out + pre_b : a.pr_out + pre_p;
+    uint32_t *dst = pass == 0 ? br_base + pre_b : pr_base + pre_p;
     for (long long w0 = 0; w0 < total; w0 += kPairOut) {
       long long o = base;
 #pragma unroll
@@ -179,6 +202,7 @@ __global__ void __launch_bounds__(kPairThreads, 5) pair_kernel(PairArgs a) {
       __syncthreads();
     }
   }
+  }  // tiles
 }
 
 // ---------------------------------------------------------------------------
@@ -211,16 +235,55 @@ constexpr int kPseSmemProds = 1024;  // production tables copied to shared memor
 // compact_tree's output for production e (parser.c:126-153): terminal
 // productions give their token's parent, the others a tree node; parents are
 // renumbered by subtracting the terminal productions before them.
-__device__ __forceinline__ void emit_node(const PseArgs &a, uint32_t prod, bool term, long long e, long long tinc_e,
-                                          long long p_new, long long T) {
+// One document's view of the walk's arrays (a batch document, or the input).
+struct PseDoc {
+  const uint32_t *elems;
+  long long E, T;
+  unsigned long long tile_first;  // virtual index of the document's first tile
+  void *node_prods, *node_parents, *token_parents;
+  DeviceStatus *st;
+};
+
+__device__ __forceinline__ PseDoc pse_doc(const PseArgs &a, unsigned long long vt, int *doc) {
+  PseDoc v;
+  if (!a.batch) {
+    *doc = 0;
+    v.elems = a.elems;
+    v.E = (long long)*a.count;
+    v.T = (long long)*a.num_tokens;
+    v.tile_first = 0;
+    v.node_prods = a.node_prods;
+    v.node_parents = a.node_parents;
+    v.token_parents = a.token_parents;
+    v.st = a.status;
+    return v;
+  }
+  const BatchDesc &b = *a.batch;
+  const bool parents = a.mode == kPseParents;
+  const unsigned long long *tile0 = parents ? b.pr_tile0 : b.br_tile0;
+  const int d = batch_doc(tile0, b.docs, vt);
+  *doc = d;
+  v.st = b.status + d;
+  v.E = (long long)(parents ? v.st->num_productions : v.st->num_brackets);
+  v.T = (long long)v.st->num_tokens;
+  v.elems = a.elems + (parents ? b.pr_off[d] : b.br_off[d]);
+  v.tile_first = tile0[d];
+  v.node_prods = static_cast<uint8_t *>(a.node_prods) + b.pr_off[d] * (unsigned long long)a.prod_w;
+  v.node_parents = static_cast<uint8_t *>(a.node_parents) + b.pr_off[d] * (unsigned long long)a.idx_w;
+  v.token_parents = static_cast<uint8_t *>(a.token_parents) + b.tok_off[d] * (unsigned long long)a.idx_w;
+  return v;
+}
+
+__device__ __forceinline__ void emit_node(const PseArgs &a, const PseDoc &dv, uint32_t prod, bool term, long long e,
+                                          long long tinc_e, long long p_new) {
   if (term) {
-    if (tinc_e >= 1 && tinc_e <= T)
-      store_uint(a.token_parents, (unsigned long long)(tinc_e - 1), a.idx_w, (unsigned long long)p_new);
+    if (tinc_e >= 1 && tinc_e <= dv.T)
+      store_uint(dv.token_parents, (unsigned long long)(tinc_e - 1), a.idx_w, (unsigned long long)p_new);
   } else {
     const long long o = e - tinc_e;
     if (o >= 0) {
-      store_uint(a.node_prods, (unsigned long long)o, a.prod_w, prod);
-      store_uint(a.node_parents, (unsigned long long)o, a.idx_w, (unsigned long long)p_new);
+      store_uint(dv.node_prods, (unsigned long long)o, a.prod_w, prod);
+      store_uint(dv.node_parents, (unsigned long long)o, a.idx_w, (unsigned long long)p_new);
     }
   }
 }
@@ -241,8 +304,6 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   const int t = threadIdx.x;
   const int lane = t & (kWarp - 1);
   const int warp = t >> 5;
-  DeviceStatus *st = a.status;
-  if (t == 0) s_tile = atomicAdd(a.ticket, 1u);
   const bool parents = a.mode == kPseParents;
   const bool prod_smem = parents && a.num_prods <= kPseSmemProds;
   if (prod_smem)
@@ -250,23 +311,34 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
       s_arity[i] = __ldg(a.arity + i);
       s_is_term[i] = __ldg(a.is_term + i);
     }
+  const unsigned long long total =
+      !a.batch ? a.num_tiles : (parents ? a.batch->pr_tile0 : a.batch->br_tile0)[a.batch->docs];
+  for (;;) {
+  __syncthreads();  // the previous tile's shared data is consumed
+  if (t == 0) s_tile = atomicAdd(a.ticket, 1u);
   __syncthreads();
-  const unsigned long long tile = s_tile;
-  const long long E = (long long)*a.count;
-  const long long tile0 = (long long)tile * kPseTile;
-  if (tile0 >= E) return;
+  const unsigned long long tile = s_tile;  // virtual tile in a batch
+  if (tile >= total) break;
+  int doc;
+  const PseDoc dv = pse_doc(a, tile, &doc);
+  DeviceStatus *st = dv.st;
+  const long long E = dv.E;
+  const unsigned long long lt = tile - dv.tile_first;
+  const long long tile0 = (long long)lt * kPseTile;  // elements are indexed within the document
+  if (tile0 >= E) continue;
   const long long c0 = tile0 + (long long)t * kPseItems;  // first element of this thread's chunk
 
   // ---- load ----
   uint32_t v[kPseItems];
-  if (c0 + kPseItems <= E) {
-    const uint4 x0 = __ldg(reinterpret_cast<const uint4 *>(a.elems + c0));
-    const uint4 x1 = __ldg(reinterpret_cast<const uint4 *>(a.elems + c0) + 1);
+  const bool vec = ((reinterpret_cast<uintptr_t>(dv.elems + c0) & 15) == 0);
+  if (c0 + kPseItems <= E && vec) {
+    const uint4 x0 = __ldg(reinterpret_cast<const uint4 *>(dv.elems + c0));
+    const uint4 x1 = __ldg(reinterpret_cast<const uint4 *>(dv.elems + c0) + 1);
     v[0] = x0.x; v[1] = x0.y; v[2] = x0.z; v[3] = x0.w;
     v[4] = x1.x; v[5] = x1.y; v[6] = x1.z; v[7] = x1.w;
   } else {
 #pragma unroll
-    for (int j = 0; j < kPseItems; ++j) v[j] = c0 + j < E ? a.elems[c0 + j] : 0u;
+    for (int j = 0; j < kPseItems; ++j) v[j] = c0 + j < E ? dv.elems[c0 + j] : 0u;
   }
 
   // ---- local steps, one packed scan ----
@@ -295,7 +367,7 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   const long long tot_t = tot & 0xffffffffll;
   const long long tot_s = (tot - tot_t) >> 32;
   // publish the aggregate at once; tile 0's aggregate is its inclusive prefix
-  if (t == 0) publish_pair(a.st, (long long)tile, Pair64{tot_s, tot_t}, tile == 0);
+  if (t == 0) publish_pair(a.st, (long long)tile, Pair64{tot_s, tot_t}, lt == 0);
 
   // ---- relative depths, chunk minimum, warp windows ----
   int cmin = INT_MAX;
@@ -430,7 +502,7 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
 #pragma unroll
       for (int j = 0; j < kPseItems; ++j)
         if (ans[j] == -1) {
-          if (qi < a.queue_cap) a.queue[qi] = (unsigned long long)(c0 + j);
+          if (qi < a.queue_cap) a.queue[qi] = ((unsigned long long)doc << 40) | (unsigned long long)(c0 + j);
           else atomicCAS(&st->error, 0, -4 /* ALPACC_E_CAPACITY */);
           ++qi;
         }
@@ -440,18 +512,17 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   // ---- the tile's prefix: look-back by warp 0, now that predecessors had time ----
   if (t < kWarp) {
     Pair64 prefix{0, 0};
-    if (tile > 0) prefix = warp_lookback_pair(a.st, (long long)tile, Pair64{0, 0}, AddPair(), st, kSitePse);
+    if (lt > 0) prefix = warp_lookback_pair(a.st, (long long)tile, Pair64{0, 0}, AddPair(), st, kSitePse);
     if (t == 0) {
       const Pair64 inc{prefix.a + tot_s, prefix.b + tot_t};
-      if (tile > 0) publish_pair(a.st, (long long)tile, inc, true);
+      if (lt > 0) publish_pair(a.st, (long long)tile, inc, true);
       sm.prefix_a = prefix.a;
       sm.prefix_b = prefix.b;
       if (tile0 + kPseTile >= E) {  // last tile: global checks
         if (!parents) {
           if (inc.a != 0) record_reject(st, &st->parse_reject_reason, 3);
         } else {
-          const long long T = (long long)*a.num_tokens;
-          if (inc.b != T) record_reject(st, &st->parse_reject_reason, 4);
+          if (inc.b != dv.T) record_reject(st, &st->parse_reject_reason, 4);
           st->num_nodes = (unsigned long long)(E - inc.b);
         }
       }
@@ -475,20 +546,20 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
     atomicMin(a.super_min + (tile >> kPseSuperShift), tm);
   }
   if (parents) {
-    const long long T = (long long)*a.num_tokens;
 #pragma unroll
     for (int j = 0; j < kPseItems; ++j) {
       const int an = ans[j];
       const bool term = tcr[j] != (j > 0 ? tcr[j - 1] : 0);
       if (an == -3) {  // the root: compute_parents gives it parent 0
-        emit_node(a, v[j], term, c0 + j, pb + ex_t + tcr[j], 0 - (pb + sm.tc[0]), T);
+        emit_node(a, dv, v[j], term, c0 + j, pb + ex_t + tcr[j], 0 - (pb + sm.tc[0]));
       } else if (an >= 0) {
         const long long p = tile0 + an;
         const long long tinc_p = pb + sm.tc[(an / kPseItems) * kPseStride + an % kPseItems];
-        emit_node(a, v[j], term, c0 + j, pb + ex_t + tcr[j], p - tinc_p, T);
+        emit_node(a, dv, v[j], term, c0 + j, pb + ex_t + tcr[j], p - tinc_p);
       }
     }
   }
+  }  // tiles
 }
 
 namespace {
@@ -506,13 +577,15 @@ __device__ __forceinline__ long long warp_latest_le(const int32_t *arr, long lon
   return -1;
 }
 
-// Depth before each element of chunk c, for lanes 0..7 (lane l: element
-// c * 8 + l); other lanes and elements past the end get INT_MAX.
-__device__ __forceinline__ int32_t chunk_depth(const PseArgs &a, long long c, long long E, int lane) {
-  const long long e = c * kPseItems + lane;
-  const bool ok = lane < kPseItems && e < E;
-  int stp = ok ? pse_step(a, a.elems[e]) : 0;
-  const int32_t h0 = a.ch_h0[c];
+// Depth before each element of a chunk, for lanes 0..7 (lane l: element
+// eb + l of the document, the chunk's state at virtual chunk index cc); other
+// lanes and elements past the end get INT_MAX.
+__device__ __forceinline__ int32_t chunk_depth(const PseArgs &a, const PseDoc &dv, long long cc, long long eb,
+                                               int lane) {
+  const long long e = eb + lane;
+  const bool ok = lane < kPseItems && e < dv.E;
+  int stp = ok ? pse_step(a, dv.elems[e]) : 0;
+  const int32_t h0 = a.ch_h0[cc];
 #pragma unroll
   for (int d = 1; d < kPseItems; d <<= 1) {
     const int o = __shfl_up_sync(0xffffffffu, stp, d);
@@ -522,61 +595,103 @@ __device__ __forceinline__ int32_t chunk_depth(const PseArgs &a, long long c, lo
   return ok ? h0 + (lane > 0 ? excl : 0) : INT_MAX;
 }
 
-// Inclusive terminal-production count up to element x (warp-wide call).
-__device__ __forceinline__ long long terminal_count(const PseArgs &a, long long x, int lane) {
+// Inclusive terminal-production count up to element x of the document (warp-wide call).
+__device__ __forceinline__ long long terminal_count(const PseArgs &a, const PseDoc &dv, long long x, int lane) {
   const long long c = x / kPseItems;
   const long long e = c * kPseItems + lane;
-  const bool t = lane <= (int)(x - c * kPseItems) && __ldg(a.is_term + a.elems[e < x ? e : x]);
-  return (long long)a.ch_tc[c] + __popc(__ballot_sync(0xffffffffu, t));
+  const bool t = lane <= (int)(x - c * kPseItems) && __ldg(a.is_term + dv.elems[e < x ? e : x]);
+  return (long long)a.ch_tc[(long long)dv.tile_first * kPseThreads + c] + __popc(__ballot_sync(0xffffffffu, t));
 }
 
 }  // namespace
 
-// One warp per queued query: latest tile whose minimum is <= the query
-// (within the query's super-tile of 256 tiles, else via super-tile minima),
-// then the latest chunk of that tile, then the latest element of that chunk
-// (depths recomputed from the chunk's start depth).
+// One warp per queued query: latest tile of the query's document whose
+// minimum is <= the query (within the query's super-tile of 256 tiles, else
+// via super-tile minima, never before the document's first tile), then the
+// latest chunk of that tile, then the latest element of that chunk (depths
+// recomputed from the chunk's start depth).
 __global__ void pse_resolve_kernel(PseArgs a) {
-  DeviceStatus *st = a.status;
   const unsigned long long qn = *a.queue_len;
-  const long long E = (long long)*a.count;
   const bool parents = a.mode == kPseParents;
   const int lane = threadIdx.x & 31;
   const unsigned long long warp = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) >> 5;
   const unsigned long long warps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
   for (unsigned long long qi = warp; qi < qn && qi < a.queue_cap; qi += warps) {
-    const long long e = (long long)a.queue[qi];
-    const uint32_t v = a.elems[e];
+    const unsigned long long qe = a.queue[qi];
+    const int doc = (int)(qe >> 40);
+    const long long e = (long long)(qe & ((1ull << 40) - 1));
+    PseDoc dv;
+    if (a.batch) {
+      const unsigned long long *tile0 = parents ? a.batch->pr_tile0 : a.batch->br_tile0;
+      int dd;
+      dv = pse_doc(a, tile0[doc], &dd);  // the document's first tile
+    } else {
+      int dd;
+      dv = pse_doc(a, 0, &dd);
+    }
+    DeviceStatus *st = dv.st;
+    const long long first = (long long)dv.tile_first;  // virtual tiles of the document start here
+    const uint32_t v = dv.elems[e];
     const long long ce = e / kPseItems;
-    const int32_t he = __shfl_sync(0xffffffffu, chunk_depth(a, ce, E, lane), (int)(e - ce * kPseItems));
+    const int32_t he = __shfl_sync(0xffffffffu, chunk_depth(a, dv, first * kPseThreads + ce, ce * kPseItems, lane),
+                                   (int)(e - ce * kPseItems));
     const int32_t qv = parents ? he : he - 1;
-    const long long tile = e / kPseTile;
+    const long long tile = first + e / kPseTile;
     const long long sup0 = (tile >> kPseSuperShift) << kPseSuperShift;
-    long long tt = warp_latest_le(a.tile_min, tile - 1, sup0, qv, lane);
-    if (tt < 0 && sup0 > 0) {
-      const long long sp = warp_latest_le(a.super_min, (sup0 >> kPseSuperShift) - 1, 0, qv, lane);
-      if (sp >= 0) tt = warp_latest_le(a.tile_min, ((sp + 1) << kPseSuperShift) - 1, sp << kPseSuperShift, qv, lane);
+    long long tt = warp_latest_le(a.tile_min, tile - 1, sup0 > first ? sup0 : first, qv, lane);
+    if (tt < 0 && sup0 > first) {
+      const long long sp = warp_latest_le(a.super_min, (sup0 >> kPseSuperShift) - 1, first >> kPseSuperShift, qv, lane);
+      if (sp >= 0) {
+        const long long lo = sp << kPseSuperShift;
+        tt = warp_latest_le(a.tile_min, ((sp + 1) << kPseSuperShift) - 1, lo > first ? lo : first, qv, lane);
+      }
     }
     long long found = -1;
     if (tt >= 0) {
       const long long c = warp_latest_le(a.ch_min + tt * kPseThreads, kPseThreads - 1, 0, qv, lane);
       if (c >= 0) {
-        const long long cc = tt * kPseThreads + c;
-        const unsigned b = __ballot_sync(0xffffffffu, chunk_depth(a, cc, E, lane) <= qv);
-        if (b) found = cc * kPseItems + (31 - __clz(b));
+        const long long eb = (tt - first) * kPseTile + c * kPseItems;  // element index in the document
+        const unsigned b = __ballot_sync(0xffffffffu, chunk_depth(a, dv, tt * kPseThreads + c, eb, lane) <= qv);
+        if (b) found = eb + (31 - __clz(b));
       }
     }
     if (parents) {
       // compute_parents takes 0 when its stack is empty
       const long long p = found >= 0 ? found : 0;
-      const long long tinc_p = terminal_count(a, p, lane);
-      const long long tinc_e = terminal_count(a, e, lane);
-      if (lane == 0) emit_node(a, v, __ldg(a.is_term + v) != 0, e, tinc_e, p - tinc_p, (long long)*a.num_tokens);
+      const long long tinc_p = terminal_count(a, dv, p, lane);
+      const long long tinc_e = terminal_count(a, dv, e, lane);
+      if (lane == 0) emit_node(a, dv, v, __ldg(a.is_term + v) != 0, e, tinc_e, p - tinc_p);
     } else if (lane == 0) {
       if (found < 0) record_reject(st, &st->parse_reject_reason, 3);
-      else if ((a.elems[found] & 0x7fffffffu) != (v & 0x7fffffffu)) record_reject(st, &st->parse_reject_reason, 2);
+      else if ((dv.elems[found] & 0x7fffffffu) != (v & 0x7fffffffu)) record_reject(st, &st->parse_reject_reason, 2);
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// Batch planning
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(1024) batch_plan_kernel(BatchDesc b, int kind, unsigned long long *tile0,
+                                                          unsigned long long tile) {
+  __shared__ long long tmp[32];
+  const int t = threadIdx.x;
+  long long carry = 0;
+  for (int base = 0; base < b.docs; base += 1024) {
+    const int d = base + t;
+    long long cnt = 0;
+    if (d < b.docs) {
+      const DeviceStatus &s = b.status[d];
+      const unsigned long long c = kind == kPlanPairs ? s.num_tokens + 2
+                                   : kind == kPlanBrackets ? s.num_brackets : s.num_productions;
+      cnt = (long long)((c + tile - 1) / tile);
+    }
+    long long tot;
+    const long long ex = block_exclusive_scan<long long>(cnt, AddI64(), 0ll, tmp, &tot);
+    if (d < b.docs) tile0[d] = (unsigned long long)(carry + ex);
+    carry += tot;
+  }
+  if (t == 0) tile0[b.docs] = (unsigned long long)carry;
 }
 
 }  // namespace alpacc

@@ -1,0 +1,139 @@
+// Kernel argument blocks filled from a grammar handle's tables and scratch
+// buffers, shared by the single-document path (api.cu) and the batch path
+// (batch.cu). The caller grows the scratch buffers first and then sets the
+// per-call fields (sizes, tickets, capacities, batch descriptor).
+#pragma once
+
+#include <algorithm>
+
+#include "handle.h"
+#include "kernels.h"
+
+namespace alpacc {
+
+inline LexArgs lex_args(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, uint64_t tiles) {
+  const HostGrammar &hg = g->hg;
+  const LexerMachine &lm = hg.lex;
+  LexArgs a{};
+  a.in = d_in;
+  a.n = n;
+  a.num_tiles = tiles;
+  a.cls_id = (const uint8_t *)g->cls_id.p;
+  a.trans_words_ptr = (const uint32_t *)g->trans_words.p;
+  a.trans_words = g->trans_word_count;
+  a.copies = g->trans_rep;
+  a.lane_of = (const uint8_t *)g->lane_of.p;
+  a.img = (const uint8_t *)g->img.p;
+  a.img_cnt = (const uint8_t *)g->img_cnt.p;
+  a.img2 = lm.img2.empty() ? nullptr : (const unsigned long long *)g->img2.p;
+  a.sterm = (const uint8_t *)g->sterm.p;
+  a.sflags = (const uint8_t *)g->sflags.p;
+  a.M = lm.M;
+  a.C = lm.C;
+  a.dead = lm.dead;
+  a.m0 = lm.m0;
+  a.ignore = hg.ignore;
+  a.len_max = hg.len_max;
+  a.tok_ids = g->tok_ids.p;
+  a.tok_starts = g->tok_starts.p;
+  a.tok_lens = g->tok_lens.p;
+  a.term_w = (int)hg.t.terminal_size;
+  a.idx_w = (int)hg.t.index_size;
+  a.len_w = (int)hg.t.length_size;
+  a.ticket = (unsigned *)g->lex_ticket.p;
+  a.st1_flag = (unsigned *)g->st1_flag.p;
+  a.st1_state = (uint8_t *)g->st1_state.p;
+  a.st1_vec = (uint8_t *)g->st1_vec.p;
+  a.st2 = PairTileState{(unsigned *)g->st2_flags.p, (unsigned long long *)g->st2_agg.p,
+                        (unsigned long long *)g->st2_inc.p};
+  a.status = g->d_status;
+  a.diag = g->diag;
+  a.stage_ids = (uint8_t *)g->stage_ids.p;
+  a.stage_starts = (uint32_t *)g->stage_starts.p;
+  a.stage_ends = (uint32_t *)g->stage_ends.p;
+  a.tile_cnt = (uint32_t *)g->tile_cnt.p;
+  a.tile_pos = (uint32_t *)g->tile_pos.p;
+  return a;
+}
+
+inline LexPlaceArgs lex_place_args(alpacc_gpu_grammar *g, const LexArgs &a, uint64_t tiles) {
+  LexPlaceArgs pa{};
+  pa.num_tiles = tiles;
+  pa.tile_data = kLexData;
+  pa.n = a.n;
+  pa.tile_cnt = a.tile_cnt;
+  pa.tile_pos = a.tile_pos;
+  pa.tile_off = (unsigned long long *)g->tile_off.p;
+  pa.tile_prev = (uint32_t *)g->tile_prev.p;
+  pa.stage_ids = a.stage_ids;
+  pa.stage_starts = a.stage_starts;
+  pa.stage_ends = a.stage_ends;
+  pa.tok_ids = a.tok_ids;
+  pa.tok_starts = a.tok_starts;
+  pa.tok_lens = a.tok_lens;
+  pa.term_w = a.term_w;
+  pa.idx_w = a.idx_w;
+  pa.len_w = a.len_w;
+  pa.len_max = a.len_max;
+  pa.status = a.status;
+  pa.batch = a.batch;
+  return pa;
+}
+
+inline PairArgs pair_args(alpacc_gpu_grammar *g) {
+  const alpacc_tables &tb = g->hg.t;
+  const PairTable &pt = g->hg.pairs;
+  PairArgs a{};
+  a.tok_ids = g->tok_ids.p;
+  a.term_w = (int)tb.terminal_size;
+  a.num_tokens = &g->d_status->num_tokens;
+  a.q = pt.q;
+  a.k = pt.k;
+  a.nt = pt.nt;
+  a.empty_t = (int)tb.empty_terminal;
+  a.start_t = (int)tb.start_terminal;
+  a.end_t = (int)tb.end_terminal;
+  a.dense = (const uint32_t *)g->dense.p;
+  a.rec = (const unsigned long long *)g->rec.p;
+  a.stacks = (const uint32_t *)g->stacks.p;
+  a.prods = (const uint32_t *)g->prods.p;
+  a.br_out = (uint32_t *)g->br.p;
+  a.pr_out = (uint32_t *)g->pr.p;
+  a.ticket = (unsigned *)g->pair_ticket.p;
+  a.st = PairTileState{(unsigned *)g->pst_flags.p, (unsigned long long *)g->pst_agg.p,
+                       (unsigned long long *)g->pst_inc.p};
+  a.status = g->d_status;
+  return a;
+}
+
+inline PseArgs pse_args(alpacc_gpu_grammar *g, int mode, unsigned long long queue_cap) {
+  const alpacc_tables &tb = g->hg.t;
+  PseArgs a{};
+  a.mode = mode;
+  a.elems = (const uint32_t *)(mode == kPseBrackets ? g->br.p : g->pr.p);
+  a.count = mode == kPseBrackets ? &g->d_status->num_brackets : &g->d_status->num_productions;
+  a.num_tokens = &g->d_status->num_tokens;
+  a.arity = (const int32_t *)g->arity.p;
+  a.is_term = (const uint8_t *)g->is_term.p;
+  a.num_prods = (int)g->hg.pairs.arity.size();
+  a.ch_h0 = (int32_t *)g->ch_h0.p;
+  a.ch_min = (int32_t *)g->chunk_min.p;
+  a.ch_tc = (int32_t *)g->ch_tc.p;
+  a.tile_min = (int32_t *)g->tile_min.p;
+  a.super_min = (int32_t *)g->super_min.p;
+  a.queue = (unsigned long long *)g->queue.p;
+  a.queue_cap = queue_cap;
+  a.queue_len = (unsigned long long *)g->queue_len.p;
+  a.node_prods = g->node_prods.p;
+  a.node_parents = g->node_parents.p;
+  a.token_parents = g->token_parents.p;
+  a.prod_w = (int)tb.production_size;
+  a.idx_w = (int)tb.index_size;
+  a.ticket = (unsigned *)g->pse_ticket.p;
+  a.st = PairTileState{(unsigned *)g->pse_flags.p, (unsigned long long *)g->pse_agg.p,
+                       (unsigned long long *)g->pse_inc.p};
+  a.status = g->d_status;
+  return a;
+}
+
+}  // namespace alpacc

@@ -87,6 +87,22 @@ def lib():
         L.alpacc_gpu_enqueue.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64]
         L.alpacc_gpu_collect.restype = ctypes.c_int
         L.alpacc_gpu_collect.argtypes = [ctypes.c_void_p, ctypes.POINTER(Result)]
+        L.alpacc_server_start.restype = ctypes.c_void_p
+        L.alpacc_server_start.argtypes = [ctypes.POINTER(Tables), ctypes.c_int, ctypes.c_int, ctypes.c_uint64,
+                                          ctypes.POINTER(ctypes.c_int)]
+        L.alpacc_server_submit.restype = ctypes.c_int
+        L.alpacc_server_submit.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                           ctypes.POINTER(ctypes.c_uint64)]
+        L.alpacc_server_wait.restype = ctypes.c_int
+        L.alpacc_server_wait.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Result),
+                                         ctypes.POINTER(ctypes.c_double)]
+        L.alpacc_server_stats.restype = ctypes.c_int
+        L.alpacc_server_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
+        L.alpacc_server_stop.restype = None
+        L.alpacc_server_stop.argtypes = [ctypes.c_void_p]
+        L.alpacc_gpu_autotune.restype = ctypes.c_int
+        L.alpacc_gpu_autotune.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                          ctypes.POINTER(ctypes.c_int)]
         L.alpacc_gpu_parse_batch.restype = ctypes.c_int
         L.alpacc_gpu_parse_batch.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
                                              ctypes.POINTER(Result)]
@@ -223,6 +239,33 @@ class Parser:
         finally:
             lib().alpacc_result_free(ctypes.byref(r))
 
+    def autotune(self, dev_ptr: int, n: int) -> int:
+        """Pick the lexer's table copies on a device-resident sample; returns the choice."""
+        c = ctypes.c_int(0)
+        self._check(lib().alpacc_gpu_autotune(self._h, dev_ptr, n, ctypes.byref(c)))
+        return c.value
+
+    def parse_batch(self, docs) -> list:
+        """Many independent inputs in one batched call; one ParseResult each."""
+        parts = [bytes(d) for d in docs]
+        offs = np.zeros(len(parts) + 1, dtype=np.int64)
+        offs[1:] = np.cumsum([len(p) for p in parts])
+        buf = np.frombuffer(b"".join(parts) or b"\0", dtype=np.uint8)
+        outs = (Result * max(len(parts), 1))()
+        self._check(lib().alpacc_gpu_parse_batch(self._h, buf.ctypes.data, offs.ctypes.data, len(parts), outs))
+        try:
+            return [self._result(outs[i], OK if outs[i].valid else REJECT) for i in range(len(parts))]
+        finally:
+            for i in range(len(parts)):
+                lib().alpacc_result_free(ctypes.byref(outs[i]))
+
+    def parse_batch_raw(self, buf_ptr: int, offs_ptr: int, count: int):
+        """Batch from raw pointers (bytes, int64 offsets[count+1]); returns the
+        Result array; release each with ``free_result``."""
+        outs = (Result * max(count, 1))()
+        self._check(lib().alpacc_gpu_parse_batch(self._h, buf_ptr, offs_ptr, count, outs))
+        return outs
+
     def parse_device(self, dev_ptr: int, n: int):
         """Bytes already on the device. Returns (status, Result with device pointers)."""
         r = Result()
@@ -303,3 +346,57 @@ def _cudart_memcpy_d2h(dst: int, src: int, nbytes: int):
     rc = _cudart.cudaMemcpy(dst, src, nbytes, 2)
     if rc != 0:
         raise AlpaccError(E_CUDA, "cudaMemcpy failed (%d)" % rc)
+
+
+class Server:
+    """In-process request server with continuous batching (alpacc_server_*)."""
+
+    def __init__(self, tables, device: int = 0, workers: int = 2, budget: int = 8 << 30):
+        self._struct, self._keep = make_tables(tables)
+        self.layout = wire.Layout.of(tables)
+        self._lib = lib()
+        err = ctypes.c_int(0)
+        self._s = self._lib.alpacc_server_start(ctypes.byref(self._struct), device, workers, budget, ctypes.byref(err))
+        if not self._s:
+            raise AlpaccError(err.value, self._lib.alpacc_strerror(err.value).decode())
+
+    def submit(self, data) -> int:
+        a = np.frombuffer(bytes(data), dtype=np.uint8)
+        rid = ctypes.c_uint64(0)
+        rc = self._lib.alpacc_server_submit(self._s, a.ctypes.data if a.size else None, a.size, ctypes.byref(rid))
+        if rc < 0:
+            raise AlpaccError(rc, self._lib.alpacc_strerror(rc).decode())
+        return rid.value
+
+    def wait(self, rid: int):
+        """(ParseResult, latency ms from submit to completion)."""
+        r = Result()
+        ms = ctypes.c_double(0)
+        rc = self._lib.alpacc_server_wait(self._s, rid, ctypes.byref(r), ctypes.byref(ms))
+        if rc < 0:
+            raise AlpaccError(rc, self._lib.alpacc_strerror(rc).decode())
+        try:
+            if rc != OK:
+                return wire.ParseResult(False), ms.value
+            lay = self.layout
+            T, N = r.num_tokens, r.num_nodes
+            return wire.ParseResult(
+                True,
+                _np_from(r.token_ids, T, lay.terminal), _np_from(r.token_starts, T, lay.index, True),
+                _np_from(r.token_lengths, T, lay.length), _np_from(r.node_productions, N, lay.production),
+                _np_from(r.node_parents, N, lay.index, True), _np_from(r.token_parents, T, lay.index, True)), ms.value
+        finally:
+            self._lib.alpacc_result_free(ctypes.byref(r))
+
+    def stats(self) -> dict:
+        v = (ctypes.c_int64 * 4)()
+        self._lib.alpacc_server_stats(self._s, v, 4)
+        return {"batches": v[0], "served": v[1], "largest_batch": v[2], "queued": v[3]}
+
+    def close(self):
+        if getattr(self, "_s", None):
+            self._lib.alpacc_server_stop(self._s)
+            self._s = None
+
+    def __del__(self):
+        self.close()

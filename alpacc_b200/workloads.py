@@ -253,9 +253,31 @@ def lognormal_lengths(count: int, median: int, lo: int, hi: int, seed: int, sigm
 
 
 def json_batch(count: int = 4096, median: int = 8192, lo: int = 200, hi: int = 4 << 20, seed: int = 4):
-    """(bytes, int64 offsets[count+1]) of ``count`` JSON documents."""
+    """(bytes, int64 offsets[count+1]) of ``count`` JSON documents with
+    log-normal lengths; each is a top-level array of elements drawn from one
+    shared pool (document i uses seed 4_000_000 + i), padded to its length."""
     lens = lognormal_lengths(count, median, lo, hi, seed)
-    docs = [json_small(int(L), 4_000_000 + i) for i, L in enumerate(lens)]
+    g = _Json(np.random.default_rng(seed + 1))
+    pool = sorted((g.element().encode() for _ in range(8192)), key=len)
+    plen = np.array([len(p) for p in pool], dtype=np.int64)
+    docs = []
+    for i, L in enumerate(lens):
+        L = int(L)
+        k = max(1, int(np.searchsorted(plen, max(8, L // 4), side="left")))
+        body = _pool_concat(pool[:k], np.random.default_rng(4_000_000 + i), L - 2, b",")
+        doc = b"[" + body + b"]"
+        if len(doc) > L:
+            doc = b"[]"
+        docs.append(doc + b" " * (L - len(doc)))
     offs = np.zeros(count + 1, dtype=np.int64)
     offs[1:] = np.cumsum([len(d) for d in docs])
     return b"".join(docs), offs
+
+
+def json_trace(count: int, rate: float, median: int = 16384, lo: int = 64, hi: int = 16 << 20, seed: int = 5):
+    """A serving trace: ``count`` JSON requests with log-normal sizes and
+    Poisson arrivals at ``rate`` requests/s. Returns (docs, arrival seconds)."""
+    buf, offs = json_batch(count, median, lo, hi, seed)
+    docs = [buf[offs[i]:offs[i + 1]] for i in range(count)]
+    gaps = np.random.default_rng(seed + 7).exponential(1.0 / rate, count)
+    return docs, np.cumsum(gaps) - gaps[0]

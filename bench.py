@@ -46,12 +46,203 @@ WORKLOADS = {
                  desc="sexp %d MiB single s-expression document per GPU (nesting up to 10000)"),
     "sexp_unbalanced": dict(grammar="sexp.alp", index32=False, ref="sexp_i64", size=1 << 30, reject=True,
                             desc="sexp %d MiB document with 5%% of forms carrying an extra ')' (rejected)"),
+    "batch": dict(grammar="json_ext.alp", index32=True, ref="json_ext_i32", size=0, reject=False,
+                  desc="4096 JSON documents, log-normal lengths (median 8 KiB, 200 B to 4 MiB; %d MiB)"),
+    "serve": dict(grammar="json_ext.alp", index32=True, ref="json_ext_i32", size=0, reject=False,
+                  desc="serving trace of JSON requests, Poisson arrivals, log-normal sizes (median 16 KiB, "
+                       "64 B to 16 MiB; %d MiB)"),
 }
+
+SERVE_RATES = (2000, 5000, 10000, 20000, 50000)
+
+
+def _pct(x, q):
+    import numpy as np
+    return float(np.percentile(np.asarray(x), q)) if len(x) else None
+
+
+def ours_serve(a, rank, world, local_rank, dist):
+    """The served form: a seeded Poisson trace of JSON requests replayed in
+    real time against alpacc_server (continuous batching, 8 GiB scratch
+    budget) and against one plain alpacc_gpu_parse per request in arrival
+    order; p50/p99 latency (arrival to result) and GB/s per arrival rate."""
+    import threading
+
+    import numpy as np
+    import torch
+
+    from alpacc_b200 import workloads as W
+    from alpacc_b200.grammar.cache import load_tables
+    from alpacc_b200.native import Parser, Server
+
+    torch.cuda.set_device(local_rank)
+    wl = WORKLOADS["serve"]
+    tables = load_tables(os.path.join(REPO, "grammars", wl["grammar"]), index32=True)
+    count = a.serve_requests
+    docs, _ = W.json_trace(count, 1.0, seed=5 + rank)
+    sizes = np.array([len(d) for d in docs], dtype=np.int64)
+    srv = Server(tables, device=local_rank, workers=2, budget=8 << 30)
+    plain = Parser(tables, device=local_rank, max_input=int(sizes.max()))
+    pins = [np.frombuffer(d, dtype=np.uint8) for d in docs]
+    for d in docs[:32]:  # warm-up of both paths
+        srv.wait(srv.submit(d))
+        plain.parse(d)
+    sweep = []
+    for rate in SERVE_RATES:
+        gaps = np.random.default_rng(1000 + rate).exponential(1.0 / rate, count)
+        arr = np.cumsum(gaps) - gaps[0]
+        # continuous batching
+        ids = [None] * count
+        t0 = time.perf_counter() + 0.01
+
+        def submitter():
+            for i in range(count):
+                dt = t0 + arr[i] - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                ids[i] = srv.submit(docs[i])
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        lat = []
+        last = t0
+        for i in range(count):
+            while ids[i] is None:
+                time.sleep(0.0001)
+            r, ms = srv.wait(ids[i])
+            lat.append(ms)
+            last = max(last, time.perf_counter())
+        th.join()
+        served_gbs = float(sizes.sum()) / (last - t0) / 1e9
+        # one plain call per request, in arrival order
+        plat = []
+        t1 = time.perf_counter() + 0.01
+        for i in range(count):
+            dt = t1 + arr[i] - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            rc, res = plain.parse_raw(pins[i].ctypes.data, len(pins[i]))
+            Parser.free_result(res)
+            plat.append((time.perf_counter() - (t1 + arr[i])) * 1e3)
+        plain_gbs = float(sizes.sum()) / (time.perf_counter() - t1) / 1e9
+        sweep.append({"rate_per_s": rate, "p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99), "gbs": served_gbs,
+                      "plain_p50_ms": _pct(plat, 50), "plain_p99_ms": _pct(plat, 99), "plain_gbs": plain_gbs})
+    st = srv.stats()
+    srv.close()
+    if rank != 0:
+        return
+    top = sweep[-1]
+    line = {
+        "metric": METRIC, "value": top["gbs"], "unit": "GB/s", "n_gpus": world, "steps": len(SERVE_RATES),
+        "warmup": 32, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8", "data": "synthetic (seeded JSON requests, seeded Poisson arrivals)",
+        "config": dict(workload_config(int(sizes.sum()), world, "serve"), requests=count, workers=2,
+                       scratch_budget_gib=8, batches=st["batches"], largest_batch=st["largest_batch"]),
+        "serve": sweep,
+        "p99_ms_at_max_rate": top["p99_ms"], "plain_p99_ms_at_max_rate": top["plain_p99_ms"],
+        "e2e": {"value": top["gbs"], "unit": "GB/s", "h2d_bytes_per_step": int(sizes.sum()), "d2h_bytes_per_step": None,
+                "note": "requests arrive as host buffers and results return to host memory"},
+    }
+    print(json.dumps(line))
+
+
+def ours_batch(a, rank, world, local_rank, dist):
+    """The batched form: 4096 documents per step through alpacc_gpu_parse_batch
+    (host buffers in and out, one launch per stage), against one plain
+    alpacc_gpu_parse per document."""
+    import numpy as np
+    import torch
+
+    from alpacc_b200 import workloads as W
+    from alpacc_b200.grammar.cache import load_tables
+    from alpacc_b200.native import Parser, Result
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    wl = WORKLOADS["batch"]
+    buf, offs = W.json_batch(count=4096, median=8192, lo=200, hi=4 << 20, seed=4 + rank)
+    total = len(buf)
+    tables = load_tables(os.path.join(REPO, "grammars", wl["grammar"]), index32=True)
+    parser = Parser(tables, device=local_rank, max_input=total)
+    pin = torch.empty(total, dtype=torch.uint8, pin_memory=True)
+    pin.numpy()[:] = np.frombuffer(buf, dtype=np.uint8)
+    offs = np.ascontiguousarray(offs, dtype=np.int64)
+    d_all = pin.to(dev)
+    choice = parser.autotune(d_all.data_ptr(), total)  # lexer table copies for this grammar
+    ext = torch.cuda.ExternalStream(parser.stream_handle(), device=dev)
+    count = len(offs) - 1
+
+    def batched():
+        outs = parser.parse_batch_raw(pin.data_ptr(), offs.ctypes.data, count)
+        ok = sum(outs[i].valid for i in range(count))
+        for i in range(count):
+            Parser.free_result(outs[i])
+        return ok
+
+    for _ in range(a.warmup):
+        accepted = batched()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    for _ in range(a.steps):
+        batched()
+    e1.record(ext)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = max_over_ranks(dist, e0.elapsed_time(e1), dev)
+    value = job_throughput(world, total, a.steps, ms)
+    # one plain call per document (the same host buffers)
+    for i in range(min(64, count)):
+        rc, r = parser.parse_raw(pin.data_ptr() + int(offs[i]), int(offs[i + 1] - offs[i]))
+        Parser.free_result(r)
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(ext)
+    for i in range(count):
+        rc, r = parser.parse_raw(pin.data_ptr() + int(offs[i]), int(offs[i + 1] - offs[i]))
+        Parser.free_result(r)
+    f1.record(ext)
+    torch.cuda.synchronize()
+    per_ms = max_over_ranks(dist, f0.elapsed_time(f1), dev)
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8", "data": "synthetic (seeded JSON generator, log-normal lengths)",
+        "config": dict(workload_config(total, world, "batch"), documents=count, accepted=int(accepted),
+                       autotune_lexer_table_copies=choice),
+        "per_input": {"value": job_throughput(world, total, 1, per_ms), "unit": "GB/s", "ms": per_ms,
+                      "what": "one alpacc_gpu_parse per document, same host buffers"},
+        "speedup_vs_per_input": (job_throughput(world, total, a.steps, ms) / job_throughput(world, total, 1, per_ms)),
+        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": total, "d2h_bytes_per_step": None,
+                "note": "the batch entry point takes and returns host buffers: value is end to end"},
+        "gpu_launches": parser.counts()["launches"] * a.steps,
+        "clocks": clk,
+    }
+    if not a.no_cpu_baseline:
+        from oracle.ref import RefOracle, available
+        if available(wl["ref"]):
+            ref = RefOracle(wl["ref"])
+            t0 = time.perf_counter()
+            for i in range(count):
+                ref.pipeline(np.frombuffer(buf[offs[i]:offs[i + 1]], dtype=np.uint8))
+            t = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": total / t / 1e9, "unit": "GB/s", "cores": 1, "kind": "reference",
+                                    "sample": "all %d documents once, reference C backend in memory (%.2fs)"
+                                              % (count, t)}
+    print(json.dumps(line))
 
 
 def make_doc(workload, n, seed):
     from alpacc_b200 import workloads as W
-    if workload == "json":
+    if workload in ("json", "batch", "serve"):
         return W.json_doc(n, seed)
     return W.sexp_doc(n, seed + 1, unbalanced_frac=0.05 if workload == "sexp_unbalanced" else 0.0, max_depth=10000)
 
@@ -375,6 +566,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=0, help="input bytes (default: the workload's size)")
     ap.add_argument("--workload", default="json", choices=sorted(WORKLOADS))
+    ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--cpu-sample", type=int, default=256 << 20)
     ap.add_argument("--ref-sample", type=int, default=16 << 20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -395,6 +587,10 @@ def main():
             dist = tdist
     if a.impl == "reference":
         reference_arm(a, rank, world)
+    elif a.workload == "batch":
+        ours_batch(a, rank, world, local_rank, dist)
+    elif a.workload == "serve":
+        ours_serve(a, rank, world, local_rank, dist)
     else:
         ours(a, rank, world, local_rank, dist)
     if dist:

@@ -169,9 +169,13 @@ int alpacc_gpu_collect(alpacc_gpu_grammar *g, alpacc_result *out);
 
 /*
  * Many independent inputs at once: `bytes` holds them back to back, input i is
- * bytes[offsets[i] .. offsets[i+1]). `outs` receives `count` results.
- * Returns ALPACC_OK when every input was processed (each outs[i].valid says
- * accept/reject) or the first error.
+ * bytes[offsets[i] .. offsets[i+1]). `outs` receives `count` results, each
+ * identical to parsing that input alone. Every stage is launched once for the
+ * whole batch (the reference sets up and launches per input,
+ * backends/cuda/cli.cu:739-792); the results share one pinned block, released
+ * when the last of them is passed to alpacc_result_free. Returns ALPACC_OK
+ * when every input was processed (each outs[i].valid says accept/reject) or
+ * the first error.
  */
 int alpacc_gpu_parse_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offsets, uint32_t count,
                            alpacc_result *outs);
@@ -179,6 +183,30 @@ int alpacc_gpu_parse_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const in
 /* Release a host result. Its pinned block returns to the handle for reuse, so
    results must be released before the handle that produced them. */
 void alpacc_result_free(alpacc_result *r);
+
+/*
+ * Request server with continuous batching (replaces the reference's
+ * sequential `--server` loop, backends/c/cli.c:153-161 and
+ * backends/cuda/cli.cu:846-875, for in-process callers). `workers` threads each
+ * own a handle and a stream; a free worker takes every queued request that
+ * fits its share (scratch_budget / workers) of the device scratch budget and
+ * parses them as one batch, so requests arriving while a batch runs join the
+ * next one and batches overlap on the device. Each result equals parsing its
+ * input alone.
+ *   submit: copies the input, returns its id;
+ *   wait:   blocks until that request is done; its status (OK / REJECT /
+ *           error), its result (release with alpacc_result_free before
+ *           stopping the server) and the latency from submit to completion;
+ *   stats:  batches run, requests served, largest batch, requests queued;
+ *   stop:   drains the queue, joins the workers, frees the handles.
+ */
+typedef struct alpacc_server alpacc_server;
+alpacc_server *alpacc_server_start(const alpacc_tables *tables, int device, int workers, uint64_t scratch_budget,
+                                   int *err);
+int alpacc_server_submit(alpacc_server *s, const uint8_t *in, uint64_t n, uint64_t *id);
+int alpacc_server_wait(alpacc_server *s, uint64_t id, alpacc_result *out, double *latency_ms);
+int alpacc_server_stats(alpacc_server *s, int64_t *vals, int n);
+void alpacc_server_stop(alpacc_server *s);
 
 /*
  * Write the combined-mode response record for input `in` to `out`, byte for
@@ -198,6 +226,15 @@ const char *alpacc_strerror(int status);
  * around the launches on the handle's stream), or a negative value.
  */
 double alpacc_gpu_last_ms(alpacc_gpu_grammar *g);
+
+/*
+ * Autotuner (no counterpart in the reference, whose CUDA backend takes its
+ * launch shapes from per-architecture tables): parses the device-resident
+ * sample with each candidate number of shared-memory copies of the lexer's
+ * tables (more copies: fewer bank conflicts; fewer: more resident CTAs) and
+ * keeps the fastest for this handle's grammar. *choice receives it.
+ */
+int alpacc_gpu_autotune(alpacc_gpu_grammar *g, const uint8_t *d_sample, uint64_t n, int *choice);
 
 /* The cudaStream_t the handle launches on, so a caller can order its own work
    (copies, events) with it. */
