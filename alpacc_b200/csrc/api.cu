@@ -42,9 +42,12 @@ namespace {
     if (r_ != ALPACC_OK) return r_; \
   } while (0)
 
+int upload_pairs(alpacc_gpu_grammar *g);
+
 int upload_tables(alpacc_gpu_grammar *g) {
   const LexerMachine &lm = g->hg.lex;
   if (lm.M > 128) return ALPACC_E_UNSUPPORTED;  // 7-bit states in the transition entries
+  if (g->hg.parts == ALPACC_PARTS_PARSER) return upload_pairs(g);
   // transition entries at class * M + state: next state | produce(next) << 7
   const size_t mc = (size_t)lm.M * lm.C;
   std::vector<uint32_t> trw((mc + 3) / 4, 0);
@@ -75,6 +78,10 @@ int upload_tables(alpacc_gpu_grammar *g) {
   if (!lm.img2.empty()) TRY(upload(g->img2, lm.img2));
   TRY(upload(g->sterm, lm.term));
   TRY(upload(g->sflags, lm.flags));
+  return g->hg.parts == ALPACC_PARTS_LEXER ? ALPACC_OK : upload_pairs(g);
+}
+
+int upload_pairs(alpacc_gpu_grammar *g) {
   const PairTable &pt = g->hg.pairs;
   TRY(upload(g->dense, pt.dense));
   // records packed as ss | ps << 24 | nb << 48 | np << 56 (spans checked < 2^24 on load)
@@ -195,8 +202,14 @@ int finish_host_result(alpacc_gpu_grammar *g, alpacc_result *out) {
   return ALPACC_OK;
 }
 
-// The whole device path for d_in[0..n). Leaves counts in g->last_T / last_N.
-int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
+// What run_device computes: the combined path, the lexer alone (lexer-mode
+// program), or the parser alone on token ids already in g->tok_ids
+// (parser-mode program: pairs and the bracket walk, no tree).
+enum RunMode { kRunBoth = 0, kRunLex = 1, kRunParse = 2 };
+
+// The whole device path for d_in[0..n) (n bytes; n token ids for kRunParse).
+// Leaves counts in g->last_T / last_N.
+int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int mode = kRunBoth) {
   const HostGrammar &hg = g->hg;
   const alpacc_tables &tb = hg.t;
   const LexerMachine &lm = hg.lex;
@@ -211,7 +224,11 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
 
   // ---------------- lexer ----------------
   uint64_t T = 0;
-  if (n > 0) {
+  if (mode == kRunParse) {
+    T = n;
+    // from pageable memory: staged before the call returns
+    CK(cudaMemcpyAsync(&g->d_status->num_tokens, &T, 8, cudaMemcpyHostToDevice, g->stream));
+  } else if (n > 0) {
     const uint64_t tiles = (n + kLexData - 1) / kLexData;
     // host input: copied in pieces of ~16 MiB, each piece's tiles lexed as soon as it arrived
     uint64_t piece_tiles = tiles, pieces = 1;
@@ -278,6 +295,16 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     T = g->h_status->num_tokens;
     if (g->host_out) TRY(start_token_copy(g, T));
   }
+  if (mode == kRunLex) {
+    CK(cudaEventRecord(g->ev1, g->stream));
+    CK(cudaStreamSynchronize(g->stream));
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, g->ev0, g->ev1) == cudaSuccess) g->last_ms = ms;
+    collect_stages(g);
+    g->last_T = T;
+    g->last_N = 0;
+    return ALPACC_OK;
+  }
 
   // ---------------- pair lookup ----------------
   const uint64_t m = T + 2;
@@ -294,7 +321,7 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
     TRY(grow(g->tok_ids, std::max<uint64_t>(T, 1) * term_w));
     CK(cudaMemsetAsync(g->pair_ticket.p, 0, 16, g->stream));
     CK(cudaMemsetAsync(g->pst_flags.p, 0, tiles * 4, g->stream));
-    if (n == 0) CK(cudaMemsetAsync(&g->d_status->num_tokens, 0, 8, g->stream));
+    if (n == 0 && mode != kRunParse) CK(cudaMemsetAsync(&g->d_status->num_tokens, 0, 8, g->stream));
     PairArgs a = pair_args(g);
     a.num_tiles = tiles;
     a.br_cap = br_cap;
@@ -328,28 +355,35 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
   TRY(grow(g->node_prods, std::max<uint64_t>(P, 1) * prod_w));
   TRY(grow(g->node_parents, std::max<uint64_t>(P, 1) * idx_w));
   TRY(grow(g->token_parents, std::max<uint64_t>(T, 1) * idx_w));
-  for (int mode = 0; mode < 2; ++mode) {
-    const uint64_t E = mode == kPseBrackets ? B : P;
+  const int walks = mode == kRunParse ? 1 : 2;  // the parser-mode result has no tree
+  for (int walk = 0; walk < walks; ++walk) {
+    const uint64_t E = walk == kPseBrackets ? B : P;
     if (E == 0) continue;
     const uint64_t tiles = (E + kPseTile - 1) / kPseTile;
     CK(cudaMemsetAsync(g->pse_ticket.p, 0, 16, g->stream));
     CK(cudaMemsetAsync(g->pse_flags.p, 0, tiles * 4, g->stream));
     CK(cudaMemsetAsync(g->queue_len.p, 0, 16, g->stream));
     CK(cudaMemsetAsync(g->super_min.p, 0x7f, ((tiles >> kPseSuperShift) + 1) * 4, g->stream));
-    PseArgs a = pse_args(g, mode, Emax);
+    PseArgs a = pse_args(g, walk, Emax);
     a.num_tiles = tiles;
-    stage_begin(g, 2 + 2 * mode);
+    stage_begin(g, 2 + 2 * walk);
     pse_tile_kernel<<<(unsigned)tiles, kPseThreads, 0, g->stream>>>(a);
     ++g->launches;
-    stage_end(g, 2 + 2 * mode);
+    stage_end(g, 2 + 2 * walk);
     CK(cudaGetLastError());
-    stage_begin(g, 3 + 2 * mode);
+    stage_begin(g, 3 + 2 * walk);
     pse_resolve_kernel<<<148 * 8, 256, 0, g->stream>>>(a);
     ++g->launches;
-    stage_end(g, 3 + 2 * mode);
+    stage_end(g, 3 + 2 * walk);
     CK(cudaGetLastError());
   }
-  if (P == 0) CK(cudaMemsetAsync(&g->d_status->num_nodes, 0, 8, g->stream));
+  if (mode == kRunParse && P > 0) {  // parse_test's productions at production_t width
+    narrow_u32_kernel<<<(unsigned)std::min<uint64_t>((P + 1023) / 1024, 148 * 8), 256, 0, g->stream>>>(
+        (const uint32_t *)g->pr.p, g->node_prods.p, P, prod_w);
+    ++g->launches;
+    CK(cudaGetLastError());
+  }
+  if (P == 0 || mode == kRunParse) CK(cudaMemsetAsync(&g->d_status->num_nodes, 0, 8, g->stream));
   CK(cudaEventRecord(g->ev1, g->stream));
   int rc = sync_status(g);
   if (rc) return rc;
@@ -357,6 +391,11 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
   if (cudaEventElapsedTime(&ms, g->ev0, g->ev1) == cudaSuccess) g->last_ms = ms;
   collect_stages(g);
   if (g->h_status->reject) return ALPACC_REJECT;
+  if (mode == kRunParse) {
+    g->last_T = T;
+    g->last_N = P;
+    return ALPACC_OK;
+  }
   if (P == 0 && T != 0) return ALPACC_REJECT;  // compact_tree: terminal count mismatch
   g->last_T = T;
   g->last_N = g->h_status->num_nodes;
@@ -478,7 +517,7 @@ void alpacc_gpu_free(alpacc_gpu_grammar *g) {
 }
 
 int alpacc_gpu_parse_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, alpacc_result *out) {
-  if (!g || !out || (n > 0 && !d_in)) return ALPACC_E_INVALID;
+  if (!g || !out || (n > 0 && !d_in) || g->hg.parts != ALPACC_PARTS_BOTH) return ALPACC_E_INVALID;
   if (cudaSetDevice(g->device) != cudaSuccess) return ALPACC_E_CUDA;
   int rc = run_device(g, d_in, n);
   g->last_status = rc;
@@ -487,7 +526,7 @@ int alpacc_gpu_parse_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t
 }
 
 int alpacc_gpu_enqueue(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n) {
-  if (!g || (n > 0 && !d_in)) return ALPACC_E_INVALID;
+  if (!g || (n > 0 && !d_in) || g->hg.parts != ALPACC_PARTS_BOTH) return ALPACC_E_INVALID;
   if (cudaSetDevice(g->device) != cudaSuccess) return ALPACC_E_CUDA;
   int rc = run_device(g, d_in, n);
   g->last_status = rc;
@@ -503,6 +542,7 @@ int alpacc_gpu_collect(alpacc_gpu_grammar *g, alpacc_result *out) {
 int alpacc_gpu_parse(alpacc_gpu_grammar *g, const uint8_t *in, uint64_t n, alpacc_result *out) {
   if (!g || !out || (n > 0 && !in)) return ALPACC_E_INVALID;
   std::memset(out, 0, sizeof(*out));
+  if (g->hg.parts != ALPACC_PARTS_BOTH) return ALPACC_E_INVALID;
   if (cudaSetDevice(g->device) != cudaSuccess) return ALPACC_E_CUDA;
   int rc = grow(g->in, n + 16);
   if (rc) return rc;
@@ -540,9 +580,106 @@ void alpacc_result_free(alpacc_result *r) {
   std::memset(r, 0, sizeof(*r));
 }
 
+int alpacc_gpu_lex(alpacc_gpu_grammar *g, const uint8_t *in, uint64_t n, alpacc_result *out) {
+  if (!g || !out || (n > 0 && !in)) return ALPACC_E_INVALID;
+  std::memset(out, 0, sizeof(*out));
+  if (g->hg.parts == ALPACC_PARTS_PARSER) return ALPACC_E_INVALID;
+  if (cudaSetDevice(g->device) != cudaSuccess) return ALPACC_E_CUDA;
+  int rc = grow(g->in, n + 16);
+  if (rc) return rc;
+  g->h_in = in;
+  g->host_out = true;
+  rc = run_device(g, (const uint8_t *)g->in.p, n, kRunLex);
+  g->h_in = nullptr;
+  g->host_out = false;
+  g->last_status = rc;
+  if (rc == ALPACC_OK && !g->tok_block) rc = start_token_copy(g, g->last_T);  // empty input: no lexer ran
+  if (rc != ALPACC_OK) {
+    cudaStreamSynchronize(g->cstream);  // no piece copy may still read the caller's buffer
+    abandon_host_result(g);
+    return rc;
+  }
+  if (cudaStreamSynchronize(g->cstream) != cudaSuccess) {
+    abandon_host_result(g);
+    return ALPACC_E_CUDA;
+  }
+  PinnedBlock *toks = reinterpret_cast<PinnedBlock *>(g->tok_block);
+  g->tok_block = nullptr;
+  out->valid = 1;
+  out->num_tokens = g->last_T;
+  out->token_ids = (char *)toks + g->tok_off[0];
+  out->token_starts = (char *)toks + g->tok_off[1];
+  out->token_lengths = (char *)toks + g->tok_off[2];
+  out->internal = toks;
+  return ALPACC_OK;
+}
+
+int alpacc_gpu_parse_tokens(alpacc_gpu_grammar *g, const void *tokens, uint64_t n, alpacc_result *out) {
+  if (!g || !out || (n > 0 && !tokens)) return ALPACC_E_INVALID;
+  std::memset(out, 0, sizeof(*out));
+  if (g->hg.parts == ALPACC_PARTS_LEXER) return ALPACC_E_INVALID;
+  if (n > (1ull << 31) - 1) return ALPACC_E_CAPACITY;
+  if (cudaSetDevice(g->device) != cudaSuccess) return ALPACC_E_CUDA;
+  const alpacc_tables &tb = g->hg.t;
+  int rc = grow(g->tok_ids, std::max<uint64_t>(n, 1) * tb.terminal_size);
+  if (rc) return rc;
+  if (n) CK(cudaMemcpyAsync(g->tok_ids.p, tokens, n * tb.terminal_size, cudaMemcpyHostToDevice, g->stream));
+  rc = run_device(g, nullptr, n, kRunParse);
+  g->last_status = rc;
+  if (rc != ALPACC_OK) {
+    cudaStreamSynchronize(g->stream);  // the token copy may still read the caller's buffer
+    return rc;
+  }
+  const uint64_t P = g->last_N;
+  const size_t bytes = P * tb.production_size;
+  PinnedBlock *b = acquire_block(g, &g->pinned_cache, &g->pinned_cache_size, sizeof(PinnedBlock) + bytes);
+  if (!b) return ALPACC_E_NOMEM;
+  if (bytes && (cudaMemcpyAsync(b + 1, g->node_prods.p, bytes, cudaMemcpyDeviceToHost, g->stream) != cudaSuccess ||
+                cudaStreamSynchronize(g->stream) != cudaSuccess)) {
+    release_block(g, b, false);
+    return ALPACC_E_CUDA;
+  }
+  out->valid = 1;
+  out->num_nodes = P;
+  out->node_productions = b + 1;
+  out->internal = b;
+  return ALPACC_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// The lexer-mode record's lexemes (terminal_t, index_t, length_t each),
+// interleaved in a bounded buffer and written in large pieces.
+void write_lexemes(FILE *out, const alpacc_tables &tb, const alpacc_result &r) {
+  const size_t tw = tb.terminal_size, iw = tb.index_size, lw = tb.length_size, rec = tw + iw + lw;
+  const size_t per = 1 << 16;
+  std::vector<uint8_t> buf(per * rec);
+  for (uint64_t i0 = 0; i0 < r.num_tokens; i0 += per) {
+    const uint64_t cnt = std::min<uint64_t>(per, r.num_tokens - i0);
+    uint8_t *p = buf.data();
+    for (uint64_t i = i0; i < i0 + cnt; i++) {
+      std::memcpy(p, (const uint8_t *)r.token_ids + i * tw, tw);
+      std::memcpy(p + tw, (const uint8_t *)r.token_starts + i * iw, iw);
+      std::memcpy(p + tw + iw, (const uint8_t *)r.token_lengths + i * lw, lw);
+      p += rec;
+    }
+    fwrite(buf.data(), rec, cnt, out);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
 int alpacc_gpu_run_case(alpacc_gpu_grammar *g, uint64_t n, const uint8_t *in, FILE *out) {
+  if (!g || !out) return ALPACC_E_INVALID;
   alpacc_result r;
-  int rc = alpacc_gpu_parse(g, in, n, &r);
+  const int parts = g->hg.parts;
+  int rc = parts == ALPACC_PARTS_LEXER    ? alpacc_gpu_lex(g, in, n, &r)
+           : parts == ALPACC_PARTS_PARSER ? alpacc_gpu_parse_tokens(g, in, n, &r)
+                                          : alpacc_gpu_parse(g, in, n, &r);
   if (rc == ALPACC_REJECT) {
     fputc(0, out);
     return rc;
@@ -551,21 +688,36 @@ int alpacc_gpu_run_case(alpacc_gpu_grammar *g, uint64_t n, const uint8_t *in, FI
   const alpacc_tables &tb = g->hg.t;
   fputc(1, out);
   uint64_t T = r.num_tokens, N = r.num_nodes;
-  fwrite(&T, 8, 1, out);
-  fwrite(r.token_ids, tb.terminal_size, T, out);
-  fwrite(r.token_starts, tb.index_size, T, out);
-  fwrite(r.token_lengths, tb.length_size, T, out);
-  fwrite(&N, 8, 1, out);
-  fwrite(r.node_productions, tb.production_size, N, out);
-  fwrite(r.node_parents, tb.index_size, N, out);
-  fwrite(r.token_parents, tb.index_size, T, out);
+  if (parts == ALPACC_PARTS_LEXER) {  // C/Generator.hs:87-102
+    fwrite(&T, 8, 1, out);
+    write_lexemes(out, tb, r);
+  } else if (parts == ALPACC_PARTS_PARSER) {  // C/Generator.hs:65-79
+    fwrite(&N, 8, 1, out);
+    fwrite(r.node_productions, tb.production_size, N, out);
+  } else {  // C/Generator.hs:114-152
+    fwrite(&T, 8, 1, out);
+    fwrite(r.token_ids, tb.terminal_size, T, out);
+    fwrite(r.token_starts, tb.index_size, T, out);
+    fwrite(r.token_lengths, tb.length_size, T, out);
+    fwrite(&N, 8, 1, out);
+    fwrite(r.node_productions, tb.production_size, N, out);
+    fwrite(r.node_parents, tb.index_size, N, out);
+    fwrite(r.token_parents, tb.index_size, T, out);
+  }
   alpacc_result_free(&r);
   return rc;
 }
 
+// print_layout of each mode (C/Generator.hs:80-84, 103-107, 153-158)
 int alpacc_gpu_layout(const alpacc_gpu_grammar *g, char *buf, size_t len) {
   if (!g) return ALPACC_E_INVALID;
   const alpacc_tables &tb = g->hg.t;
+  if (g->hg.parts == ALPACC_PARTS_LEXER)
+    return snprintf(buf, len, "terminal_t=%u\nindex_t=%u\nlength_t=%u\n", tb.terminal_size, tb.index_size,
+                    tb.length_size);
+  if (g->hg.parts == ALPACC_PARTS_PARSER)
+    return snprintf(buf, len, "terminal_t=%u\nproduction_t=%u\nindex_t=%u\n", tb.terminal_size,
+                    tb.production_size, tb.index_size);
   return snprintf(buf, len, "terminal_t=%u\nproduction_t=%u\nindex_t=%u\nlength_t=%u\n", tb.terminal_size,
                   tb.production_size, tb.index_size, tb.length_size);
 }
@@ -587,7 +739,8 @@ const char *alpacc_strerror(int status) {
 double alpacc_gpu_last_ms(alpacc_gpu_grammar *g) { return g ? g->last_ms : -1.0; }
 
 int alpacc_gpu_autotune(alpacc_gpu_grammar *g, const uint8_t *d_sample, uint64_t n, int *choice) {
-  if (!g || (n > 0 && !d_sample)) return ALPACC_E_INVALID;
+  if (!g || (n > 0 && !d_sample) || g->hg.parts == ALPACC_PARTS_PARSER) return ALPACC_E_INVALID;
+  const int run_mode = g->hg.parts == ALPACC_PARTS_LEXER ? kRunLex : kRunBoth;
   if (cudaSetDevice(g->device) != cudaSuccess) return ALPACC_E_CUDA;
   const int keep = g->trans_rep;
   const size_t per_copy = (size_t)g->trans_word_count * 4 + 512;
@@ -608,7 +761,7 @@ int alpacc_gpu_autotune(alpacc_gpu_grammar *g, const uint8_t *d_sample, uint64_t
     double ms = 0;
     int ok = 1;
     for (int rep = 0; rep < 3 && ok; ++rep) {  // first run warms up
-      const int rc = run_device(g, d_sample, n);
+      const int rc = run_device(g, d_sample, n, run_mode);
       if (rc < 0) ok = 0;
       else if (rep > 0) ms += g->stage_ms[0];
     }

@@ -302,6 +302,7 @@ int run_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offset
 extern "C" int alpacc_gpu_parse_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offsets,
                                       uint32_t count, alpacc_result *outs) {
   if (!g || !offsets || (count && !outs)) return ALPACC_E_INVALID;
+  if (g->hg.parts != ALPACC_PARTS_BOTH) return ALPACC_E_INVALID;  // the batch path is the combined one
   for (uint32_t i = 0; i < count; i++) {
     if (offsets[i + 1] < offsets[i] || offsets[i + 1] - offsets[i] > (int64_t)(1ll << 31) - 1)
       return ALPACC_E_INVALID;

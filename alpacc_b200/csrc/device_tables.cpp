@@ -258,11 +258,15 @@ static int build_pairs(const alpacc_tables *t, PairTable *pt, std::string *why) 
     if (sym >= (1ull << 31)) { *why = "bracket symbol too large"; return ALPACC_E_UNSUPPORTED; }
     pt->stacks[i] = (uint32_t)sym | ((b & top) ? 0x80000000u : 0u);
   }
-  const uint64_t P = t->number_of_productions;
+  // the parser-mode program carries no production count and no arities
+  const uint64_t P = t->parts == ALPACC_PARTS_BOTH ? t->number_of_productions : 0;
   pt->prods.resize(t->productions_size);
   for (uint64_t i = 0; i < t->productions_size; i++) {
     uint64_t p = read_uint(t->productions, i, t->production_size);
-    if (p >= P) { *why = "production id out of range"; return ALPACC_E_INVALID; }
+    if ((t->parts == ALPACC_PARTS_BOTH && p >= P) || p >= (1ull << 31)) {
+      *why = "production id out of range";
+      return ALPACC_E_INVALID;
+    }
     pt->prods[i] = (uint32_t)p;
   }
   pt->arity.resize(P);
@@ -277,33 +281,42 @@ static int build_pairs(const alpacc_tables *t, PairTable *pt, std::string *why) 
 
 int build_host_grammar(const alpacc_tables *t, HostGrammar *out, std::string *why) {
   if (!t || t->abi_version != ALPACC_ABI_VERSION) { *why = "abi_version mismatch"; return ALPACC_E_INVALID; }
-  if (!valid_width(t->terminal_size) || !valid_width(t->production_size) || !valid_width(t->bracket_size) ||
-      !valid_width(t->state_size) || !(t->index_size == 4 || t->index_size == 8) || !valid_width(t->length_size)) {
+  if (t->parts > ALPACC_PARTS_PARSER) { *why = "unknown parts value"; return ALPACC_E_INVALID; }
+  const bool lexer = t->parts != ALPACC_PARTS_PARSER, parser = t->parts != ALPACC_PARTS_LEXER;
+  if (!valid_width(t->terminal_size) || !(t->index_size == 4 || t->index_size == 8) ||
+      (lexer && (!valid_width(t->state_size) || !valid_width(t->length_size))) ||
+      (parser && (!valid_width(t->production_size) || !valid_width(t->bracket_size)))) {
     *why = "bad type width";
     return ALPACC_E_INVALID;
   }
-  if (!t->to_state || !t->compose || !t->accept || !t->hash_table_is_valid || !t->hash_table_keys ||
-      !t->hash_table_stacks_span || !t->hash_table_productions_span || !t->production_to_arity ||
-      !t->production_to_terminal_is_valid || (t->stacks_size && !t->stacks) ||
-      (t->productions_size && !t->productions) || t->num_states == 0 || t->hash_table_size == 0) {
+  const bool tree = t->parts == ALPACC_PARTS_BOTH;  // arities only in the combined program
+  if ((lexer && (!t->to_state || !t->compose || !t->accept || t->num_states == 0)) ||
+      (parser && (!t->hash_table_is_valid || !t->hash_table_keys || !t->hash_table_stacks_span ||
+                  !t->hash_table_productions_span || (t->stacks_size && !t->stacks) ||
+                  (t->productions_size && !t->productions) || t->hash_table_size == 0)) ||
+      (tree && (!t->production_to_arity || !t->production_to_terminal_is_valid))) {
     *why = "missing table";
     return ALPACC_E_INVALID;
   }
-  if (t->end_terminal > 255 || t->start_terminal > 255 || t->empty_terminal > 255) {
+  if (parser && (t->end_terminal > 255 || t->start_terminal > 255 || t->empty_terminal > 255)) {
     *why = "terminal ids above 255 are not supported";
     return ALPACC_E_UNSUPPORTED;
   }
   out->t = *t;
-  out->ignore = t->ignore_token >= 0 ? (int)t->ignore_token : -1;
-  out->len_max = t->length_size >= 8 ? ~0ull : ((1ull << (8 * t->length_size)) - 1);
-  int rc = build_lexer(t, out->ignore, &out->lex, why);
-  if (rc != ALPACC_OK) return rc;
-  for (uint8_t tm : out->lex.term)
-    if ((uint64_t)tm > t->end_terminal) {
-      *why = "a lexer terminal id is not a parser terminal";
-      return ALPACC_E_INVALID;
-    }
-  return build_pairs(t, &out->pairs, why);
+  out->parts = (int)t->parts;
+  out->ignore = lexer && t->ignore_token >= 0 ? (int)t->ignore_token : -1;
+  out->len_max = !lexer || t->length_size >= 8 ? ~0ull : ((1ull << (8 * t->length_size)) - 1);
+  if (lexer) {
+    int rc = build_lexer(t, out->ignore, &out->lex, why);
+    if (rc != ALPACC_OK) return rc;
+    if (parser)
+      for (uint8_t tm : out->lex.term)
+        if ((uint64_t)tm > t->end_terminal) {
+          *why = "a lexer terminal id is not a parser terminal";
+          return ALPACC_E_INVALID;
+        }
+  }
+  return parser ? build_pairs(t, &out->pairs, why) : ALPACC_OK;
 }
 
 }  // namespace alpacc

@@ -61,6 +61,7 @@ struct HostGrammar {
   PairTable pairs;
   uint64_t len_max = 0;
   int ignore = -1;
+  int parts = 0;      // ALPACC_PARTS_*
 };
 
 // Validates the tables and builds the device forms. Returns ALPACC_OK or an

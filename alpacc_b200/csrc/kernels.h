@@ -187,5 +187,6 @@ struct PseArgs {
 
 __global__ void pse_tile_kernel(PseArgs args);
 __global__ void pse_resolve_kernel(PseArgs args);
+__global__ void narrow_u32_kernel(const uint32_t *src, void *dst, unsigned long long count, int width);
 
 }  // namespace alpacc

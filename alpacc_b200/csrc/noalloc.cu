@@ -79,6 +79,7 @@ extern "C" int alpacc_gpu_lex_noalloc(alpacc_gpu_grammar *g, const uint8_t *d_in
                                       void *d_token_starts, void *d_token_lengths, uint64_t *num_tokens) {
   if (!g || !num_tokens || (n > 0 && (!d_in || !d_token_ids || !d_token_starts || !d_token_lengths)))
     return ALPACC_E_INVALID;
+  if (g->hg.parts == ALPACC_PARTS_PARSER) return ALPACC_E_INVALID;  // tables without a lexer
   if (n > kNoAllocMaxInput) return ALPACC_E_CAPACITY;  // inputs above 16 MiB need the allocating path
   *num_tokens = 0;
   if (n == 0) return ALPACC_OK;  // lex_string accepts the empty input with no tokens

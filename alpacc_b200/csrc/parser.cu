@@ -694,4 +694,20 @@ __global__ void __launch_bounds__(1024) batch_plan_kernel(BatchDesc b, int kind,
   if (t == 0) tile0[b.docs] = (unsigned long long)carry;
 }
 
+// ---------------------------------------------------------------------------
+// Parser-mode output: the u32 production ids of the pair stage narrowed to
+// production_t (the width parse_test writes). Each thread converts 4
+// consecutive ids per step.
+// ---------------------------------------------------------------------------
+
+__global__ void narrow_u32_kernel(const uint32_t *src, void *dst, unsigned long long count, int width) {
+  const unsigned long long quads = (count + 3) / 4;
+  for (unsigned long long q = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; q < quads;
+       q += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long i0 = 4 * q;
+    const int k = count - i0 < 4 ? (int)(count - i0) : 4;
+    for (int j = 0; j < k; ++j) store_uint(dst, i0 + j, width, __ldg(src + i0 + j));
+  }
+}
+
 }  // namespace alpacc

@@ -129,7 +129,7 @@ alpacc_server *alpacc_server_start(const alpacc_tables *tables, int device, int 
                                    int *err) {
   int dummy;
   if (!err) err = &dummy;
-  if (!tables || workers < 1 || workers > 16) {
+  if (!tables || workers < 1 || workers > 16 || tables->parts != ALPACC_PARTS_BOTH) {
     *err = ALPACC_E_INVALID;
     return nullptr;
   }

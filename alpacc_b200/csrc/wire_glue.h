@@ -1,10 +1,19 @@
 /*
  * Glue between a grammar's emitted constants (the C emitter's output,
  * src/Alpacc/Generator/C/{Lexer,Parser}.hs) and the C ABI: builds the
- * alpacc_tables descriptor from the constants in scope and loads the grammar
- * on device 0 on first use.
+ * alpacc_tables descriptor from the constants in scope (those of the
+ * combined, lexer-mode or parser-mode program) and loads the grammar on
+ * device 0 on first use.
  */
 #include "alpacc_b200.h"
+
+/* Bytes per unit of a frame's n: terminal ids for the parser-mode program
+   (INPUT_BYTES, C/Generator.hs:66, 88, 116). */
+#if defined(Q) && !defined(NUM_TRANS)
+#define WIRE_UNIT ((uint64_t)sizeof(terminal_t))
+#else
+#define WIRE_UNIT ((uint64_t)1)
+#endif
 
 static alpacc_gpu_grammar *gpu_grammar(void) {
   static alpacc_gpu_grammar *g = NULL;
@@ -13,11 +22,17 @@ static alpacc_gpu_grammar *gpu_grammar(void) {
     memset(&t, 0, sizeof t);
     t.abi_version = ALPACC_ABI_VERSION;
     t.terminal_size = sizeof(terminal_t);
-    t.production_size = sizeof(production_t);
-    t.bracket_size = sizeof(bracket_t);
-    t.state_size = sizeof(state_t);
     t.index_size = sizeof(index_t);
     t.length_size = sizeof(length_t);
+#if defined(NUM_TRANS) && defined(Q)
+    t.parts = ALPACC_PARTS_BOTH;
+#elif defined(NUM_TRANS)
+    t.parts = ALPACC_PARTS_LEXER;
+#else
+    t.parts = ALPACC_PARTS_PARSER;
+#endif
+#ifdef NUM_TRANS /* lexer constants (C/Lexer.hs:16-58) */
+    t.state_size = sizeof(state_t);
     t.num_states = NUM_STATES;
     t.endo_mask = ENDO_MASK;
     t.endo_offset = ENDO_OFFSET;
@@ -34,6 +49,10 @@ static alpacc_gpu_grammar *gpu_grammar(void) {
     t.to_state = TO_STATE;
     t.compose = COMPOSE;
     t.accept = (const uint8_t *)ACCEPT;
+#endif
+#ifdef Q /* parser constants (C/Parser.hs:21-95) */
+    t.production_size = sizeof(production_t);
+    t.bracket_size = sizeof(bracket_t);
     t.q = Q;
     t.k = K;
     t.empty_terminal = EMPTY_TERMINAL;
@@ -51,9 +70,12 @@ static alpacc_gpu_grammar *gpu_grammar(void) {
     t.hash_table_keys = HASH_TABLE_KEYS;
     t.hash_table_stacks_span = &HASH_TABLE_STACKS_SPAN[0][0];
     t.hash_table_productions_span = &HASH_TABLE_PRODUCTIONS_SPAN[0][0];
+#endif
+#ifdef ALPACC_WITH_TREE
     t.number_of_productions = NUMBER_OF_PRODUCTIONS;
     t.production_to_arity = PRODUCTION_TO_ARITY;
     t.production_to_terminal_is_valid = (const uint8_t *)PRODUCTION_TO_TERMINAL_IS_VALID;
+#endif
     int err = 0;
     g = alpacc_gpu_load(&t, 0, 0, &err);
     if (!g) {

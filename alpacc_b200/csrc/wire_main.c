@@ -1,6 +1,7 @@
 /*
  * Wire-protocol program around the B200 path (docs/wire-protocols.md of
- * alpacc): the same interface as a generated combined-mode program
+ * alpacc): the same interface as a generated combined-, lexer- or
+ * parser-mode program
  * (backends/c/cli.c) — counted batches of frames on stdin, one response
  * record per frame on stdout, `--server` loops over batches until EOF with a
  * flush after every record, `--layout` prints the native type sizes.
@@ -42,7 +43,7 @@ static int one_frame(FILE *in, FILE *out) {
   }
   uint64_t n;
   memcpy(&n, frame, 8);
-  if (frame_len != 8 + n) {
+  if (n > (frame_len - 8) / WIRE_UNIT || n * WIRE_UNIT != frame_len - 8) {
     fprintf(stderr, "error: frame length mismatch\n");
     free(frame);
     return -1;

@@ -135,9 +135,12 @@ def parser_constants(t: GrammarTables, with_tree: bool = True) -> str:
     return text
 
 
+PROGRAM_KIND = {"both": "combined lexer+parser", "lexer": "lexer", "parser": "parser"}
+
+
 def program_prefix(t: GrammarTables) -> str:
-    """Everything before the lexer constants (C/Generator.hs:188-196)."""
-    meta = ["// alpacc combined lexer+parser for grammar %s" % t.name]
+    """Everything before the lexer or parser constants (C/Generator.hs:161-196)."""
+    meta = ["// alpacc %s for grammar %s" % (PROGRAM_KIND[t.parts], t.name)]
     return unlines([
         unlines(meta),
         unlines(INCLUDES),
@@ -145,3 +148,15 @@ def program_prefix(t: GrammarTables) -> str:
         index_typedef(t),
         unlines(["static void     write_u64le(FILE *f, uint64_t v);"]),
     ])
+
+
+def constants(t: GrammarTables) -> str:
+    """The constant sections of the program ``t.parts`` names: the lexer's for
+    the lexer-mode program, the parser's without the tree section for the
+    parser-mode one, both (with the tree section) for the combined one."""
+    parts = [program_prefix(t)]
+    if t.parts != "parser":
+        parts.append(lexer_constants(t))
+    if t.parts != "lexer":
+        parts.append(parser_constants(t, with_tree=t.parts == "both"))
+    return unlines(parts)

@@ -84,6 +84,9 @@ class GrammarTables:
     terminal_names: list = field(default_factory=list)
     production_names: list = field(default_factory=list)
     llp_pairs: dict = field(default_factory=dict)  # int key tuple -> (brackets, prods)
+    # which program the tables belong to: "both" (combined), "lexer" (lexer
+    # constants only, lexer numbering) or "parser" (parser constants, no tree)
+    parts: str = "both"
 
     @property
     def hash_size(self) -> int:
@@ -110,6 +113,7 @@ class GrammarTables:
         h.update(struct.pack("<10q", self.q, self.k, int(self.index32), self.terminal_bits, self.production_bits,
                              self.bracket_bits, self.length_bits, self.lexer.identity, self.max_iters,
                              -1 if self.ignore_token is None else self.ignore_token))
+        h.update(self.parts.encode())
         return h.hexdigest()[:16]
 
 
@@ -205,6 +209,64 @@ def open_addressing(items):
     return arr, max_iters
 
 
+def _length_bits(cfg: CFG, index32: bool) -> int:
+    if cfg.params.length is not None:
+        return cfg.params.length
+    return 32 if index32 else 64
+
+
+def generate_lexer(text: str, name: str = "grammar", index32: bool = False) -> GrammarTables:
+    """The lexer-mode program's tables (``mkLexer``, Analyzer.hs:114-150).
+
+    The DFA is the combined program's, but terminals are numbered by the
+    lexer's own encoder (``encodeTerminals`` over ``parsingTerminals
+    (dfaTerminals spec)``, Encode.hs:144-158, Grammar.hs:321-325): the lexer
+    spec's terminals in ``Ord T`` order (``Map.keys`` of its order map,
+    DFA.hs:312-313) with ``ignore`` moved behind them, then ``Unused`` (the
+    dead token). The combined program numbers them in declaration order
+    instead, so the two programs can give one token different ids. Parser
+    fields are empty."""
+    cfg = parse_alp(text)
+    rules = lexer_spec(cfg)
+    ign = T("ignore")
+    lts = sorted({t for t, _ in rules})
+    order = [t for t in lts if t != ign] + ([ign] if ign in lts else [])
+    lid = {t: i for i, t in enumerate(order)}
+    dead = len(order)
+    pl = lexgen.parallel_lexer(lexgen.merged_lexer_dfa(rules))
+    enc_lex = lexgen.encode_lexer(pl, lambda r: lid[rules[r][0]], dead + 1, dead)
+    # nameTerminals (Analyzer.hs:104-111)
+    names = [t[1] if t[0] == 0 else "literal_%d" % i for i, t in enumerate(order)] + ["empty_%d" % dead]
+    return GrammarTables(
+        name=name, q=0, k=0, index32=index32,
+        terminal_bits=lexgen.uint_type_bits(dead), production_bits=8, bracket_bits=8,
+        length_bits=_length_bits(cfg, index32),
+        lexer=enc_lex, ignore_token=lid.get(ign), dead_token=dead,
+        empty_terminal=dead, start_terminal=0, end_terminal=0,
+        stacks=np.zeros(0, dtype=np.uint8), productions=np.zeros(0, dtype=np.uint8),
+        ht_valid=np.zeros(0, dtype=np.bool_), ht_keys=np.zeros((0, 0), dtype=np.uint64),
+        ht_stack_span=np.zeros((0, 2), dtype=np.int64), ht_prod_span=np.zeros((0, 2), dtype=np.int64),
+        max_iters=0, max_brackets_per_pos=0, max_prods_per_pos=0,
+        arity=np.zeros(0, dtype=np.uint64), prod_is_terminal=np.zeros(0, dtype=np.bool_),
+        terminal_names=names, production_names=[], parts="lexer",
+    )
+
+
+def generate_parts(text: str, name: str = "grammar", index32: bool = False, parts: str = "both") -> GrammarTables:
+    """Tables of the combined (``both``), lexer-mode (``lexer``) or
+    parser-mode (``parser``) program. The parser-mode program (``mkParser``,
+    Analyzer.hs:167-209) numbers symbols exactly as the combined one, so its
+    tables are the combined tables' parser part."""
+    if parts == "lexer":
+        return generate_lexer(text, name, index32)
+    t = generate(text, name, index32)
+    if parts == "parser":
+        t.parts = "parser"
+    elif parts != "both":
+        raise ValueError("parts must be both, lexer or parser")
+    return t
+
+
 def generate(text: str, name: str = "grammar", index32: bool = False) -> GrammarTables:
     """Build every table of the combined program for an ``.alp`` grammar
     (``mkLexerParser``, Analyzer.hs:211-279)."""
@@ -285,10 +347,7 @@ def generate(text: str, name: str = "grammar", index32: bool = False) -> Grammar
     enc_lex = lexgen.encode_lexer(pl, lambda r: term_id[used(rules[r][0])], num_lex_terminals, empty_terminal)
     ignore_token = term_id.get(used(T("ignore")))
 
-    if cfg.params.length is not None:
-        length_bits = cfg.params.length
-    else:
-        length_bits = 32 if index32 else 64
+    length_bits = _length_bits(cfg, index32)
 
     return GrammarTables(
         name=name, q=q, k=k, index32=index32,

@@ -39,7 +39,7 @@ class Tables(ctypes.Structure):
     _fields_ = [
         ("abi_version", ctypes.c_uint32), ("terminal_size", ctypes.c_uint32), ("production_size", ctypes.c_uint32),
         ("bracket_size", ctypes.c_uint32), ("state_size", ctypes.c_uint32), ("index_size", ctypes.c_uint32),
-        ("length_size", ctypes.c_uint32), ("reserved0", ctypes.c_uint32),
+        ("length_size", ctypes.c_uint32), ("parts", ctypes.c_uint32),
         ("num_states", ctypes.c_uint64), ("endo_mask", ctypes.c_uint64), ("endo_offset", ctypes.c_uint64),
         ("terminal_mask", ctypes.c_uint64), ("terminal_offset", ctypes.c_uint64), ("produce_mask", ctypes.c_uint64),
         ("produce_offset", ctypes.c_uint64), ("identity", ctypes.c_uint64), ("ignore_token", ctypes.c_int64),
@@ -107,6 +107,11 @@ def lib():
         L.alpacc_gpu_parse_batch.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
                                              ctypes.POINTER(Result)]
         L.alpacc_result_free.argtypes = [ctypes.POINTER(Result)]
+        L.alpacc_gpu_lex.restype = ctypes.c_int
+        L.alpacc_gpu_lex.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Result)]
+        L.alpacc_gpu_parse_tokens.restype = ctypes.c_int
+        L.alpacc_gpu_parse_tokens.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                              ctypes.POINTER(Result)]
         L.alpacc_gpu_layout.restype = ctypes.c_int
         L.alpacc_gpu_layout.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
         L.alpacc_strerror.restype = ctypes.c_char_p
@@ -128,10 +133,16 @@ def lib():
     return _lib
 
 
+PARTS = {"both": 0, "lexer": 1, "parser": 2}
+
+
 def make_tables(t):
-    """Fill the C struct from generated tables; returns (struct, keepalive)."""
+    """Fill the C struct from generated tables; returns (struct, keepalive).
+    The fields of the part a lexer-mode or parser-mode program lacks stay zero
+    / NULL, as that program has no such constants."""
     L = t.lexer
     keep = []
+    parts = getattr(t, "parts", "both")
 
     def arr(a, dtype=None):
         a = np.ascontiguousarray(a if dtype is None else np.asarray(a).astype(dtype))
@@ -146,6 +157,16 @@ def make_tables(t):
     s.state_size = L.state_bits // 8
     s.index_size = t.index_bits // 8
     s.length_size = t.length_bits // 8
+    s.parts = PARTS[parts]
+    if parts != "parser":
+        _lexer_fields(s, t, arr)
+    if parts != "lexer":
+        _parser_fields(s, t, arr, tree=parts == "both")
+    return s, keep
+
+
+def _lexer_fields(s, t, arr):
+    L = t.lexer
     s.num_states = L.num_states
     s.endo_mask, s.endo_offset = L.index_mask, L.index_offset
     s.terminal_mask, s.terminal_offset = L.token_mask, L.token_offset
@@ -155,6 +176,9 @@ def make_tables(t):
     s.to_state = arr(L.to_state)
     s.compose = arr(L.compose)
     s.accept = arr(L.accept, np.uint8)
+
+
+def _parser_fields(s, t, arr, tree: bool):
     s.q, s.k = t.q, t.k
     s.empty_terminal, s.start_terminal, s.end_terminal = t.empty_terminal, t.start_terminal, t.end_terminal
     s.hash_table_size = t.hash_size
@@ -168,10 +192,10 @@ def make_tables(t):
     s.hash_table_keys = arr(t.ht_keys, tw)
     s.hash_table_stacks_span = arr(t.ht_stack_span, np.int64)
     s.hash_table_productions_span = arr(t.ht_prod_span, np.int64)
-    s.number_of_productions = t.num_productions
-    s.production_to_arity = arr(t.arity, np.uint64)
-    s.production_to_terminal_is_valid = arr(t.prod_is_terminal, np.uint8)
-    return s, keep
+    if tree:
+        s.number_of_productions = t.num_productions
+        s.production_to_arity = arr(t.arity, np.uint64)
+        s.production_to_terminal_is_valid = arr(t.prod_is_terminal, np.uint8)
 
 
 def _np_from(ptr, count, nbytes, signed=False):
@@ -239,6 +263,37 @@ class Parser:
         finally:
             lib().alpacc_result_free(ctypes.byref(r))
 
+    def lex(self, data) -> wire.LexResult:
+        """Lexer-only mode (``alpacc_gpu_lex``): the lexemes of the input, or a
+        reject."""
+        a = np.ascontiguousarray(np.frombuffer(bytes(data), dtype=np.uint8))
+        r = Result()
+        rc = self._check(lib().alpacc_gpu_lex(self._h, a.ctypes.data, a.size, ctypes.byref(r)))
+        try:
+            if rc != OK:
+                return wire.LexResult(False)
+            lay, T = self.layout, r.num_tokens
+            return wire.LexResult(True, _np_from(r.token_ids, T, lay.terminal),
+                                  _np_from(r.token_starts, T, lay.index, True),
+                                  _np_from(r.token_lengths, T, lay.length))
+        finally:
+            lib().alpacc_result_free(ctypes.byref(r))
+
+    def parse_tokens(self, tokens) -> wire.TokenParseResult:
+        """Parser-only mode (``alpacc_gpu_parse_tokens``): terminal ids in, the
+        production sequence of the derivation (or a reject) out."""
+        lay = self.layout
+        a = np.ascontiguousarray(np.asarray(tokens).astype(wire._dt(lay.terminal)))
+        r = Result()
+        rc = self._check(lib().alpacc_gpu_parse_tokens(self._h, a.ctypes.data if a.size else None, a.size,
+                                                       ctypes.byref(r)))
+        try:
+            if rc != OK:
+                return wire.TokenParseResult(False)
+            return wire.TokenParseResult(True, _np_from(r.node_productions, r.num_nodes, lay.production))
+        finally:
+            lib().alpacc_result_free(ctypes.byref(r))
+
     def autotune(self, dev_ptr: int, n: int) -> int:
         """Pick the lexer's table copies on a device-resident sample; returns the choice."""
         c = ctypes.c_int(0)
@@ -294,7 +349,15 @@ class Parser:
                                 dl(r.node_parents, N, lay.index, True), dl(r.token_parents, T, lay.index, True))
 
     def run_case(self, data) -> bytes:
-        """The response record bytes ``run_case`` would write."""
+        """The response record bytes ``run_case`` of this grammar's program
+        (combined, lexer-mode or parser-mode) would write; for the parser-mode
+        program ``data`` is the terminal ids' bytes."""
+        parts = getattr(self.tables, "parts", "both")
+        if parts == "lexer":
+            return wire.encode_lex_record(self.lex(data), self.layout)
+        if parts == "parser":
+            toks = np.frombuffer(bytes(data), dtype=wire._dt(self.layout.terminal))
+            return wire.encode_token_parse_record(self.parse_tokens(toks), self.layout)
         return wire.encode_record(self.parse(data), self.layout)
 
     def counts(self) -> dict:

@@ -1,7 +1,8 @@
 """Build a grammar's wire-protocol program on the B200 path.
 
-The program is what alpacc's C emitter would generate for combined mode,
-except that ``run_case`` goes through the C ABI: the grammar's constants
+The program is what alpacc's C emitter would generate for the tables' mode
+(combined, lexer-only or parser-only), except that ``run_case`` goes through
+the C ABI: the grammar's constants
 (emitted as the reference emitter writes them, ``grammar/emit_c.py``), the glue
 that fills ``alpacc_tables`` from them (``csrc/wire_glue.h``) and the batch /
 server / layout loop (``csrc/wire_main.c``), linked against
@@ -22,9 +23,7 @@ CSRC = os.path.join(HERE, "csrc")
 
 def source(tables) -> str:
     parts = [
-        emit_c.program_prefix(tables),
-        emit_c.lexer_constants(tables),
-        emit_c.parser_constants(tables, with_tree=True),
+        emit_c.constants(tables),
         '#include "wire_glue.h"',
         '#include "wire_main.c"',
     ]

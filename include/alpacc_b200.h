@@ -17,6 +17,10 @@
  *   - ``run_case(uint64_t n, const uint8_t *in, FILE *out)``
  *     (src/Alpacc/Generator/C/Generator.hs:114-152)      -> alpacc_gpu_run_case
  *     and its in-memory form                            -> alpacc_gpu_parse
+ *   - the lexer-mode and parser-mode ``run_case`` (C/Generator.hs:64-108) and
+ *     the CUDA backend's ``lex_one`` / ``runParserPipeline``
+ *     (backends/cuda/cli.cu:237-275, 513-526)  -> alpacc_gpu_lex,
+ *                                                  alpacc_gpu_parse_tokens
  *   - ``print_layout`` (C/Generator.hs:153-158, cli.c --layout)
  *                                                       -> alpacc_gpu_layout
  *
@@ -50,6 +54,19 @@ extern "C" {
 #define ALPACC_E_UNSUPPORTED (-6) /* tables exceed what the kernels handle */
 
 /*
+ * Which tables a generated program holds (src/Alpacc/Generator/C/Generator.hs:
+ * 161-201): the combined program has both, the lexer-mode program only the
+ * lexer constants (with the lexer's own terminal numbering, mkLexer in
+ * src/Alpacc/Generator/Analyzer.hs:114-150), the parser-mode program only
+ * the parser constants without the tree section (no arities: the
+ * production_to_* pointers are NULL and number_of_productions is 0). Fields
+ * of the absent part are ignored.
+ */
+#define ALPACC_PARTS_BOTH 0
+#define ALPACC_PARTS_LEXER 1
+#define ALPACC_PARTS_PARSER 2
+
+/*
  * Grammar tables exactly as alpacc's C emitter produces them. Element widths
  * are given in bytes; arrays use those native widths, little-endian.
  */
@@ -61,7 +78,7 @@ typedef struct alpacc_tables {
   uint32_t state_size;         /* sizeof(state_t)      */
   uint32_t index_size;         /* sizeof(index_t): 4 (--index32) or 8 */
   uint32_t length_size;        /* sizeof(length_t)     */
-  uint32_t reserved0;
+  uint32_t parts;              /* ALPACC_PARTS_*: which program the tables come from */
   /* lexer: C/Lexer.hs:16-58 */
   uint64_t num_states;         /* NUM_STATES (endomorphisms) */
   uint64_t endo_mask, endo_offset;
@@ -209,13 +226,41 @@ int alpacc_server_stats(alpacc_server *s, int64_t *vals, int n);
 void alpacc_server_stop(alpacc_server *s);
 
 /*
- * Write the combined-mode response record for input `in` to `out`, byte for
- * byte what the generated run_case writes: u8 valid, then (when valid) the
- * token and tree sections. Returns the status of the parse.
+ * Lexer-only mode: the lexemes of lex_string (backends/c/lexer.c:39-97) for
+ * host bytes, as the lexer-mode program's run_case (C/Generator.hs:87-102) and
+ * the CUDA backend's lex_one (backends/cuda/cli.cu:237-275) compute them.
+ * Fills valid, num_tokens, token_ids, token_starts and token_lengths; the tree
+ * fields stay 0 / NULL. Works on lexer-only and combined tables (token ids
+ * follow the tables' own numbering).
+ */
+int alpacc_gpu_lex(alpacc_gpu_grammar *g, const uint8_t *in, uint64_t n, alpacc_result *out);
+
+/*
+ * Parser-only mode: `tokens` holds n terminal_t ids (host memory); the result
+ * is parse_test's production sequence (backends/c/parser.c:49-98; the
+ * parser-mode run_case, C/Generator.hs:65-79; runParserPipeline of
+ * backends/cuda/cli.cu:513-526): valid, num_nodes = number of productions,
+ * node_productions = production_t[num_nodes] in derivation order (not
+ * compacted); the token and parent fields stay 0 / NULL. Works on parser-only
+ * and combined tables.
+ */
+int alpacc_gpu_parse_tokens(alpacc_gpu_grammar *g, const void *tokens, uint64_t n, alpacc_result *out);
+
+/*
+ * Write the response record of the handle's mode for one input to `out`, byte
+ * for byte what the generated run_case writes (u8 valid, then when valid):
+ *   combined tables: the token and tree sections (C/Generator.hs:114-152),
+ *     `in` = n bytes;
+ *   lexer-only tables: u64 count, then per lexeme terminal_t, index_t start,
+ *     length_t length (C/Generator.hs:87-102), `in` = n bytes;
+ *   parser-only tables: u64 count, then production_t ids
+ *     (C/Generator.hs:65-79), `in` = n terminal_t ids.
+ * Returns the status of the call.
  */
 int alpacc_gpu_run_case(alpacc_gpu_grammar *g, uint64_t n, const uint8_t *in, FILE *out);
 
-/* `--layout` text ("terminal_t=1\nproduction_t=1\n..."); returns its length. */
+/* `--layout` text of the handle's mode ("terminal_t=1\nproduction_t=1\n...",
+   the lines print_layout writes in that mode); returns its length. */
 int alpacc_gpu_layout(const alpacc_gpu_grammar *g, char *buf, size_t len);
 
 /* Human-readable text of a status code. */

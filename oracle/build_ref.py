@@ -14,6 +14,11 @@ emitter would generate for a grammar (src/Alpacc/Generator/C/Generator.hs:161-20
 then compiles it with ``cc -std=c99 -O2`` (as tests/test-long-input.sh:72 does)
 into ``oracle/_ref/<config>`` (the wire-protocol CLI) and, together with
 ``oracle/ref_harness.c``, into ``oracle/_ref/lib<config>.so`` for in-memory calls.
+
+The lexer-mode and parser-mode programs (C/Generator.hs:161-186) are assembled
+the same way from ``lexerTestCase`` / ``parserTestCase`` with only the lexer's
+(``backends/c/lexer.c``) or only the parser's (``backends/c/parser.c``, no tree
+constants) part, as ``<config>_lexer`` and ``<config>_parser``.
 Nothing from the reference is written outside ``oracle/_ref/`` (git-ignored).
 
 Usage: python oracle/build_ref.py [--reference /root/reference] [config ...]
@@ -23,6 +28,7 @@ from __future__ import annotations
 
 import argparse
 import ast
+import hashlib
 import os
 import re
 import subprocess
@@ -58,6 +64,10 @@ def haskell_text_block(hs_source: str, name: str) -> str:
     return "".join(l + "\n" for l in lines)
 
 
+# configurations whose lexer-mode and parser-mode programs are also built
+MODE_CONFIGS = ("arithmetic_i64", "json_i32", "json_ext_i32", "sexp_i64", "paper_grammar_i64", "llp01_i64")
+
+
 def assemble(reference: str, tables) -> str:
     from alpacc_b200.grammar import emit_c
 
@@ -66,6 +76,14 @@ def assemble(reference: str, tables) -> str:
             return f.read()
 
     gen_hs = rd("src/Alpacc/Generator/C/Generator.hs")
+    if tables.parts == "lexer":  # auxiliary, Lex case (C/Generator.hs:164-174)
+        parts = [emit_c.program_prefix(tables), emit_c.lexer_constants(tables), rd("backends/c/lexer.c"),
+                 haskell_text_block(gen_hs, "lexerTestCase"), rd("backends/c/cli.c")]
+        return "".join(p + "\n" for p in parts)
+    if tables.parts == "parser":  # auxiliary, Parse case (C/Generator.hs:176-186)
+        parts = [emit_c.program_prefix(tables), emit_c.parser_constants(tables, with_tree=False),
+                 rd("backends/c/parser.c"), haskell_text_block(gen_hs, "parserTestCase"), rd("backends/c/cli.c")]
+        return "".join(p + "\n" for p in parts)
     both_case = haskell_text_block(gen_hs, "bothTestCase")
     parts = [
         emit_c.program_prefix(tables),
@@ -79,17 +97,19 @@ def assemble(reference: str, tables) -> str:
     return "".join(p + "\n" for p in parts)
 
 
-def build(config: str, reference: str, cc: str = "gcc", force: bool = False) -> str:
+def build(config: str, reference: str, cc: str = "gcc", force: bool = False, parts: str = "both") -> str:
     from alpacc_b200.grammar.cache import load_tables
 
     gfile, index32 = CONFIGS[config]
     os.makedirs(OUT, exist_ok=True)
-    src = os.path.join(OUT, config + ".c")
-    exe = os.path.join(OUT, config)
-    so = os.path.join(OUT, "lib%s.so" % config)
-    tables = load_tables(os.path.join(REPO, "grammars", gfile), index32=index32)
-    stamp = os.path.join(OUT, config + ".stamp")
-    key = tables.digest()
+    name = config if parts == "both" else "%s_%s" % (config, parts)
+    src = os.path.join(OUT, name + ".c")
+    exe = os.path.join(OUT, name)
+    so = os.path.join(OUT, "lib%s.so" % name)
+    tables = load_tables(os.path.join(REPO, "grammars", gfile), index32=index32, parts=parts)
+    stamp = os.path.join(OUT, name + ".stamp")
+    with open(os.path.join(HERE, "ref_harness.c"), "rb") as f:
+        key = tables.digest() + ":" + hashlib.sha256(f.read()).hexdigest()[:12]
     if not force and os.path.exists(so) and os.path.exists(exe) and os.path.exists(stamp):
         with open(stamp) as f:
             if f.read().strip() == key:
@@ -116,6 +136,9 @@ def main(argv=None):
         return 0
     for c in a.configs or list(CONFIGS):
         print("building", c, "->", build(c, a.reference, force=a.force))
+        if c in MODE_CONFIGS:
+            for parts in ("lexer", "parser"):
+                print("building", c, parts, "->", build(c, a.reference, force=a.force, parts=parts))
     return 0
 
 

@@ -13,6 +13,8 @@
  *   compute_parents  backends/c/parser.c:103-118
  *   compact_tree     backends/c/parser.c:126-153
  *   run_case         src/Alpacc/Generator/C/Generator.hs:114-152 (record bytes)
+ *                    and, by the tables' `parts`, the lexer-mode (:87-102) and
+ *                    parser-mode (:65-79) run_case
  *
  * Build: gcc -O2 -std=c99 -shared -fPIC oracle.c -o _port/liboracle_port.so
  */
@@ -189,8 +191,59 @@ static void put(uint8_t **buf, size_t *len, size_t *cap, const void *src, size_t
 
 static void put_uint(uint8_t **buf, size_t *len, size_t *cap, uint64_t v, uint32_t w) { put(buf, len, cap, &v, w); }
 
-/* run_case (src/Alpacc/Generator/C/Generator.hs:114-152) into a malloc'd buffer. */
+/* The lexer-mode run_case (src/Alpacc/Generator/C/Generator.hs:87-102):
+   u8 valid, u64 count, per lexeme terminal_t, index_t start, length_t length. */
+static int lexer_run_case(const alpacc_tables *t, uint64_t n, const uint8_t *in, uint8_t **out, size_t *out_len) {
+  uint8_t *buf = NULL;
+  size_t len = 0, cap = 0;
+  const uint8_t zero = 0, one = 1;
+  lexeme *lx = NULL;
+  uint64_t nl = 0;
+  if (!lex(t, in, n, &lx, &nl)) {
+    put(&buf, &len, &cap, &zero, 1);
+  } else {
+    put(&buf, &len, &cap, &one, 1);
+    put_uint(&buf, &len, &cap, nl, 8);
+    for (uint64_t i = 0; i < nl; i++) {
+      put_uint(&buf, &len, &cap, lx[i].terminal, t->terminal_size);
+      put_uint(&buf, &len, &cap, lx[i].start, t->index_size);
+      put_uint(&buf, &len, &cap, lx[i].length, t->length_size);
+    }
+    free(lx);
+  }
+  *out = buf;
+  *out_len = len;
+  return 1;
+}
+
+/* The parser-mode run_case (src/Alpacc/Generator/C/Generator.hs:65-79): the
+   input is n terminal_t ids; u8 valid, u64 count, production_t[count]. */
+static int parser_run_case(const alpacc_tables *t, uint64_t n, const uint8_t *in, uint8_t **out, size_t *out_len) {
+  uint8_t *buf = NULL;
+  size_t len = 0, cap = 0;
+  const uint8_t zero = 0, one = 1;
+  uint64_t *tokens = (uint64_t *)malloc((n + 1) * sizeof(uint64_t));
+  for (uint64_t i = 0; i < n; i++) tokens[i] = rd(in, i, t->terminal_size);
+  uint64_t *prods = NULL, np = 0;
+  if (!parse(t, tokens, n, &prods, &np)) {
+    put(&buf, &len, &cap, &zero, 1);
+  } else {
+    put(&buf, &len, &cap, &one, 1);
+    put_uint(&buf, &len, &cap, np, 8);
+    for (uint64_t i = 0; i < np; i++) put_uint(&buf, &len, &cap, prods[i], t->production_size);
+    free(prods);
+  }
+  free(tokens);
+  *out = buf;
+  *out_len = len;
+  return 1;
+}
+
+/* run_case (src/Alpacc/Generator/C/Generator.hs:114-152) into a malloc'd
+   buffer; lexer-only and parser-only tables give their mode's record. */
 int oracle_run_case(const alpacc_tables *t, uint64_t n, const uint8_t *in, uint8_t **out, size_t *out_len) {
+  if (t->parts == ALPACC_PARTS_LEXER) return lexer_run_case(t, n, in, out, out_len);
+  if (t->parts == ALPACC_PARTS_PARSER) return parser_run_case(t, n, in, out, out_len);
   uint8_t *buf = NULL;
   size_t len = 0, cap = 0;
   const uint8_t zero = 0, one = 1;

@@ -50,7 +50,9 @@ class PortOracle:
     def run_case(self, data: bytes) -> bytes:
         out = ctypes.POINTER(ctypes.c_uint8)()
         n = ctypes.c_size_t()
-        lib().oracle_run_case(ctypes.addressof(self.struct), len(data), data, ctypes.byref(out), ctypes.byref(n))
+        # the parser-mode program's input is counted in terminal ids
+        count = len(data) // self.struct.terminal_size if self.struct.parts == 2 else len(data)
+        lib().oracle_run_case(ctypes.addressof(self.struct), count, data, ctypes.byref(out), ctypes.byref(n))
         try:
             return ctypes.string_at(out, n.value)
         finally:

@@ -29,17 +29,21 @@ class RefOracle:
                                           ctypes.POINTER(ctypes.POINTER(ctypes.c_uint8)),
                                           ctypes.POINTER(ctypes.c_size_t)]
         self.lib.ref_run_case.restype = ctypes.c_int
-        self.lib.ref_pipeline.argtypes = [ctypes.c_uint64, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64),
-                                          ctypes.POINTER(ctypes.c_uint64)]
-        self.lib.ref_pipeline.restype = ctypes.c_int
+        if hasattr(self.lib, "ref_pipeline"):  # combined programs only
+            self.lib.ref_pipeline.argtypes = [ctypes.c_uint64, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64),
+                                              ctypes.POINTER(ctypes.c_uint64)]
+            self.lib.ref_pipeline.restype = ctypes.c_int
         self.lib.ref_free.argtypes = [ctypes.c_void_p]
         self.lib.ref_layout.argtypes = [ctypes.POINTER(ctypes.c_uint64)]
+        self.lib.ref_input_unit.restype = ctypes.c_uint64
 
     def run_case(self, data: bytes) -> bytes:
-        """The exact response record ``run_case`` writes for ``data``."""
+        """The exact response record ``run_case`` writes for ``data`` (bytes;
+        for a parser-mode program the terminal ids' bytes)."""
         out = ctypes.POINTER(ctypes.c_uint8)()
         n = ctypes.c_size_t()
-        if self.lib.ref_run_case(len(data), data, ctypes.byref(out), ctypes.byref(n)) != 0:
+        count = len(data) // self.lib.ref_input_unit()
+        if self.lib.ref_run_case(count, data, ctypes.byref(out), ctypes.byref(n)) != 0:
             raise RuntimeError("open_memstream failed")
         try:
             return ctypes.string_at(out, n.value)

@@ -12,7 +12,10 @@
  *     open_memstream;
  *   - ref_pipeline: lex_string -> parse_test -> compute_parents -> compact_tree
  *     without serialisation, the in-memory timing harness for the CPU baseline;
- *   - ref_layout: the type sizes print_layout reports.
+ *   - ref_layout: the type sizes print_layout reports;
+ *   - ref_input_unit: the bytes per unit of run_case's n.
+ * The same harness wraps the lexer-mode and parser-mode programs (no
+ * ref_pipeline there).
  */
 #define main alpacc_generated_main
 #include ALPACC_GENERATED
@@ -32,7 +35,12 @@ int ref_run_case(uint64_t n, const uint8_t *in, uint8_t **out, size_t *out_len) 
 
 void ref_free(void *p) { free(p); }
 
-/* Returns 1 when accepted (sets the counts), 0 when rejected. */
+/* Units of run_case's n: bytes, or terminal ids in the parser-mode program
+   (INPUT_BYTES, C/Generator.hs:66, 88). */
+uint64_t ref_input_unit(void) { return INPUT_BYTES(1); }
+
+#ifdef ALPACC_WITH_TREE
+/* Combined programs: returns 1 when accepted (sets the counts), 0 when rejected. */
 int ref_pipeline(uint64_t n, const uint8_t *in, uint64_t *num_tokens, uint64_t *num_nodes) {
   lexeme_t *lexemes;
   uint64_t num_lexemes;
@@ -68,9 +76,16 @@ int ref_pipeline(uint64_t n, const uint8_t *in, uint64_t *num_tokens, uint64_t *
   return ok ? 1 : 0;
 }
 
+#endif
+
+/* Type sizes; production_t is 0 in the lexer-mode program, which has none. */
 void ref_layout(uint64_t *sizes) {
   sizes[0] = sizeof(terminal_t);
+#ifdef Q
   sizes[1] = sizeof(production_t);
+#else
+  sizes[1] = 0;
+#endif
   sizes[2] = sizeof(index_t);
   sizes[3] = sizeof(length_t);
 }

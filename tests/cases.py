@@ -26,14 +26,24 @@ CONFIGS = {
     "llp01_i64": ("llp01.alp", False),
 }
 
+# configurations whose lexer-mode and parser-mode programs are tested too
+MODE_CONFIGS = ("arithmetic_i64", "json_i32", "json_ext_i32", "sexp_i64", "paper_grammar_i64", "llp01_i64")
+
 _TABLES = {}
 
 
-def tables(config: str):
-    if config not in _TABLES:
+def tables(config: str, parts: str = "both"):
+    """Tables of the combined program of ``config``, or of its lexer-mode /
+    parser-mode program."""
+    if (config, parts) not in _TABLES:
         g, i32 = CONFIGS[config]
-        _TABLES[config] = load_tables(os.path.join(GRAMMARS, g), index32=i32)
-    return _TABLES[config]
+        _TABLES[(config, parts)] = load_tables(os.path.join(GRAMMARS, g), index32=i32, parts=parts)
+    return _TABLES[(config, parts)]
+
+
+def mode_name(config: str, parts: str) -> str:
+    """Name of the reference program built for ``config`` in that mode."""
+    return config if parts == "both" else "%s_%s" % (config, parts)
 
 
 FIXED = {
@@ -146,4 +156,39 @@ def case_inputs(config: str, sizes=TILE_SIZES, seeds=(0, 1)):
             d = generated(config, max(n, 2) if f != "sexp" else max(n, 4), 100 + s + n)
             out.append(d)
             out.append(mutate(d, rng, 1 + int(rng.integers(0, 3))))
+    return out
+
+
+def token_inputs(config: str, sizes=(1, 64, 1000, 20000), seeds=(0,)):
+    """Parser-mode inputs (terminal ids as bytes at terminal_t width): the
+    tokens of the accepted case inputs, and mutations of them that delete,
+    swap or insert ids, including ids outside the grammar's terminal range."""
+    from alpacc_b200 import wire
+    from oracle.port import PortOracle
+
+    t = tables(config)
+    lay = wire.Layout.of(t)
+    dt = np.dtype("<u%d" % lay.terminal)
+    po = PortOracle(t)
+    rng = np.random.default_rng(4321)
+    hi = min(256, 1 << t.terminal_bits)
+    out = [b""]
+    for data in case_inputs(config, sizes=sizes, seeds=seeds):
+        r, _ = wire.decode_record(po.run_case(data), lay)
+        if not r.valid:
+            continue
+        ids = np.asarray(r.token_ids, dtype=np.int64)
+        out.append(ids.astype(dt).tobytes())
+        for _ in range(2):
+            m = list(ids)
+            for _ in range(1 + int(rng.integers(0, 3))):
+                op = int(rng.integers(0, 3))
+                if op == 0 and m:
+                    del m[int(rng.integers(0, len(m)))]
+                elif op == 1 and len(m) > 1:
+                    i, j = rng.integers(0, len(m), 2)
+                    m[i], m[j] = m[j], m[i]
+                else:
+                    m.insert(int(rng.integers(0, len(m) + 1)), int(rng.integers(0, hi)))
+            out.append(np.asarray(m, dtype=np.int64).astype(dt).tobytes())
     return out

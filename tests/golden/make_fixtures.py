@@ -11,7 +11,10 @@ box never runs this script. It writes
   productions-only form;
 * ``records.json`` - response records written by the reference's C backend
   (oracle/_ref, built by oracle/build_ref.py) for small inputs of every grammar
-  configuration, as hex.
+  configuration, as hex;
+* ``records_modes.json`` - the same for the lexer-mode and parser-mode
+  programs (oracle/_ref/<config>_lexer, <config>_parser): bytes in for the
+  lexer, terminal ids in for the parser.
 """
 
 from __future__ import annotations
@@ -208,6 +211,27 @@ def records() -> dict:
     return out
 
 
+def mode_records() -> dict:
+    from oracle.ref import RefOracle, available
+    from tests import cases
+
+    out = {}
+    for config in cases.MODE_CONFIGS:
+        for parts in ("lexer", "parser"):
+            name = cases.mode_name(config, parts)
+            if not available(name):
+                continue
+            ref = RefOracle(name)
+            if parts == "lexer":
+                ins = list(cases.FIXED[cases.family(config)])
+                ins += [cases.generated(config, n, 7 + n) for n in (16, 100, 700)]
+                ins += [b"\xff", b"\x00 \x7f"]  # bytes no grammar here lexes
+            else:
+                ins = cases.token_inputs(config, sizes=(16, 100), seeds=(0,))
+            out[name] = [{"input": d.hex(), "record": ref.run_case(d).hex()} for d in ins]
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -218,7 +242,11 @@ def main(argv=None):
     rec = records()
     with open(os.path.join(HERE, "records.json"), "w") as f:
         json.dump(rec, f, indent=1, sort_keys=True)
-    print("known answers:", sorted(ka), "records:", {k: len(v) for k, v in rec.items()})
+    modes = mode_records()
+    with open(os.path.join(HERE, "records_modes.json"), "w") as f:
+        json.dump(modes, f, indent=1, sort_keys=True)
+    print("known answers:", sorted(ka), "records:", {k: len(v) for k, v in rec.items()},
+          "mode records:", {k: len(v) for k, v in modes.items()})
 
 
 if __name__ == "__main__":

@@ -72,3 +72,18 @@ def test_strerror_and_invalid_tables_without_gpu():
     err = ctypes.c_int(0)
     h = lib.alpacc_gpu_load(ctypes.byref(bad), 0, 0, ctypes.byref(err))
     assert not h and err.value == native.E_INVALID
+
+
+def test_parts_validation_without_gpu():
+    """Tables of a lexer-mode or parser-mode program are checked for the part
+    they carry before any device work; an unknown parts value is refused."""
+    lib = native.lib()
+    err = ctypes.c_int(0)
+    for parts in (native.PARTS["lexer"], native.PARTS["parser"], 7):
+        t = native.Tables()
+        t.abi_version = native.ABI_VERSION
+        t.terminal_size, t.index_size, t.length_size = 1, 4, 4
+        t.state_size, t.production_size, t.bracket_size = 2, 1, 1
+        t.parts = parts  # no tables attached
+        h = lib.alpacc_gpu_load(ctypes.byref(t), 0, 0, ctypes.byref(err))
+        assert not h and err.value == native.E_INVALID

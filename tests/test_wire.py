@@ -38,3 +38,31 @@ def test_batch_framing():
 def test_layout_text():
     lay = wire.Layout.of(cases.tables("json_ext_i32"))
     assert lay.text() == "terminal_t=1\nproduction_t=1\nindex_t=4\nlength_t=2\n"
+
+
+def test_mode_records_round_trip_golden():
+    """Lexer-mode and parser-mode records decode and re-encode to the
+    reference's bytes."""
+    recs = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "records_modes.json")))
+    for name, items in recs.items():
+        parts = "lexer" if name.endswith("_lexer") else "parser"
+        config = name[: -len(parts) - 1]
+        lay = wire.Layout.of(cases.tables(config, parts))
+        for item in items:
+            rec = bytes.fromhex(item["record"])
+            if parts == "lexer":
+                r, pos = wire.decode_lex_record(rec, lay)
+                assert wire.encode_lex_record(r, lay) == rec
+            else:
+                r, pos = wire.decode_token_parse_record(rec, lay)
+                assert wire.encode_token_parse_record(r, lay) == rec
+            assert pos == len(rec)
+
+
+def test_mode_layout_text_and_frames():
+    lex = wire.Layout.of(cases.tables("json_i32", "lexer"))
+    par = wire.Layout.of(cases.tables("json_i32", "parser"))
+    assert lex.text() == "terminal_t=1\nindex_t=4\nlength_t=2\n"  # json.alp: 16-bit lengths
+    assert par.text() == "terminal_t=1\nproduction_t=1\nindex_t=4\n"
+    frame = wire.encode_mode_frame(b"\x01\x02\x03", par)
+    assert frame[:16] == (11).to_bytes(8, "little") + (3).to_bytes(8, "little")
