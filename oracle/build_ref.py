@@ -101,13 +101,24 @@ def build(config: str, reference: str, cc: str = "gcc", force: bool = False, par
     from alpacc_b200.grammar.cache import load_tables
 
     gfile, index32 = CONFIGS[config]
-    os.makedirs(OUT, exist_ok=True)
     name = config if parts == "both" else "%s_%s" % (config, parts)
-    src = os.path.join(OUT, name + ".c")
-    exe = os.path.join(OUT, name)
-    so = os.path.join(OUT, "lib%s.so" % name)
     tables = load_tables(os.path.join(REPO, "grammars", gfile), index32=index32, parts=parts)
-    stamp = os.path.join(OUT, name + ".stamp")
+    return compile_program(tables, name, OUT, reference, cc, force)
+
+
+def build_tables(tables, name: str, reference: str, cc: str = "gcc") -> str:
+    """The reference program for tables generated from any grammar text (the
+    random grammars of the differential fuzz tests), under oracle/_ref/fuzz/."""
+    return compile_program(tables, name, os.path.join(OUT, "fuzz"), reference, cc, False, opt="-O1")
+
+
+def compile_program(tables, name: str, out: str, reference: str, cc: str = "gcc", force: bool = False,
+                    opt: str = "-O2") -> str:
+    os.makedirs(out, exist_ok=True)
+    src = os.path.join(out, name + ".c")
+    exe = os.path.join(out, name)
+    so = os.path.join(out, "lib%s.so" % name)
+    stamp = os.path.join(out, name + ".stamp")
     with open(os.path.join(HERE, "ref_harness.c"), "rb") as f:
         key = tables.digest() + ":" + hashlib.sha256(f.read()).hexdigest()[:12]
     if not force and os.path.exists(so) and os.path.exists(exe) and os.path.exists(stamp):
@@ -117,8 +128,8 @@ def build(config: str, reference: str, cc: str = "gcc", force: bool = False, par
     text = assemble(reference, tables)
     with open(src, "w", encoding="utf-8") as f:
         f.write(text)
-    subprocess.check_call([cc, "-std=c99", "-O2", "-o", exe, src])
-    subprocess.check_call([cc, "-std=c99", "-O2", "-shared", "-fPIC", "-o", so,
+    subprocess.check_call([cc, "-std=c99", opt, "-o", exe, src])
+    subprocess.check_call([cc, "-std=c99", opt, "-shared", "-fPIC", "-o", so,
                            "-DALPACC_GENERATED=\"%s\"" % src, os.path.join(HERE, "ref_harness.c")])
     with open(stamp, "w") as f:
         f.write(key)

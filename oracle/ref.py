@@ -19,8 +19,8 @@ def available(config: str) -> bool:
 class RefOracle:
     """The reference C backend for one grammar configuration."""
 
-    def __init__(self, config: str):
-        path = os.path.join(REF_DIR, "lib%s.so" % config)
+    def __init__(self, config: str, path: str = None):
+        path = path or os.path.join(REF_DIR, "lib%s.so" % config)
         if not os.path.exists(path):
             raise FileNotFoundError("%s missing: run oracle/build_ref.py %s" % (path, config))
         self.config = config

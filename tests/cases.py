@@ -160,20 +160,25 @@ def case_inputs(config: str, sizes=TILE_SIZES, seeds=(0, 1)):
 
 
 def token_inputs(config: str, sizes=(1, 64, 1000, 20000), seeds=(0,)):
+    """Parser-mode inputs for ``config`` (see ``token_inputs_for``)."""
+    return token_inputs_for(tables(config), case_inputs(config, sizes=sizes, seeds=seeds))
+
+
+def token_inputs_for(t, inputs, seed: int = 4321):
     """Parser-mode inputs (terminal ids as bytes at terminal_t width): the
-    tokens of the accepted case inputs, and mutations of them that delete,
-    swap or insert ids, including ids outside the grammar's terminal range."""
+    tokens of the accepted inputs under the combined tables ``t``, and
+    mutations of them that delete, swap or insert ids, including ids outside
+    the grammar's terminal range."""
     from alpacc_b200 import wire
     from oracle.port import PortOracle
 
-    t = tables(config)
     lay = wire.Layout.of(t)
     dt = np.dtype("<u%d" % lay.terminal)
     po = PortOracle(t)
-    rng = np.random.default_rng(4321)
+    rng = np.random.default_rng(seed)
     hi = min(256, 1 << t.terminal_bits)
     out = [b""]
-    for data in case_inputs(config, sizes=sizes, seeds=seeds):
+    for data in inputs:
         r, _ = wire.decode_record(po.run_case(data), lay)
         if not r.valid:
             continue
