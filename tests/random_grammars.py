@@ -208,7 +208,8 @@ class RandomGrammar:
         return [s.encode() for s in out]
 
 
-QKS = ((1, 1), (1, 2), (2, 1), (2, 2))
+# the lookback/lookahead pairs of the reference's random-grammar matrix (Makefile:79-88)
+QKS = ((0, 1), (1, 1), (2, 2), (3, 3))
 
 
 def fuzz_grammars(count: int, first_seed: int = 0):

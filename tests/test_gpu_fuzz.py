@@ -1,5 +1,5 @@
 """Random-grammar differential fuzzing of the CUDA path: for grammars drawn like
-``alpacc random`` (tests/random_grammars.py, q and k in 1..2), the device
+``alpacc random`` (tests/random_grammars.py, the reference's (q, k) matrix), the device
 path's records against the C restatement oracle (itself checked against the
 reference's C programs on the same grammars in tests/test_fuzz.py) in the
 combined, lexer-only and parser-only modes, and the batched form against the
