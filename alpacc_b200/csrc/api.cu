@@ -207,9 +207,17 @@ int finish_host_result(alpacc_gpu_grammar *g, alpacc_result *out) {
 // (parser-mode program: pairs and the bracket walk, no tree).
 enum RunMode { kRunBoth = 0, kRunLex = 1, kRunParse = 2 };
 
+// One window of chunked lexing (kRunLex): whether the input continues after
+// the window, and the window's offset (added to token starts).
+struct LexWindow {
+  int open_end;
+  uint64_t index_base;
+};
+
 // The whole device path for d_in[0..n) (n bytes; n token ids for kRunParse).
 // Leaves counts in g->last_T / last_N.
-int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int mode = kRunBoth) {
+int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int mode = kRunBoth,
+               const LexWindow *win = nullptr) {
   const HostGrammar &hg = g->hg;
   const alpacc_tables &tb = hg.t;
   const LexerMachine &lm = hg.lex;
@@ -263,7 +271,9 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int mode 
     CK(cudaMemsetAsync(g->st1_flag.p, 0, tiles * 4, g->stream));
     CK(cudaMemsetAsync(g->st2_flags.p, 0, tiles * 4, g->stream));
     LexArgs a = lex_args(g, d_in, n, tiles);
-    const LexPlaceArgs pa = lex_place_args(g, a, tiles);
+    if (win) a.open_end = win->open_end;
+    LexPlaceArgs pa = lex_place_args(g, a, tiles);
+    if (win) pa.index_base = win->index_base;
     stage_begin(g, 0);
     for (uint64_t k = 0; k < pieces; ++k) {
       const uint64_t tb = k * piece_tiles, te = std::min(tiles, tb + piece_tiles);
@@ -614,6 +624,63 @@ int alpacc_gpu_lex(alpacc_gpu_grammar *g, const uint8_t *in, uint64_t n, alpacc_
   return ALPACC_OK;
 }
 
+int alpacc_gpu_lex_stream(alpacc_gpu_grammar *g, const uint8_t *in, uint64_t n, uint64_t window,
+                          alpacc_lex_sink sink, void *user, uint64_t *num_tokens) {
+  if (!g || !sink || (n > 0 && !in)) return ALPACC_E_INVALID;
+  if (num_tokens) *num_tokens = 0;
+  if (g->hg.parts == ALPACC_PARTS_PARSER) return ALPACC_E_INVALID;
+  const alpacc_tables &tb = g->hg.t;
+  if (tb.index_size < 8 && n > (1ull << 31) - 1) return ALPACC_E_CAPACITY;  // starts must fit index_t
+  if (cudaSetDevice(g->device) != cudaSuccess) return ALPACC_E_CUDA;
+  constexpr uint64_t kMaxWindow = (1ull << 31) - 1;  // the lexer kernels' 31-bit positions
+  uint64_t w = window ? std::min(window, kMaxWindow) : (1ull << 30);
+  uint64_t s = 0, total = 0;
+  while (s < n) {
+    const uint64_t e = n - s <= w ? n : s + w;
+    const LexWindow win{e < n ? 1 : 0, s};
+    int rc = grow(g->in, (e - s) + 16);
+    if (rc) return rc;
+    g->h_in = in + s;
+    rc = run_device(g, (const uint8_t *)g->in.p, e - s, kRunLex, &win);
+    g->h_in = nullptr;
+    if (rc != ALPACC_OK) {
+      cudaStreamSynchronize(g->cstream);  // no piece copy may still read the caller's buffer
+      return rc;
+    }
+    const uint64_t T = g->last_T;
+    const uint64_t lb = g->h_status->last_boundary;
+    if (win.open_end && lb == 0) {  // one token spans the whole window: widen it and lex again
+      if (w >= kMaxWindow) return ALPACC_E_CAPACITY;
+      w = std::min(2 * w, kMaxWindow);
+      continue;
+    }
+    if (T) {
+      const size_t sz[3] = {T * tb.terminal_size, T * tb.index_size, T * tb.length_size};
+      size_t off[3], bytes = sizeof(PinnedBlock);
+      for (int i = 0; i < 3; i++) {
+        off[i] = bytes;
+        bytes += (sz[i] + 15) & ~(size_t)15;
+      }
+      PinnedBlock *b = acquire_block(g, &g->pinned_cache, &g->pinned_cache_size, bytes);
+      if (!b) return ALPACC_E_NOMEM;
+      const void *src[3] = {g->tok_ids.p, g->tok_starts.p, g->tok_lens.p};
+      bool ok = true;
+      for (int i = 0; i < 3 && ok; i++)
+        ok = cudaMemcpyAsync((char *)b + off[i], src[i], sz[i], cudaMemcpyDeviceToHost, g->stream) == cudaSuccess;
+      ok = ok && cudaStreamSynchronize(g->stream) == cudaSuccess;
+      const int stop = ok ? sink(user, total, T, (char *)b + off[0], (char *)b + off[1], (char *)b + off[2]) : 0;
+      release_block(g, b, false);
+      if (!ok) return ALPACC_E_CUDA;
+      if (stop) return ALPACC_E_ABORTED;
+    }
+    total += T;
+    if (num_tokens) *num_tokens = total;
+    if (!win.open_end) break;
+    s += lb;
+  }
+  return ALPACC_OK;
+}
+
 int alpacc_gpu_parse_tokens(alpacc_gpu_grammar *g, const void *tokens, uint64_t n, alpacc_result *out) {
   if (!g || !out || (n > 0 && !tokens)) return ALPACC_E_INVALID;
   std::memset(out, 0, sizeof(*out));
@@ -732,6 +799,7 @@ const char *alpacc_strerror(int status) {
     case ALPACC_E_CAPACITY: return "input exceeds capacity";
     case ALPACC_E_TIMEOUT: return "device wait timed out";
     case ALPACC_E_UNSUPPORTED: return "tables exceed the supported limits";
+    case ALPACC_E_ABORTED: return "stopped by the caller's callback";
   }
   return "unknown status";
 }

@@ -41,6 +41,7 @@ struct DeviceStatus {
   int lex_reject_reason;    // 1 dead state, 2 not accepting, 3 length overflow
   int parse_reject_reason;  // 1 missing pair, 2 bracket mismatch, 3 unbalanced, 4 terminal count
   unsigned long long scratch[4];
+  unsigned long long last_boundary;  // last token boundary of the input (single-document lexer)
 };
 
 // Upper bound on spin iterations of one wait; with the back-off below this is

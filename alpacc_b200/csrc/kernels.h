@@ -94,6 +94,10 @@ struct LexArgs {
   uint32_t *stage_starts, *stage_ends;
   uint32_t *tile_cnt, *tile_pos;
   const BatchDesc *batch;  // null: one document (in, n, status); else tiles are virtual (lex_tile0)
+  // One window of a longer input (chunked lexing): the input continues after
+  // byte n, so the token in progress at n is neither emitted nor judged; the
+  // window's last boundary is left in status->last_boundary. Staged path only.
+  int open_end;
 };
 
 __global__ void lex_kernel(LexArgs args);
@@ -112,6 +116,7 @@ struct LexPlaceArgs {
   unsigned long long len_max;
   DeviceStatus *status;
   const BatchDesc *batch;  // null: one document; else counts restart at each document's first tile
+  unsigned long long index_base;  // added to every token start (a window's offset in chunked lexing)
 };
 
 constexpr int kLexScanThreads = 1024;

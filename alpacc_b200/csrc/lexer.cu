@@ -429,7 +429,7 @@ __global__ void __launch_bounds__(kLexThreads, 6) lex_kernel(LexArgs args) {
         if (sm->sflags[tb8[j]] & 4) ++cnt;
       }
       if (bmask) lastb = g0 + 63 - __clzll((long long)bmask);
-      if (g0 + nb == n) {  // this chunk holds the last byte
+      if (g0 + nb == n && !a.open_end) {  // this chunk holds the last byte of the input
         final_tok = true;
         final_term = sm->sterm[x];
         final_kept = (sm->sflags[x] & 4) != 0;
@@ -580,7 +580,10 @@ __global__ void __launch_bounds__(kLexScanThreads) lex_scan_kernel(LexPlaceArgs 
     }
     carry = SegCntPosOp()(carry, tot);
   }
-  if (t == 0 && !bd) a.status->num_tokens = (unsigned long long)(carry.a);
+  if (t == 0 && !bd) {
+    a.status->num_tokens = (unsigned long long)(carry.a);
+    a.status->last_boundary = (unsigned long long)(carry.b & ~kSeg);
+  }
 }
 
 // Each CTA copies whole tiles' staged tokens to their final places; a token
@@ -606,7 +609,7 @@ __global__ void __launch_bounds__(256) lex_place_kernel(LexPlaceArgs a) {
       const unsigned long long len = end - start;
       if (len > a.len_max) too_long = true;
       store_uint(a.tok_ids, off + i, a.term_w, a.stage_ids[base + i]);
-      store_uint(a.tok_starts, off + i, a.idx_w, start);
+      store_uint(a.tok_starts, off + i, a.idx_w, a.index_base + start);
       store_uint(a.tok_lens, off + i, a.len_w, len);
     }
   }

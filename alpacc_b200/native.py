@@ -25,7 +25,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libalpacc_b200.so")
 
 OK, REJECT = 0, 1
-E_INVALID, E_CUDA, E_NOMEM, E_CAPACITY, E_TIMEOUT, E_UNSUPPORTED = -1, -2, -3, -4, -5, -6
+E_INVALID, E_CUDA, E_NOMEM, E_CAPACITY, E_TIMEOUT, E_UNSUPPORTED, E_ABORTED = -1, -2, -3, -4, -5, -6, -7
 ABI_VERSION = 1
 
 
@@ -64,6 +64,10 @@ class Result(ctypes.Structure):
         ("internal", ctypes.c_void_p),
     ]
 
+
+# int sink(void *user, uint64_t first, uint64_t count, const void *ids, const void *starts, const void *lengths)
+LEX_SINK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p,
+                            ctypes.c_void_p, ctypes.c_void_p)
 
 _lib = None
 
@@ -109,6 +113,9 @@ def lib():
         L.alpacc_result_free.argtypes = [ctypes.POINTER(Result)]
         L.alpacc_gpu_lex.restype = ctypes.c_int
         L.alpacc_gpu_lex.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Result)]
+        L.alpacc_gpu_lex_stream.restype = ctypes.c_int
+        L.alpacc_gpu_lex_stream.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                            LEX_SINK, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]
         L.alpacc_gpu_parse_tokens.restype = ctypes.c_int
         L.alpacc_gpu_parse_tokens.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                               ctypes.POINTER(Result)]
@@ -278,6 +285,40 @@ class Parser:
                                   _np_from(r.token_lengths, T, lay.length))
         finally:
             lib().alpacc_result_free(ctypes.byref(r))
+
+    def lex_stream(self, data, window: int = 0, on_window=None):
+        """Chunked lexing (``alpacc_gpu_lex_stream``): the input is lexed in
+        windows of ``window`` bytes (0: 1 GiB). Without ``on_window`` the
+        windows' lexemes are concatenated into one ``wire.LexResult``; with it,
+        ``on_window(first, ids, starts, lengths)`` gets each window's arrays
+        and nothing is kept. Returns (result or None, number of windows)."""
+        a = data if isinstance(data, np.ndarray) else np.frombuffer(bytes(data), dtype=np.uint8)
+        a = np.ascontiguousarray(a, dtype=np.uint8)
+        lay = self.layout
+        parts = []
+        calls = [0]
+
+        def sink(user, first, count, ids, starts, lens):
+            calls[0] += 1
+            arrs = (_np_from(ids, count, lay.terminal), _np_from(starts, count, lay.index, True),
+                    _np_from(lens, count, lay.length))
+            if on_window is not None:
+                on_window(first, *arrs)
+            else:
+                parts.append(arrs)
+            return 0
+
+        cb = LEX_SINK(sink)
+        nt = ctypes.c_uint64(0)
+        rc = self._check(lib().alpacc_gpu_lex_stream(self._h, a.ctypes.data if a.size else None, a.size, window,
+                                                     cb, None, ctypes.byref(nt)))
+        if rc != OK:
+            return wire.LexResult(False), calls[0]
+        if on_window is not None:
+            return None, calls[0]
+        cat = [np.concatenate([p[i] for p in parts]) if parts else _np_from(0, 0, w, i == 1)
+               for i, w in enumerate((lay.terminal, lay.index, lay.length))]
+        return wire.LexResult(True, *cat), calls[0]
 
     def parse_tokens(self, tokens) -> wire.TokenParseResult:
         """Parser-only mode (``alpacc_gpu_parse_tokens``): terminal ids in, the

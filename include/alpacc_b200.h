@@ -52,6 +52,7 @@ extern "C" {
 #define ALPACC_E_CAPACITY (-4) /* input larger than the configured capacity */
 #define ALPACC_E_TIMEOUT (-5)  /* a bounded device wait gave up */
 #define ALPACC_E_UNSUPPORTED (-6) /* tables exceed what the kernels handle */
+#define ALPACC_E_ABORTED (-7)  /* a caller's callback asked to stop */
 
 /*
  * Which tables a generated program holds (src/Alpacc/Generator/C/Generator.hs:
@@ -234,6 +235,28 @@ void alpacc_server_stop(alpacc_server *s);
  * follow the tables' own numbering).
  */
 int alpacc_gpu_lex(alpacc_gpu_grammar *g, const uint8_t *in, uint64_t n, alpacc_result *out);
+
+/*
+ * Chunked lexing for inputs larger than device memory or than one device pass
+ * (2^31 - 1 bytes): the counterpart of the reference's streaming chunk carry
+ * (LexerCtx::update, backends/cuda/lexer.cu:224-432; lex_step, lexer.fut:96-196).
+ * The host input is lexed in windows of `window` bytes (0: 1 GiB). A window
+ * that ends inside the input leaves its last token open: the next window
+ * starts at that token's first byte, where lex_string's state is the initial
+ * one again, so the lexemes are exactly lex_string's (backends/c/lexer.c:
+ * 39-97). A window in which no token ends is doubled and lexed again (up to
+ * 2^31 - 1 bytes, else ALPACC_E_CAPACITY). After each window `sink` receives
+ * its lexemes (host arrays of `count` terminal_t ids, index_t absolute
+ * starts and length_t lengths, valid during the call; `first` = index of the
+ * first one); a nonzero return stops with ALPACC_E_ABORTED. Returns
+ * ALPACC_OK with *num_tokens set, ALPACC_REJECT (lexemes already passed to
+ * the sink are then void), or an error. Tables with 32-bit index_t take at
+ * most 2^31 - 1 bytes.
+ */
+typedef int (*alpacc_lex_sink)(void *user, uint64_t first, uint64_t count, const void *token_ids,
+                               const void *token_starts, const void *token_lengths);
+int alpacc_gpu_lex_stream(alpacc_gpu_grammar *g, const uint8_t *in, uint64_t n, uint64_t window,
+                          alpacc_lex_sink sink, void *user, uint64_t *num_tokens);
 
 /*
  * Parser-only mode: `tokens` holds n terminal_t ids (host memory); the result
