@@ -95,3 +95,17 @@ def test_lexer_mode_numbers_terminals_in_order():
     assert both.terminal_names[:2] == ["string", "number"]
     assert lex.terminal_names[:2] == ["number", "string"]
     assert lex.ignore_token == lex.dead_token - 1
+
+
+def test_reference_cuda_backend_builds():
+    """The reference's CUDA backend (the baseline kernels) assembles with the
+    restated constants and compiles for sm_100a; its --layout, printed before
+    any device call, agrees with the C program's type sizes."""
+    import shutil
+    import subprocess
+    if not os.path.isdir("/root/reference") or shutil.which("nvcc") is None:
+        pytest.skip("reference sources or nvcc not present")
+    from oracle.build_ref_cuda import build
+    exe = build("json_i32", "/root/reference")
+    out = subprocess.run([exe, "--layout"], capture_output=True, text=True, timeout=60).stdout
+    assert out.startswith("terminal_t=1\nproduction_t=1\nindex_t=4\n"), out
