@@ -15,6 +15,19 @@
 #define WIRE_UNIT ((uint64_t)1)
 #endif
 
+/* print_layout of the program's mode (C/Generator.hs:80-84, 103-107,
+   153-158): the same lines alpacc_gpu_layout gives for these tables. */
+static void print_layout(FILE *f) {
+  fprintf(f, "terminal_t=%zu\n", sizeof(terminal_t));
+#ifdef Q
+  fprintf(f, "production_t=%zu\n", sizeof(production_t));
+#endif
+  fprintf(f, "index_t=%zu\n", sizeof(index_t));
+#ifdef NUM_TRANS
+  fprintf(f, "length_t=%zu\n", sizeof(length_t));
+#endif
+}
+
 static alpacc_gpu_grammar *gpu_grammar(void) {
   static alpacc_gpu_grammar *g = NULL;
   if (!g) {

@@ -97,9 +97,7 @@ int main(int argc, char **argv) {
     } else if (!strcmp(argv[i], "--server")) {
       server = 1;
     } else if (!strcmp(argv[i], "--layout")) {
-      char buf[256];
-      alpacc_gpu_layout(gpu_grammar(), buf, sizeof buf);
-      fputs(buf, stdout);
+      print_layout(stdout);  /* from the types in scope: no device needed */
       return 0;
     } else if (!strcmp(argv[i], "-i") && i + 1 < argc) {
       ifile = argv[++i];

@@ -44,8 +44,41 @@ def build_program(tables, name: str, force: bool = False) -> str:
         f.write(source(tables))
     subprocess.check_call(["gcc", "-std=c99", "-O2", "-D_POSIX_C_SOURCE=200809L", "-I", CSRC, "-I",
                            os.path.join(REPO, "include"), src, "-o", out, "-L", LIBDIR, "-lalpacc_b200",
-                           "-Wl,-rpath,$ORIGIN"])
+                           "-Wl,-rpath,$ORIGIN:" + LIBDIR])
     with open(stamp, "w") as f:
         f.write(key)
     os.remove(src)
     return out
+
+
+def main(argv=None) -> int:
+    """``python -m alpacc_b200.wire_program grammar.alp [--lexer|--parser]
+    [--index32] [-o program]``: the counterpart of ``alpacc c grammar.alp``
+    followed by ``cc`` (tests/testc.sh:89-95 of the reference), building the
+    wire-protocol program of that mode on the B200 path."""
+    import argparse
+    import shutil
+
+    from .grammar.cache import load_tables
+
+    ap = argparse.ArgumentParser(prog="python -m alpacc_b200.wire_program")
+    ap.add_argument("grammar")
+    mode = ap.add_mutually_exclusive_group()
+    mode.add_argument("--lexer", action="store_true", help="lexer-only program")
+    mode.add_argument("--parser", action="store_true", help="parser-only program")
+    ap.add_argument("--index32", action="store_true", help="32-bit index_t")
+    ap.add_argument("-o", "--output", help="path of the program (default: the grammar's name)")
+    a = ap.parse_args(argv)
+    parts = "lexer" if a.lexer else "parser" if a.parser else "both"
+    t = load_tables(a.grammar, index32=a.index32, parts=parts)
+    name = "%s_%s%s" % (t.name, "i32" if a.index32 else "i64", "" if parts == "both" else "_" + parts)
+    exe = build_program(t, name)
+    out = a.output or os.path.splitext(os.path.basename(a.grammar))[0]
+    shutil.copy2(exe, out)
+    print(out)
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+    sys.exit(main())

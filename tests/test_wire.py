@@ -66,3 +66,21 @@ def test_mode_layout_text_and_frames():
     assert par.text() == "terminal_t=1\nproduction_t=1\nindex_t=4\n"
     frame = wire.encode_mode_frame(b"\x01\x02\x03", par)
     assert frame[:16] == (11).to_bytes(8, "little") + (3).to_bytes(8, "little")
+
+
+def test_wire_program_layout_matches_reference_without_gpu():
+    """The wire-protocol programs of all three modes print the reference
+    programs' --layout (from the types in scope; no device is touched)."""
+    import subprocess
+
+    from alpacc_b200.wire_program import build_program
+    from oracle.ref import REF_DIR
+    for config in ("arithmetic_i64", "json_i32", "sexp_i64"):
+        for parts in ("both", "lexer", "parser"):
+            name = cases.mode_name(config, parts)
+            exe = build_program(cases.tables(config, parts), name)
+            got = subprocess.run([exe, "--layout"], capture_output=True, check=True).stdout
+            assert got.decode() == wire.Layout.of(cases.tables(config, parts)).text()
+            ref = os.path.join(REF_DIR, name)
+            if os.path.exists(ref):
+                assert got == subprocess.run([ref, "--layout"], capture_output=True, check=True).stdout
