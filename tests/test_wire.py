@@ -84,3 +84,50 @@ def test_wire_program_layout_matches_reference_without_gpu():
             ref = os.path.join(REF_DIR, name)
             if os.path.exists(ref):
                 assert got == subprocess.run([ref, "--layout"], capture_output=True, check=True).stdout
+
+
+def test_reference_cli_with_b200_run_case_builds(tmp_path):
+    """The binding INTEGRATION.md describes for the Haskell generator: the
+    emitted constants and runtime templates, the glue of csrc/wire_glue.h, a
+    run_case calling alpacc_gpu_run_case and the reference's own cli.c
+    compile together in all three modes, and --layout (no device) prints the
+    reference program's lines. Needs the reference sources."""
+    import subprocess
+
+    import pytest
+
+    from alpacc_b200.build import LIBDIR, REPO
+    from alpacc_b200.grammar import emit_c
+    from oracle.ref import REF_DIR
+
+    ref = "/root/reference"
+    if not os.path.isdir(ref):
+        pytest.skip("reference sources not present")
+
+    def rd(p):
+        return open(os.path.join(ref, p)).read()
+
+    glue = open(os.path.join(REPO, "alpacc_b200", "csrc", "wire_glue.h")).read()
+    for parts in ("both", "lexer", "parser"):
+        t = cases.tables("json_i32", parts)
+        ib = "#define INPUT_BYTES(n) ((n) * sizeof(terminal_t))" if parts == "parser" else "#define INPUT_BYTES(n) (n)"
+        run_case = "\n".join([ib, "static void run_case(uint64_t n, const uint8_t *in, FILE *out) {",
+                              "  int rc = alpacc_gpu_run_case(gpu_grammar(), n, in, out);",
+                              '  if (rc < 0) { fprintf(stderr, "%s\\n", alpacc_strerror(rc)); exit(1); }', "}"])
+        secs = [emit_c.program_prefix(t)]
+        if parts != "parser":
+            secs += [emit_c.lexer_constants(t), rd("backends/c/lexer.c")]
+        if parts != "lexer":
+            secs += [emit_c.parser_constants(t, with_tree=parts == "both"), rd("backends/c/parser.c")]
+        secs += [glue, run_case, rd("backends/c/cli.c")]
+        src = tmp_path / ("b200_%s.c" % parts)
+        src.write_text("\n".join(secs))
+        exe = str(tmp_path / ("b200_%s" % parts))
+        subprocess.check_call(["gcc", "-std=c99", "-O1", "-I", os.path.join(REPO, "include"), "-o", exe, str(src),
+                               "-L", LIBDIR, "-lalpacc_b200", "-Wl,-rpath," + LIBDIR])
+        got = subprocess.run([exe, "--layout"], capture_output=True, check=True).stdout
+        want = os.path.join(REF_DIR, cases.mode_name("json_i32", parts))
+        if os.path.exists(want):
+            assert got == subprocess.run([want, "--layout"], capture_output=True, check=True).stdout
+        else:
+            assert got.decode() == wire.Layout.of(t).text()
