@@ -109,7 +109,8 @@ static int build_lexer(const alpacc_tables *t, int ignore, LexerMachine *lm, std
     if ((int)sig.size() == before) break;
   }
   const int M = *std::max_element(cls.begin(), cls.end()) + 1;
-  if (M > kMaxMachine) { *why = "minimised lexer automaton exceeds 255 states"; return ALPACC_E_UNSUPPORTED; }
+  // the device transition entries hold a 7-bit state and the produce bit
+  if (M > 128) { *why = "minimised lexer automaton exceeds 128 states"; return ALPACC_E_UNSUPPORTED; }
   std::vector<std::vector<int>> T(M, std::vector<int>(C0));
   std::vector<uint8_t> sterm(M), sflags(M);
   for (int i = 0; i < R; i++) {
