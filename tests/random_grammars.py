@@ -232,3 +232,59 @@ def fuzz_grammars(count: int, first_seed: int = 0):
             continue
         found += 1
         yield name, g, t
+
+
+# C's keywords: a lexer whose machine grows with every keyword that shares
+# prefixes with the identifier rule
+KEYWORDS = ("if", "else", "while", "for", "return", "break", "continue", "int", "float", "char", "void", "struct",
+            "switch", "case", "default", "do", "goto", "sizeof", "static", "const", "unsigned", "signed", "long",
+            "short", "double", "enum", "union", "typedef", "extern", "register", "volatile", "auto")
+
+
+def keyword_grammar(nkw: int) -> str:
+    """A lexer of ``nkw`` keywords, identifiers, numbers and whitespace under
+    an LLP(1, 1) list grammar. The keywords come first, so they win over the
+    identifier rule on equal length (the reference's priority by order)."""
+    lines = ["params { lookback=1. lookahead=1. }", ""]
+    lines += ["kw%d = /%s/." % (i, w) for i, w in enumerate(KEYWORDS[:nkw])]
+    lines += ["ident = /[a-z][a-z0-9]*/.", "num = /[0-9]+/.", "ignore = /\\s|\\n|\\t/.", ""]
+    lines += ["S -> T S.", "S -> ."]
+    lines += ["T -> kw%d." % i for i in range(nkw)] + ["T -> ident.", "T -> num."]
+    return "\n".join(lines) + "\n"
+
+
+def keyword_inputs(nkw: int, seed: int = 0, sizes=(0, 1, 20, 300, 15000, 40000)) -> list:
+    """Sequences of keywords, near-keywords (prefixes and extensions, which
+    are identifiers), identifiers and numbers with whitespace runs; each size
+    once clean and once with a byte no rule accepts."""
+    rng = np.random.default_rng(seed)
+    kws = KEYWORDS[:nkw]
+
+    def word():
+        x = rng.random()
+        w = kws[int(rng.integers(0, len(kws)))]
+        if x < 0.4:
+            return w
+        if x < 0.55:
+            return w[: max(1, len(w) - 1)]
+        if x < 0.7:
+            return w + "xyz0"[int(rng.integers(0, 4))]
+        if x < 0.85:
+            return "".join("abcdefghijklmnopqrstuvwxyz"[int(i)] for i in rng.integers(0, 26, int(rng.integers(1, 9))))
+        return str(int(rng.integers(0, 10 ** 6)))
+
+    out = []
+    for n in sizes:
+        parts, size = [], 0
+        while size < n:
+            w = word()
+            sep = " \n\t"[int(rng.integers(0, 3))] * int(rng.integers(1, 3))
+            parts.append(w + sep)
+            size += len(w) + len(sep)
+        s = "".join(parts)[:n]
+        out.append(s.encode())
+        if n > 1:
+            b = bytearray(s.encode())
+            b[int(rng.integers(0, len(b)))] = ord("#")
+            out.append(bytes(b))
+    return out

@@ -53,3 +53,18 @@ def test_random_grammars_all_modes(grammars):
 def test_random_grammars_cover_qk():
     qks = {(g.q, g.k) for _, g, _ in fuzz_grammars(COUNT)}
     assert len(qks) >= 3, qks
+
+
+@pytest.mark.parametrize("nkw", [8, 24])
+def test_keyword_lexers_all_modes(nkw):
+    """C-like keyword lexers (machines of 50 and 124 states), all three modes."""
+    if not os.path.isdir(REFERENCE):
+        pytest.skip("reference sources not present")
+    from tests.random_grammars import keyword_grammar, keyword_inputs
+    text = keyword_grammar(nkw)
+    ins = keyword_inputs(nkw)
+    name = "kw%d" % nkw
+    t = generate_parts(text, name, False, "both")
+    assert 0 < _check(t, name, ins) < len(ins)
+    _check(generate_parts(text, name, False, "lexer"), name + "_lexer", ins)
+    _check(generate_parts(text, name, False, "parser"), name + "_parser", cases.token_inputs_for(t, ins))

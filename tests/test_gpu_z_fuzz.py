@@ -59,3 +59,24 @@ def test_random_grammars_batch_equals_single(gpu, grammars):
                 assert r.equal(p.parse(d)), (name, d[:50])
         finally:
             p.close()
+
+
+@pytest.mark.parametrize("nkw", [8, 16, 24])
+def test_keyword_lexers(gpu, nkw):
+    """C-like keyword lexers: 50 machine states (state-set walk), 86 and 124
+    states (above 64: per-start lanes from the first byte), in all three
+    modes against the oracle, on inputs up to several lexer tiles."""
+    from alpacc_b200.native import Parser
+    from tests.random_grammars import keyword_grammar, keyword_inputs
+    text = keyword_grammar(nkw)
+    name = "kw%d" % nkw
+    t = generate_parts(text, name, False, "both")
+    ins = keyword_inputs(nkw, seed=nkw)
+    p = Parser(t)
+    try:
+        assert (p.info()["M"] > 64) == (nkw >= 16)
+    finally:
+        p.close()
+    assert _check(t, ins) > 0
+    assert _check(generate_parts(text, name, False, "lexer"), ins) > 0
+    assert _check(generate_parts(text, name, False, "parser"), cases.token_inputs_for(t, ins)) > 0
