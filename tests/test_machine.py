@@ -1,0 +1,78 @@
+"""The lexer machine the loader derives for the GPU, run on the CPU.
+
+``device_tables.cpp`` turns TO_STATE / COMPOSE / ACCEPT into a minimised Moore
+machine over byte classes, which the lexer kernels walk. ``tests/native/
+machine_lex.cpp`` walks that machine sequentially with the kernels' boundary
+rule; its lexemes must equal the oracle's ``lex_string`` lexemes (lexer-mode
+records) for the shipped grammars, random grammars and keyword lexers — a
+check of the host-side derivation that needs no GPU.
+"""
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from alpacc_b200 import native, wire
+from alpacc_b200.grammar.tables import generate_parts
+from oracle.port import PortOracle
+from tests import cases
+from tests.random_grammars import fuzz_grammars, keyword_grammar, keyword_inputs
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+
+
+@pytest.fixture(scope="module")
+def harness(tmp_path_factory):
+    so = str(tmp_path_factory.mktemp("machine") / "libmachine_lex.so")
+    subprocess.check_call(["g++", "-O1", "-std=c++17", "-shared", "-fPIC",
+                           "-I", os.path.join(REPO, "alpacc_b200", "csrc"), "-I", os.path.join(REPO, "include"),
+                           os.path.join(HERE, "native", "machine_lex.cpp"),
+                           os.path.join(REPO, "alpacc_b200", "csrc", "device_tables.cpp"), "-o", so])
+    L = ctypes.CDLL(so)
+    L.machine_lex.restype = ctypes.c_int
+    L.machine_lex.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64,
+                              ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int)]
+    return L
+
+
+def _compare(L, t, inputs):
+    s, keep = native.make_tables(t)
+    po = PortOracle(t)
+    lay = wire.Layout.of(t)
+    states = ctypes.c_int(0)
+    for d in inputs:
+        cap = len(d) + 1
+        out = np.zeros(3 * cap, dtype=np.uint64)
+        cnt = ctypes.c_uint64(0)
+        rc = L.machine_lex(ctypes.byref(s), d, len(d), out.ctypes.data, cap, ctypes.byref(cnt), ctypes.byref(states))
+        assert rc in (native.OK, native.REJECT), rc
+        want, _ = wire.decode_lex_record(po.run_case(d), lay)
+        assert (rc == native.OK) == want.valid, (t.name, d[:40])
+        if want.valid:
+            got = out[: 3 * cnt.value].reshape(-1, 3).astype(np.int64)
+            assert len(got) == len(want.token_ids), (t.name, d[:40])
+            assert np.array_equal(got[:, 0], want.token_ids), (t.name, d[:40])
+            assert np.array_equal(got[:, 1], want.token_starts), (t.name, d[:40])
+            assert np.array_equal(got[:, 2], want.token_lengths), (t.name, d[:40])
+    return states.value
+
+
+@pytest.mark.parametrize("config", cases.MODE_CONFIGS)
+def test_machine_matches_lex_string(harness, config):
+    _compare(harness, cases.tables(config, "lexer"), cases.case_inputs(config, sizes=(1, 64, 3000), seeds=(0,)))
+
+
+def test_machine_random_grammars(harness):
+    for name, g, _ in fuzz_grammars(16):
+        _compare(harness, generate_parts(g.text(), name, False, "lexer"), g.inputs(0, sentences=(8, 300), noise=(500,)))
+
+
+@pytest.mark.parametrize("nkw", [8, 24])
+def test_machine_keyword_lexers(harness, nkw):
+    t = generate_parts(keyword_grammar(nkw), "kw%d" % nkw, False, "lexer")
+    states = _compare(harness, t, keyword_inputs(nkw, sizes=(0, 1, 20, 300, 5000)))
+    assert states == {8: 50, 24: 124}[nkw]
