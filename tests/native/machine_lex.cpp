@@ -53,3 +53,36 @@ extern "C" int machine_lex(const alpacc_tables *t, const uint8_t *in, uint64_t n
   *count = k;
   return ALPACC_OK;
 }
+
+// The pair record the dense table of device_tables.cpp gives for each of
+// `count` keys (q + k terminal ids each): found flag and the stack and
+// production spans, as the pair kernel reads them.
+extern "C" int pair_lookup(const alpacc_tables *t, const uint64_t *keys, uint64_t count, int64_t *out) {
+  alpacc::HostGrammar hg;
+  std::string why;
+  const int rc = alpacc::build_host_grammar(t, &hg, &why);
+  if (rc != ALPACC_OK) return rc;
+  const alpacc::PairTable &pt = hg.pairs;
+  const int L = pt.q + pt.k;
+  for (uint64_t i = 0; i < count; i++) {
+    uint64_t d = 0;
+    bool bad = false;
+    for (int j = 0; j < L; j++) {
+      const uint64_t v = keys[i * L + j];
+      if (v >= (uint64_t)pt.nt) bad = true;
+      d = d * (uint64_t)pt.nt + (bad ? 0 : v);
+    }
+    const uint32_t r = bad ? 0xffffffffu : pt.dense[d];
+    int64_t *o = out + 5 * i;
+    if (r == 0xffffffffu) {
+      o[0] = 0;
+      continue;
+    }
+    o[0] = 1;
+    o[1] = pt.rec_ss[r];
+    o[2] = (int64_t)pt.rec_ss[r] + pt.rec_nb[r];
+    o[3] = pt.rec_ps[r];
+    o[4] = (int64_t)pt.rec_ps[r] + pt.rec_np[r];
+  }
+  return ALPACC_OK;
+}

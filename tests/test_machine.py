@@ -76,3 +76,62 @@ def test_machine_keyword_lexers(harness, nkw):
     t = generate_parts(keyword_grammar(nkw), "kw%d" % nkw, False, "lexer")
     states = _compare(harness, t, keyword_inputs(nkw, sizes=(0, 1, 20, 300, 5000)))
     assert states == {8: 50, 24: 124}[nkw]
+
+
+def _lookup_key(t, key):
+    """``lookup_key`` (backends/c/parser.c:17-45): FNV-1a, linear probing up
+    to MAX_ITERS, and a found key with a negative span counts as missing."""
+    from alpacc_b200.grammar.tables import fnv1a
+    H = t.hash_size
+    h = fnv1a(key) % H
+    for _ in range(t.max_iters):
+        if t.ht_valid[h] and all(int(a) == int(b) for a, b in zip(t.ht_keys[h], key)):
+            ss, se = (int(x) for x in t.ht_stack_span[h])
+            ps, pe = (int(x) for x in t.ht_prod_span[h])
+            if min(ss, se, ps, pe) < 0:
+                return None
+            return (ss, se, ps, pe)
+        h = (h + 1) % H
+    return None
+
+
+def _check_pairs(L, t, seed=0):
+    import itertools
+    s, keep = native.make_tables(t)
+    n = t.q + t.k
+    nt = t.end_terminal + 1
+    space = nt ** n
+    if space <= 50000:
+        keys = np.array(list(itertools.product(range(nt), repeat=n)), dtype=np.uint64).reshape(-1, n)
+    else:
+        rng = np.random.default_rng(seed)
+        stored = np.array([k for k, v in zip(t.ht_keys, t.ht_valid) if v], dtype=np.uint64).reshape(-1, n)
+        keys = np.concatenate([stored, rng.integers(0, nt, (20000, n)).astype(np.uint64)])
+    # ids past the terminal range are never a key
+    keys = np.concatenate([keys, np.full((1, n), nt, dtype=np.uint64)])
+    out = np.zeros((len(keys), 5), dtype=np.int64)
+    assert L.pair_lookup(ctypes.byref(s), keys.ctypes.data, len(keys), out.ctypes.data) == native.OK
+    found = 0
+    for key, o in zip(keys, out):
+        want = _lookup_key(t, key)
+        assert (o[0] == 1) == (want is not None), (t.name, key)
+        if want is not None:
+            assert tuple(int(x) for x in o[1:]) == want, (t.name, key)
+            found += 1
+    return found
+
+
+@pytest.mark.parametrize("config", sorted(cases.CONFIGS))
+def test_pair_table_matches_lookup_key(harness, config):
+    L = harness
+    L.pair_lookup.restype = ctypes.c_int
+    L.pair_lookup.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
+    assert _check_pairs(L, cases.tables(config)) > 0
+
+
+def test_pair_table_random_grammars(harness):
+    L = harness
+    L.pair_lookup.restype = ctypes.c_int
+    L.pair_lookup.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
+    for name, g, t in fuzz_grammars(16):
+        assert _check_pairs(L, t) > 0, name
