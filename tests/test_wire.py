@@ -131,3 +131,23 @@ def test_reference_cli_with_b200_run_case_builds(tmp_path):
             assert got == subprocess.run([want, "--layout"], capture_output=True, check=True).stdout
         else:
             assert got.decode() == wire.Layout.of(t).text()
+
+
+def test_wire_program_frame_errors_without_gpu():
+    """Malformed requests end the program with status 1 before any device
+    work, as the reference's cli.c does: a truncated count, a truncated frame,
+    and a frame whose length disagrees with n (for the parser-mode program
+    with n counted in terminal ids)."""
+    import struct
+    import subprocess
+
+    from alpacc_b200.wire_program import build_program
+    for parts in ("both", "lexer", "parser"):
+        t = cases.tables("sexp_i64", parts)
+        exe = build_program(t, cases.mode_name("sexp_i64", parts))
+        cases_bad = [b"\x01\x00", struct.pack("<Q", 1) + struct.pack("<QQ", 20, 12) + b"(a)",
+                     struct.pack("<Q", 1) + struct.pack("<QQ", 8 + 4, 3) + b"\x00\x01\x02\x03"]
+        for data in cases_bad:
+            r = subprocess.run([exe], input=data, capture_output=True, timeout=60)
+            assert r.returncode == 1, (parts, data, r.stderr)
+        assert subprocess.run([exe, "--help"], capture_output=True, timeout=60).returncode == 0
