@@ -2,8 +2,9 @@
 
 * ``alpacc_b200/_lib/libalpacc_b200.so`` - the CUDA path and C ABI, compiled
   for sm_100a only (``-gencode arch=compute_100a,code=sm_100a``);
-* ``alpacc_b200/grammar/_closure.so``  - the generator's endomorphism closure;
-* ``alpacc_b200/_lib/alpacc_cli``      - the wire-protocol program.
+* ``alpacc_b200/grammar/_closure.so``  - the generator's endomorphism closure.
+
+The wire-protocol programs are built per grammar by ``wire_program.py``.
 
 Run ``python -m alpacc_b200.build``; rebuilds only when sources are newer.
 """
@@ -20,7 +21,6 @@ REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libalpacc_b200.so")
-CLI = os.path.join(LIBDIR, "alpacc_cli")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -43,7 +43,7 @@ def headers():
 
 def build_lib(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
-    srcs = [s for s in sources() if not s.endswith("cli.cpp")]
+    srcs = sources()
     if not force and not _newer(LIB, srcs + headers()):
         return LIB
     objs = []
@@ -61,23 +61,11 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
-def build_cli(force: bool = False) -> str:
-    src = os.path.join(CSRC, "cli.cpp")
-    if not os.path.exists(src):
-        return ""
-    if not force and not _newer(CLI, [src, LIB]):
-        return CLI
-    subprocess.check_call(["g++", "-O2", "-std=c++17", src, "-o", CLI, "-I", os.path.join(REPO, "include"),
-                           "-L", LIBDIR, "-lalpacc_b200", "-Wl,-rpath,$ORIGIN"])
-    return CLI
-
-
 def build_all(force: bool = False, verbose: bool = False) -> None:
     from .grammar import lexgen
 
     lexgen._closure_lib()
     build_lib(force=force, verbose=verbose)
-    build_cli(force=force)
 
 
 if __name__ == "__main__":

@@ -462,7 +462,7 @@ alpacc_gpu_grammar *alpacc_gpu_load(const alpacc_tables *tables, int device, uin
           if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return true;
         return false;
       }() ||
-      cudaMalloc(&g->d_status, sizeof(DeviceStatus)) != cudaSuccess ||
+      alpacc::dev_malloc(reinterpret_cast<void **>(&g->d_status), sizeof(DeviceStatus)) != cudaSuccess ||
       cudaMallocHost(&g->h_status, sizeof(DeviceStatus)) != cudaSuccess) {
     cudaGetLastError();
     *err = ALPACC_E_CUDA;
@@ -868,6 +868,8 @@ int alpacc_gpu_info(const alpacc_gpu_grammar *g, int64_t *vals, int nvals) {
 }
 
 const char *alpacc_gpu_last_error(const alpacc_gpu_grammar *g) { return g ? g->last_error.c_str() : ""; }
+
+uint64_t alpacc_device_allocations(void) { return alpacc::g_device_allocs.load(std::memory_order_relaxed); }
 
 int alpacc_gpu_counts(const alpacc_gpu_grammar *g, int64_t *vals, int n) {
   if (!g || !vals || !g->h_status) return ALPACC_E_INVALID;

@@ -12,7 +12,18 @@
 #include "common.cuh"
 #include "device_tables.h"
 
+#include <atomic>
+
 namespace alpacc {
+
+// Device allocations this library has made in the process (every cudaMalloc
+// goes through dev_malloc); read by alpacc_device_allocations.
+inline std::atomic<unsigned long long> g_device_allocs{0};
+
+inline cudaError_t dev_malloc(void **p, size_t bytes) {
+  g_device_allocs.fetch_add(1, std::memory_order_relaxed);
+  return cudaMalloc(p, bytes);
+}
 
 struct DevBuf {
   void *p = nullptr;
@@ -26,7 +37,7 @@ inline int grow(DevBuf &b, size_t bytes) {
   b.p = nullptr;
   b.cap = 0;
   size_t want = std::max<size_t>(bytes, 256);
-  if (cudaMalloc(&b.p, want) != cudaSuccess) {
+  if (dev_malloc(&b.p, want) != cudaSuccess) {
     cudaGetLastError();
     return ALPACC_E_NOMEM;
   }

@@ -21,7 +21,9 @@
 //    handles on one device) race on it;
 //  * the array's device address is looked up once per device, with that
 //    device current, on the first call there (cudaGetSymbolAddress); make
-//    that first call before any stream capture.
+//    that first call before any stream capture;
+//  * every call reads the status words back and waits for the handle's
+//    stream before returning, and restores the caller's current device.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -75,6 +77,13 @@ int scratch_address(int device, unsigned char **out) {
 
 }  // namespace
 
+namespace {
+
+int lex_noalloc_on_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, void *d_token_ids,
+                          void *d_token_starts, void *d_token_lengths, uint64_t *num_tokens);
+
+}  // namespace
+
 extern "C" int alpacc_gpu_lex_noalloc(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, void *d_token_ids,
                                       void *d_token_starts, void *d_token_lengths, uint64_t *num_tokens) {
   if (!g || !num_tokens || (n > 0 && (!d_in || !d_token_ids || !d_token_starts || !d_token_lengths)))
@@ -83,7 +92,29 @@ extern "C" int alpacc_gpu_lex_noalloc(alpacc_gpu_grammar *g, const uint8_t *d_in
   if (n > kNoAllocMaxInput) return ALPACC_E_CAPACITY;  // inputs above 16 MiB need the allocating path
   *num_tokens = 0;
   if (n == 0) return ALPACC_OK;  // lex_string accepts the empty input with no tokens
-  if (cudaSetDevice(g->device) != cudaSuccess) return ALPACC_E_CUDA;
+  // the caller's current device is put back on every return path
+  int caller_device = -1;
+  if (cudaGetDevice(&caller_device) != cudaSuccess) {
+    cudaGetLastError();
+    return ALPACC_E_CUDA;
+  }
+  if (caller_device != g->device && cudaSetDevice(g->device) != cudaSuccess) {
+    cudaGetLastError();
+    return ALPACC_E_CUDA;
+  }
+  const int rc = lex_noalloc_on_device(g, d_in, n, d_token_ids, d_token_starts, d_token_lengths, num_tokens);
+  if (caller_device != g->device && cudaSetDevice(caller_device) != cudaSuccess) {
+    cudaGetLastError();
+    return rc < 0 ? rc : ALPACC_E_CUDA;
+  }
+  return rc;
+}
+
+namespace {
+
+// The call itself, with the handle's device current.
+int lex_noalloc_on_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, void *d_token_ids,
+                          void *d_token_starts, void *d_token_lengths, uint64_t *num_tokens) {
   unsigned char *base = nullptr;
   int rc = scratch_address(g->device, &base);
   if (rc != ALPACC_OK) return rc;
@@ -146,3 +177,5 @@ extern "C" int alpacc_gpu_lex_noalloc(alpacc_gpu_grammar *g, const uint8_t *d_in
   *num_tokens = h.num_tokens;
   return ALPACC_OK;
 }
+
+}  // namespace

@@ -32,6 +32,7 @@ struct Request {
   Clock::time_point submitted, done_at;
   int status = 0;
   bool done = false;
+  bool claimed = false;  // a caller is waiting for it (only one may)
   alpacc_result res{};
 };
 
@@ -175,10 +176,11 @@ int alpacc_server_wait(alpacc_server *s, uint64_t id, alpacc_result *out, double
   {
     std::unique_lock<std::mutex> lock(s->mu);
     auto it = s->reqs.find(id);
-    if (it == s->reqs.end()) return ALPACC_E_INVALID;
+    if (it == s->reqs.end() || it->second->claimed) return ALPACC_E_INVALID;  // unknown, or another caller waits
     r = it->second;
+    r->claimed = true;
     s->cv_done.wait(lock, [&] { return r->done; });
-    s->reqs.erase(it);
+    s->reqs.erase(id);
   }
   *out = r->res;
   if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->done_at - r->submitted).count();

@@ -136,6 +136,8 @@ def lib():
         L.alpacc_gpu_stream.argtypes = [ctypes.c_void_p]
         L.alpacc_gpu_last_error.restype = ctypes.c_char_p
         L.alpacc_gpu_last_error.argtypes = [ctypes.c_void_p]
+        L.alpacc_device_allocations.restype = ctypes.c_uint64
+        L.alpacc_device_allocations.argtypes = []
         _lib = L
     return _lib
 
@@ -425,6 +427,39 @@ class Parser:
     @staticmethod
     def free_result(r: Result):
         lib().alpacc_result_free(ctypes.byref(r))
+
+    def record_digest_raw(self, host_ptr: int, n: int):
+        """(status, SHA-256 hex, byte count) of the combined-mode response
+        record for the host input at ``host_ptr``: the result arrays are
+        hashed in place, in record order (valid byte, T, ids, starts,
+        lengths, N, productions, parents, token parents), so a record of
+        several GB is never assembled."""
+        import hashlib
+        import struct
+
+        rc, r = self.parse_raw(host_ptr, n)
+        h = hashlib.sha256()
+        try:
+            if rc != OK:
+                h.update(b"\x00")
+                return rc, h.hexdigest(), 1
+            lay = self.layout
+            T, N = r.num_tokens, r.num_nodes
+            size = 0
+            for ptr, nbytes in ((None, b"\x01" + struct.pack("<Q", T)),
+                                (r.token_ids, T * lay.terminal), (r.token_starts, T * lay.index),
+                                (r.token_lengths, T * lay.length), (None, struct.pack("<Q", N)),
+                                (r.node_productions, N * lay.production), (r.node_parents, N * lay.index),
+                                (r.token_parents, T * lay.index)):
+                if ptr is None:
+                    h.update(nbytes)
+                    size += len(nbytes)
+                elif nbytes:
+                    h.update((ctypes.c_uint8 * nbytes).from_address(ptr))
+                    size += nbytes
+            return rc, h.hexdigest(), size
+        finally:
+            self.free_result(r)
 
     def last_ms(self) -> float:
         return lib().alpacc_gpu_last_ms(self._h)

@@ -198,27 +198,55 @@ def arithmetic(n: int, seed: int = 1) -> bytes:
     return body + b" " * (n - len(body))
 
 
+_ATOM_CHARS = np.frombuffer(b"abcdefghijklmnopqrstuvwxyz0123456789", dtype=np.uint8)
+_OPEN, _ATOM, _CLOSE = 0, 1, 2
+
+
 def _sexp_form(rng, depth: int, unbalanced: bool) -> bytes:
-    parts = []
+    """One spine of ``depth`` nested lists. Level i has ``kids`` ~ U[1, 6]
+    children: the list that continues the spine sits at position ``pos`` ~
+    U[0, kids), the others are atoms ``[a-z0-9]{1,10}``; the innermost list
+    holds one atom. Siblings are separated by single spaces.
 
-    def atom():
-        k = int(rng.integers(1, 11))
-        return "".join("abcdefghijklmnopqrstuvwxyz0123456789"[int(x)] for x in rng.integers(0, 36, k))
-
-    closers = []
-    for _ in range(depth):
-        kids = int(rng.integers(1, 7))
-        pos = int(rng.integers(0, kids))
-        pre = [atom() for _ in range(pos)]
-        post = [atom() for _ in range(kids - 1 - pos)]
-        parts.append("(" + " ".join(pre) + (" " if pre else ""))
-        closers.append((" " if post else "") + " ".join(post) + ")")
-    parts.append(atom())
-    parts.extend(reversed(closers))
-    s = "".join(parts)
+    Built with array operations: the token sequence (open, atom, close), the
+    spaces between siblings (after an atom or a close, before an atom or an
+    open), then every token's bytes scattered to its offset."""
+    kids = rng.integers(1, 7, depth)
+    pos = rng.integers(0, kids)
+    post = kids - 1 - pos
+    # opening half: per level "(" then pos atoms; then the core atom;
+    # closing half, innermost level first: post atoms then ")"
+    pre_len = 1 + pos
+    types_pre = np.full(int(pre_len.sum()), _ATOM, dtype=np.int8)
+    types_pre[np.concatenate(([0], np.cumsum(pre_len)[:-1]))] = _OPEN
+    post_r = post[::-1]
+    post_len = post_r + 1
+    types_post = np.full(int(post_len.sum()), _ATOM, dtype=np.int8)
+    types_post[np.cumsum(post_len) - 1] = _CLOSE
+    types = np.concatenate((types_pre, np.array([_ATOM], dtype=np.int8), types_post))
     if unbalanced:
-        s += ")"
-    return s.encode()
+        types = np.concatenate((types, np.array([_CLOSE], dtype=np.int8)))
+    is_atom = types == _ATOM
+    alen = rng.integers(1, 11, int(is_atom.sum()))
+    tlen = np.ones(len(types), dtype=np.int64)
+    tlen[is_atom] = alen
+    left = (types == _ATOM) | (types == _CLOSE)
+    right = (types == _ATOM) | (types == _OPEN)
+    space = np.zeros(len(types), dtype=bool)
+    space[:-1] = left[:-1] & right[1:]
+    if unbalanced:
+        space[-2] = False  # the extra ")" follows the form directly
+    width = tlen + space
+    off = np.concatenate(([0], np.cumsum(width)[:-1]))
+    out = np.full(int(width.sum()), ord(" "), dtype=np.uint8)
+    out[off[types == _OPEN]] = ord("(")
+    out[off[types == _CLOSE]] = ord(")")
+    # atom characters: each atom's bytes at its offset
+    a_off = off[is_atom]
+    total = int(alen.sum())
+    starts = np.repeat(a_off - np.concatenate(([0], np.cumsum(alen)[:-1])), alen)
+    out[starts + np.arange(total)] = _ATOM_CHARS[rng.integers(0, 36, total)]
+    return out.tobytes()
 
 
 def sexp_doc(n: int, seed: int = 3, unbalanced_frac: float = 0.0, max_depth: int = 10000,

@@ -544,7 +544,29 @@ def ours(a, rank, world, local_rank, dist):
     if not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(host, a.cpu_sample, wl["ref"], a.workload,
                                                    reps=2 if n > (512 << 20) else 4)
+    line["parity"] = record_parity(parser, pin, host, wl["ref"]) if not a.no_parity else None
     print(json.dumps(line))
+    if line["parity"] and line["parity"]["match"] is False:
+        raise SystemExit("parity failure: the GPU record of the timed document differs from oracle/_ref's")
+
+
+def record_parity(parser, pin, host: bytes, ref_config: str):
+    """Outside the timed region: the SHA-256 of the response record the GPU
+    path returns for the timed document (through alpacc_gpu_parse, host
+    buffers) against the record the reference's own C backend (oracle/_ref)
+    writes for the same bytes."""
+    import numpy as np
+
+    from oracle.ref import RefOracle, available
+
+    rc, got, got_size = parser.record_digest_raw(pin.data_ptr(), len(host))
+    if not available(ref_config):
+        return {"oracle": None, "match": None, "note": "oracle/_ref/lib%s.so is not built" % ref_config}
+    t0 = time.perf_counter()
+    want, want_size = RefOracle(ref_config).record_digest(np.frombuffer(host, dtype=np.uint8))
+    return {"oracle": "oracle/_ref/lib%s.so" % ref_config, "what": "sha256 of the run_case response record",
+            "record_bytes": got_size, "valid": rc == 0, "sha256": got[:16], "match": got == want and got_size == want_size,
+            "oracle_s": round(time.perf_counter() - t0, 2)}
 
 
 def committed_traffic(kernel: str):
@@ -570,6 +592,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=256 << 20)
     ap.add_argument("--ref-sample", type=int, default=16 << 20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the record comparison with oracle/_ref")
     a = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -171,8 +171,12 @@ int alpacc_gpu_parse_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t
  * shares that array, so calls must not overlap on the GPU (two streams, two
  * threads or two handles on one device race on it); the array's address is
  * looked up on the first call on each device, which should therefore come
- * before any stream capture. Returns ALPACC_OK with *num_tokens set,
- * ALPACC_REJECT, or an error.
+ * before any stream capture. Every call, the first and the later ones, ends
+ * by copying the status words back and waiting for the handle's stream
+ * (cudaStreamSynchronize) before it returns. The call makes the handle's
+ * device current while it runs and restores the caller's current device
+ * before returning. Returns ALPACC_OK with *num_tokens set, ALPACC_REJECT, or
+ * an error.
  */
 int alpacc_gpu_lex_noalloc(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, void *d_token_ids,
                            void *d_token_starts, void *d_token_lengths, uint64_t *num_tokens);
@@ -214,7 +218,9 @@ void alpacc_result_free(alpacc_result *r);
  *   submit: copies the input, returns its id;
  *   wait:   blocks until that request is done; its status (OK / REJECT /
  *           error), its result (release with alpacc_result_free before
- *           stopping the server) and the latency from submit to completion;
+ *           stopping the server) and the latency from submit to completion.
+ *           One caller may wait for an id; a second wait on the same id
+ *           (concurrent or later) returns ALPACC_E_INVALID;
  *   stats:  batches run, requests served, largest batch, requests queued;
  *   stop:   drains the queue, joins the workers, frees the handles.
  */
@@ -325,6 +331,10 @@ int alpacc_gpu_stage_ms(const alpacc_gpu_grammar *g, double *out, int n);
    the number of kernels the call launched. */
 int alpacc_gpu_counts(const alpacc_gpu_grammar *g, int64_t *vals, int n);
 void alpacc_gpu_set_diagnostics(alpacc_gpu_grammar *g, int on);
+/* Number of device allocations (cudaMalloc) this library has made in the
+   process so far, over all handles (diagnostics: lets a caller check that a
+   call allocated nothing). */
+uint64_t alpacc_device_allocations(void);
 
 #ifdef __cplusplus
 }

@@ -21,7 +21,12 @@ the same way from ``lexerTestCase`` / ``parserTestCase`` with only the lexer's
 constants) part, as ``<config>_lexer`` and ``<config>_parser``.
 Nothing from the reference is written outside ``oracle/_ref/`` (git-ignored).
 
-Usage: python oracle/build_ref.py [--reference /root/reference] [config ...]
+Usage: python oracle/build_ref.py [--reference DIR] [config ...]
+
+The reference sources are read from ``--reference``, else from the
+environment variable ALPACC_REFERENCE, else from /root/reference (where they
+are mounted read-only in the build container); ``reference_dir()`` gives the
+same answer to the tests, which skip when the sources are absent.
 """
 
 from __future__ import annotations
@@ -66,6 +71,16 @@ def haskell_text_block(hs_source: str, name: str) -> str:
 
 # configurations whose lexer-mode and parser-mode programs are also built
 MODE_CONFIGS = ("arithmetic_i64", "json_i32", "json_ext_i32", "sexp_i64", "paper_grammar_i64", "llp01_i64")
+# lexer-mode programs built beside those: json_ext with 64-bit starts checks
+# the chunked lexing of inputs beyond 2^31 bytes
+EXTRA_LEXER_CONFIGS = ("json_ext_i64",)
+
+
+def reference_dir():
+    """Directory of the reference's sources (ALPACC_REFERENCE, else the build
+    container's mount), or None when they are not present (the GPU box)."""
+    d = os.environ.get("ALPACC_REFERENCE", "/root/reference")
+    return d if d and os.path.isdir(d) else None
 
 
 def assemble(reference: str, tables) -> str:
@@ -138,10 +153,11 @@ def compile_program(tables, name: str, out: str, reference: str, cc: str = "gcc"
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=None)
     ap.add_argument("--force", action="store_true")
     ap.add_argument("configs", nargs="*")
     a = ap.parse_args(argv)
+    a.reference = a.reference or reference_dir() or ""
     if not os.path.isdir(a.reference):
         print("reference sources not present; oracle/_ref not rebuilt")
         return 0
@@ -150,6 +166,8 @@ def main(argv=None):
         if c in MODE_CONFIGS:
             for parts in ("lexer", "parser"):
                 print("building", c, parts, "->", build(c, a.reference, force=a.force, parts=parts))
+        elif c in EXTRA_LEXER_CONFIGS:
+            print("building", c, "lexer", "->", build(c, a.reference, force=a.force, parts="lexer"))
     return 0
 
 

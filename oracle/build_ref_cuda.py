@@ -18,7 +18,8 @@ which is how the "existing Blackwell-capable kernel" is timed beside this
 repository's kernels. Nothing from the reference is written outside
 ``oracle/_ref/`` (git-ignored).
 
-Usage: python oracle/build_ref_cuda.py [--reference /root/reference] [config ...]
+Usage: python oracle/build_ref_cuda.py [--reference DIR] [config ...]
+(the reference sources' location as in build_ref.py: ``reference_dir()``)
 """
 
 from __future__ import annotations
@@ -36,7 +37,7 @@ REPO = os.path.dirname(HERE)
 OUT = os.path.join(HERE, "_ref")
 sys.path.insert(0, REPO)
 
-from oracle.build_ref import CONFIGS  # noqa: E402
+from oracle.build_ref import CONFIGS, reference_dir  # noqa: E402
 
 # B200: opt-in shared memory per block and the SM architecture number, the
 # values the emitter bakes in after probing the device (Cuda/Generator.hs:70-92)
@@ -208,10 +209,11 @@ def build(config: str, reference: str, force: bool = False) -> str:
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=None)
     ap.add_argument("--force", action="store_true")
     ap.add_argument("configs", nargs="*", default=["json_i32"])
     a = ap.parse_args(argv)
+    a.reference = a.reference or reference_dir() or ""
     if not os.path.isdir(a.reference):
         print("reference sources not present; not built")
         return 0

@@ -12,6 +12,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 
 
+_SINK = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t)
+
+
 def available(config: str) -> bool:
     return os.path.exists(os.path.join(REF_DIR, "lib%s.so" % config))
 
@@ -34,6 +37,9 @@ class RefOracle:
                                               ctypes.POINTER(ctypes.c_uint64)]
             self.lib.ref_pipeline.restype = ctypes.c_int
         self.lib.ref_free.argtypes = [ctypes.c_void_p]
+        if hasattr(self.lib, "ref_run_case_sink"):
+            self.lib.ref_run_case_sink.argtypes = [ctypes.c_uint64, ctypes.c_void_p, _SINK, ctypes.c_void_p]
+            self.lib.ref_run_case_sink.restype = ctypes.c_int
         self.lib.ref_layout.argtypes = [ctypes.POINTER(ctypes.c_uint64)]
         self.lib.ref_input_unit.restype = ctypes.c_uint64
 
@@ -49,6 +55,38 @@ class RefOracle:
             return ctypes.string_at(out, n.value)
         finally:
             self.lib.ref_free(out)
+
+    def record_digest(self, buf, head: int = 0):
+        """(SHA-256 hex, byte count) of the response record ``run_case``
+        writes for ``buf`` (a numpy uint8 array or bytes), streamed through a
+        callback in 64 MiB pieces: records of several GB are never held.
+        With ``head`` > 0 the first ``head`` bytes are left out of the digest
+        and returned as a third item (e.g. a record's validity byte and
+        count, which a caller streaming its own record learns last)."""
+        import hashlib
+
+        import numpy as np
+        a = np.frombuffer(buf, dtype=np.uint8) if isinstance(buf, (bytes, bytearray)) else buf
+        h = hashlib.sha256()
+        size = [0]
+        first = bytearray()
+
+        def sink(_user, p, nbytes):
+            data = ctypes.string_at(p, nbytes)
+            if len(first) < head:
+                k = min(head - len(first), nbytes)
+                first.extend(data[:k])
+                data = data[k:]
+            h.update(data)
+            size[0] += nbytes
+
+        cb = _SINK(sink)
+        count = len(a) // self.lib.ref_input_unit()
+        if self.lib.ref_run_case_sink(count, a.ctypes.data, cb, None) != 0:
+            raise RuntimeError("fopencookie failed")
+        if head:
+            return h.hexdigest(), size[0], bytes(first)
+        return h.hexdigest(), size[0]
 
     def pipeline(self, buf, n=None):
         """lex -> parse -> parents -> compact without serialisation.

@@ -14,9 +14,15 @@
  *     without serialisation, the in-memory timing harness for the CPU baseline;
  *   - ref_layout: the type sizes print_layout reports;
  *   - ref_input_unit: the bytes per unit of run_case's n.
+ *   - ref_run_case_sink: the same record streamed to a callback in large
+ *     pieces (fopencookie), so records of several GB can be digested without
+ *     holding them in memory.
  * The same harness wraps the lexer-mode and parser-mode programs (no
  * ref_pipeline there).
  */
+#define _GNU_SOURCE 1 /* fopencookie */
+#include <stdio.h>
+#include <sys/types.h>
 #define main alpacc_generated_main
 #include ALPACC_GENERATED
 #undef main
@@ -34,6 +40,29 @@ int ref_run_case(uint64_t n, const uint8_t *in, uint8_t **out, size_t *out_len) 
 }
 
 void ref_free(void *p) { free(p); }
+
+typedef void (*ref_sink_fn)(void *user, const char *buf, size_t size);
+struct ref_sink_cookie {
+  ref_sink_fn fn;
+  void *user;
+};
+
+static ssize_t ref_sink_write(void *c, const char *buf, size_t size) {
+  struct ref_sink_cookie *k = (struct ref_sink_cookie *)c;
+  k->fn(k->user, buf, size);
+  return (ssize_t)size;
+}
+
+int ref_run_case_sink(uint64_t n, const uint8_t *in, ref_sink_fn fn, void *user) {
+  struct ref_sink_cookie k = {fn, user};
+  cookie_io_functions_t io = {NULL, ref_sink_write, NULL, NULL};
+  FILE *f = fopencookie(&k, "w", io);
+  if (!f) return -1;
+  setvbuf(f, NULL, _IOFBF, (size_t)64 << 20);
+  run_case(n, in, f);
+  fclose(f);
+  return 0;
+}
 
 /* Units of run_case's n: bytes, or terminal ids in the parser-mode program
    (INPUT_BYTES, C/Generator.hs:66, 88). */

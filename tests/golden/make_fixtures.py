@@ -234,8 +234,13 @@ def mode_records() -> dict:
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=None, help="the reference sources (default: build_ref.reference_dir())")
     a = ap.parse_args(argv)
+    if a.reference is None:
+        from oracle.build_ref import reference_dir
+        a.reference = reference_dir()
+        if a.reference is None:
+            raise SystemExit("the reference sources are not present (set ALPACC_REFERENCE)")
     ka = known_answers(a.reference)
     with open(os.path.join(HERE, "known_answers.json"), "w") as f:
         json.dump(ka, f, indent=1, sort_keys=True)

@@ -5,23 +5,22 @@ the combined, lexer-only and parser-only modes (the reference's
 tests/testc.sh does the same with its Haskell-generated expected outputs).
 Needs the reference sources to build those programs; skipped without them."""
 
-import os
-
 import pytest
 
 from alpacc_b200.grammar.tables import generate_parts
+from oracle.build_ref import reference_dir
 from oracle.port import PortOracle
 from oracle.ref import RefOracle
 from tests import cases
 from tests.random_grammars import fuzz_grammars
 
-REFERENCE = "/root/reference"
+REFERENCE = reference_dir()
 COUNT = 16
 
 
 @pytest.fixture(scope="module")
 def grammars():
-    if not os.path.isdir(REFERENCE):
+    if REFERENCE is None:
         pytest.skip("reference sources not present")
     return list(fuzz_grammars(COUNT))
 
@@ -58,7 +57,7 @@ def test_random_grammars_cover_qk():
 @pytest.mark.parametrize("nkw", [8, 24])
 def test_keyword_lexers_all_modes(nkw):
     """C-like keyword lexers (machines of 50 and 124 states), all three modes."""
-    if not os.path.isdir(REFERENCE):
+    if REFERENCE is None:
         pytest.skip("reference sources not present")
     from tests.random_grammars import keyword_grammar, keyword_inputs
     text = keyword_grammar(nkw)

@@ -4,10 +4,13 @@
   call (itself checked against the reference's lexer-mode program) for every
   window size, including windows shorter than a token (the window is widened)
   and inputs that are rejected.
-* An input beyond 2^31 bytes (json_ext, 64-bit index_t): two different
-  windowings give the same lexeme sequence (order-sensitive checksums), the
-  spans are ordered and inside the input, and the lexemes near the start and
-  near the end equal single calls on the input cut at a token boundary.
+* An input beyond 2^31 bytes (json_ext, 64-bit index_t): the whole lexeme
+  stream equals the lexer-mode record of the reference's own C program
+  (oracle/_ref, SHA-256 of the lexemes in record order, streamed on both
+  sides); two different windowings give the same lexeme sequence
+  (order-sensitive checksums); the spans are ordered and inside the input;
+  and the lexemes near the start and near the end equal single calls on the
+  input cut at a token boundary.
 """
 
 import numpy as np
@@ -70,8 +73,11 @@ def test_stream_combined_tables(gpu):
 class _Summary:
     """Order-sensitive checksum of a lexeme stream plus its first and last lexemes."""
 
-    def __init__(self, n, edge):
+    def __init__(self, n, edge, lay=None):
+        import hashlib
         self.n, self.edge = n, edge
+        self.lay = lay  # when set: SHA-256 of the lexemes as the lexer-mode record lays them out
+        self.sha = hashlib.sha256()
         self.count = 0
         self.h = np.uint64(0)
         self.prev_end = 0
@@ -89,6 +95,11 @@ class _Summary:
             v = v * np.uint64(0x9E3779B97F4A7C15)
             v = v ^ (v >> np.uint64(29))
             self.h = self.h + v.sum(dtype=np.uint64)
+        if self.lay is not None:
+            from alpacc_b200 import wire
+            rec = np.zeros(len(ids), dtype=wire._lexeme_dtype(self.lay))
+            rec["id"], rec["start"], rec["length"] = ids, starts, lens
+            self.sha.update(rec.tobytes())
         ends = starts + lens
         self.ordered &= bool(starts[0] >= self.prev_end) and bool(np.all(starts[1:] >= ends[:-1]))
         self.ordered &= bool(ends[-1] <= self.n)
@@ -112,11 +123,19 @@ def test_stream_beyond_2_gib(gpu):
     data = np.frombuffer(W.json_doc(n, 9), dtype=np.uint8)
     p = parser("json_ext_i64")
     edge = 8 << 20
-    a, b = _Summary(n, edge), _Summary(n, edge)
+    a, b = _Summary(n, edge, p.layout), _Summary(n, edge)
     p.lex_stream(data, window=1 << 30, on_window=a)
     p.lex_stream(data, window=(768 << 20) + 12345, on_window=b)
     assert a.count == b.count and a.count > 0
     assert a.h == b.h and a.ordered and b.ordered
+    # the whole stream against the reference's lexer-mode program
+    import struct
+
+    from oracle.ref import RefOracle, available
+    if available("json_ext_i64_lexer"):
+        want, _, head = RefOracle("json_ext_i64_lexer").record_digest(data, head=9)
+        assert head == b"\x01" + struct.pack("<Q", a.count)
+        assert a.sha.hexdigest() == want
     # the first lexemes: a single call on the input cut at a token start
     ids, starts, lens = a.cat("head")
     cut = int(starts[-1])

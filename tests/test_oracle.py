@@ -103,9 +103,10 @@ def test_reference_cuda_backend_builds():
     any device call, agrees with the C program's type sizes."""
     import shutil
     import subprocess
-    if not os.path.isdir("/root/reference") or shutil.which("nvcc") is None:
+    from oracle.build_ref import reference_dir
+    if reference_dir() is None or shutil.which("nvcc") is None:
         pytest.skip("reference sources or nvcc not present")
     from oracle.build_ref_cuda import build
-    exe = build("json_i32", "/root/reference")
+    exe = build("json_i32", reference_dir())
     out = subprocess.run([exe, "--layout"], capture_output=True, text=True, timeout=60).stdout
     assert out.startswith("terminal_t=1\nproduction_t=1\nindex_t=4\n"), out

@@ -87,7 +87,7 @@ def test_wire_program_layout_matches_reference_without_gpu():
 
 
 def test_reference_cli_with_b200_run_case_builds(tmp_path):
-    """The binding INTEGRATION.md describes for the Haskell generator: the
+    """The binding a maintainer adds to the Haskell generator's C output: the
     emitted constants and runtime templates, the glue of csrc/wire_glue.h, a
     run_case calling alpacc_gpu_run_case and the reference's own cli.c
     compile together in all three modes, and --layout (no device) prints the
@@ -100,8 +100,9 @@ def test_reference_cli_with_b200_run_case_builds(tmp_path):
     from alpacc_b200.grammar import emit_c
     from oracle.ref import REF_DIR
 
-    ref = "/root/reference"
-    if not os.path.isdir(ref):
+    from oracle.build_ref import reference_dir
+    ref = reference_dir()
+    if ref is None:
         pytest.skip("reference sources not present")
 
     def rd(p):

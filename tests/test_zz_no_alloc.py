@@ -2,12 +2,17 @@
 
 It serves callers that cannot call cudaMalloc where they lex (a framework
 that owns the device memory pool, a real-time loop). Its working memory is a
-fixed array inside the library, so this test calls it through the C ABI on
-inputs up to its 16 MiB limit and checks its tokens against the tokens the
-ordinary allocating entry point (alpacc_gpu_parse_device) produces for the
-same input, on two calls in a row (the shared array must be cleared between
-calls), and checks that oversize inputs are refused. It is collected last so a
-failure here cannot hide failures elsewhere.
+fixed array inside the library, so these tests call it through the C ABI and
+check its tokens against the tokens the ordinary allocating entry point
+(alpacc_gpu_parse_device) produces for the same input, on two calls in a row
+(the shared array must be cleared between calls); against the lexer-mode
+records of the reference's own C program (oracle/_ref) and of the C
+restatement oracle; at exactly its 16 MiB limit; on a 124-state keyword lexer
+(near the 128-state limit of its per-tile vectors); on a token longer than
+length_t holds (reject) and one at the limit (accept); and that its calls make
+no device allocation, even the first one on a fresh handle. Oversize inputs
+are refused. The file is collected last so a failure here cannot hide
+failures elsewhere.
 """
 
 import ctypes
@@ -85,3 +90,124 @@ def test_noalloc_reject_empty_and_limit(gpu):
                                        d_in.data_ptr(), ctypes.byref(cnt))
     assert rc == native.E_CAPACITY
     p.close()
+
+
+def _lex_record(p, data, lay):
+    """The lexer-mode response record built from the no-alloc entry point's tokens."""
+    import torch
+
+    from alpacc_b200 import wire
+    d_in = torch.frombuffer(bytearray(data) or bytearray(1), dtype=torch.uint8).cuda()
+    rc, (ids, starts, lens) = _tokens_noalloc(p, d_in, len(data), lay)
+    assert rc in (native.OK, native.REJECT), rc
+    if rc == native.REJECT:
+        return b"\x00"
+    return wire.encode_lex_record(wire.LexResult(True, ids, starts, lens), lay)
+
+
+@pytest.mark.parametrize("config", ["json_ext_i32", "arithmetic_i64", "sexp_i64"])
+def test_noalloc_matches_reference_lexer_records(gpu, config):
+    """Against the reference's own lexer-mode program (oracle/_ref) and its
+    committed records, with a handle holding the lexer-mode tables."""
+    import json
+    import os
+
+    from oracle.ref import RefOracle, available
+    name = cases.mode_name(config, "lexer")
+    p = native.Parser(cases.tables(config, "lexer"), device=0)
+    lay = p.layout
+    try:
+        golden = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                             "records_modes.json"))).get(name, [])
+        for it in golden:
+            data = bytes.fromhex(it["input"])
+            assert _lex_record(p, data, lay).hex() == it["record"], data[:40]
+        if available(name):
+            ref = RefOracle(name)
+            for data in cases.case_inputs(config)[:40] + [cases.generated(config, 5 << 20, 21)]:
+                assert _lex_record(p, data, lay) == ref.run_case(data), data[:40]
+    finally:
+        p.close()
+
+
+def test_noalloc_exactly_at_limit(gpu):
+    """An input of exactly 16 MiB (the largest accepted) against the oracle."""
+    from oracle.port import PortOracle
+    t = cases.tables("json_ext_i32", "lexer")
+    data = W.json_doc(16 << 20, 31)
+    p = native.Parser(t, device=0)
+    try:
+        assert _lex_record(p, data, p.layout) == PortOracle(t).run_case(data)
+    finally:
+        p.close()
+
+
+def test_noalloc_keyword_lexer_near_state_limit(gpu):
+    """A 24-keyword lexer (124 machine states: per-start lanes, per-tile
+    transition vectors of 124 entries) against the oracle."""
+    from alpacc_b200.grammar.tables import generate_parts
+    from oracle.port import PortOracle
+    from tests.random_grammars import keyword_grammar, keyword_inputs
+    t = generate_parts(keyword_grammar(24), "kw24", False, "lexer")
+    p = native.Parser(t, device=0)
+    po = PortOracle(t)
+    try:
+        assert p.info()["M"] > 100
+        for data in keyword_inputs(24, seed=5, sizes=(1, 300, 15000, 40000, 400000)):
+            assert _lex_record(p, data, p.layout) == po.run_case(data), data[:40]
+    finally:
+        p.close()
+
+
+def test_noalloc_length_overflow(gpu):
+    """json_ext's length_t is 16 bits: a 70 000-byte string token is rejected
+    (lex_string's length check), a 65 535-byte one is accepted with that
+    length; both span several lexer tiles."""
+    from oracle.port import PortOracle
+    t = cases.tables("json_ext_i32", "lexer")
+    po = PortOracle(t)
+    p = native.Parser(t, device=0)
+    try:
+        for body, ok in ((70000 - 2, False), (65535 - 2, True), (65536 - 2, False)):
+            data = b'[1, "' + b"x" * body + b'", 2]'
+            rec = _lex_record(p, data, p.layout)
+            assert rec == po.run_case(data)
+            assert rec[0] == (1 if ok else 0)
+    finally:
+        p.close()
+
+
+def test_noalloc_allocates_nothing(gpu):
+    """On a fresh handle, the first and the later calls make no device
+    allocation (the library's own counter, and the device's free memory)."""
+    import torch
+    p = native.Parser(cases.tables("json_ext_i32"), device=0)
+    lay = p.layout
+    data = cases.generated("json_ext_i32", 2 << 20, 8)
+    n = len(data)
+    d_in = torch.frombuffer(bytearray(data), dtype=torch.uint8).cuda()
+    ids = torch.zeros(n * lay.terminal, dtype=torch.uint8, device="cuda")
+    starts = torch.zeros(n * lay.index, dtype=torch.uint8, device="cuda")
+    lens = torch.zeros(n * lay.length, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    L = _lib()
+    cnt = ctypes.c_uint64(0)
+
+    def call():
+        return L.alpacc_gpu_lex_noalloc(p._h, d_in.data_ptr(), n, ids.data_ptr(), starts.data_ptr(),
+                                        lens.data_ptr(), ctypes.byref(cnt))
+
+    try:
+        allocs0 = native.lib().alpacc_device_allocations()
+        assert call() == native.OK  # the first call on this handle
+        assert native.lib().alpacc_device_allocations() == allocs0
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        for _ in range(3):
+            assert call() == native.OK
+        torch.cuda.synchronize()
+        assert native.lib().alpacc_device_allocations() == allocs0
+        assert torch.cuda.mem_get_info()[0] == free0
+        assert cnt.value > 0
+    finally:
+        p.close()
