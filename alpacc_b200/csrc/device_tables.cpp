@@ -109,8 +109,8 @@ static int build_lexer(const alpacc_tables *t, int ignore, LexerMachine *lm, std
     if ((int)sig.size() == before) break;
   }
   const int M = *std::max_element(cls.begin(), cls.end()) + 1;
-  // the device transition entries hold a 7-bit state and the produce bit
-  if (M > 128) { *why = "minimised lexer automaton exceeds 128 states"; return ALPACC_E_UNSUPPORTED; }
+  // the device keeps machine states in bytes
+  if (M > kMaxMachine) { *why = "minimised lexer automaton exceeds 255 states"; return ALPACC_E_UNSUPPORTED; }
   std::vector<std::vector<int>> T(M, std::vector<int>(C0));
   std::vector<uint8_t> sterm(M), sflags(M);
   for (int i = 0; i < R; i++) {
@@ -173,7 +173,7 @@ static int build_lexer(const alpacc_tables *t, int ignore, LexerMachine *lm, std
     }
     lm->max_lanes = std::max(lm->max_lanes, (int)targets.size());
     if ((int)targets.size() > kMaxLanes) {
-      *why = "a byte class reaches more than 16 live states";
+      *why = "a byte class reaches more than 32 live states";
       return ALPACC_E_UNSUPPORTED;
     }
     lm->img_cnt[c] = (uint8_t)targets.size();
@@ -191,6 +191,47 @@ static int build_lexer(const alpacc_tables *t, int ignore, LexerMachine *lm, std
         lm->img2[(size_t)c0 * C + c1] = mask;
       }
   }
+  return ALPACC_OK;
+}
+
+int build_lexer_table(const LexerMachine &lm, LexerTable *out, std::string *why) {
+  int cp = 1, lg = 0;
+  while (cp < lm.C) {
+    cp <<= 1;
+    lg++;
+  }
+  const uint32_t swz = (uint32_t)std::min(cp, 32) - 1;
+  const int shift = lg + 2;
+  const size_t words = (size_t)lm.M * cp;
+  if (words * 4 + 512 > 160 * 1024) {
+    *why = "lexer table exceeds the shared-memory budget (states x padded byte classes)";
+    return ALPACC_E_UNSUPPORTED;
+  }
+  auto F = [&](uint32_t x) { return (x << shift) | ((x & swz) << 2); };
+  out->tab.assign(words, 0);
+  for (int s = 0; s < lm.M; s++)
+    for (int c = 0; c < cp; c++) {
+      uint32_t e = F((uint32_t)s) | (0xFFu << 24);  // columns >= C are never read
+      if (c < lm.C) {
+        const uint32_t nx = lm.trans[(size_t)s * lm.C + c];
+        uint32_t code = 0xFF;
+        if (lm.flags[nx] & 1) {
+          const bool kept = (lm.flags[s] & 4) != 0;
+          if (kept && lm.term[s] >= 0xFE) {
+            *why = "terminal id 254 or 255 collides with the lexer's boundary codes";
+            return ALPACC_E_UNSUPPORTED;
+          }
+          code = kept ? lm.term[s] : 0xFE;
+        }
+        e = F(nx) | (code << 24);
+      }
+      out->tab[(size_t)s * cp + ((uint32_t)c ^ ((uint32_t)s & swz))] = e;
+    }
+  out->cls4.resize(256);
+  for (int b = 0; b < 256; b++) out->cls4[b] = (uint16_t)(lm.cls[b] * 4);
+  out->shift = shift;
+  out->swz = (int)swz;
+  out->wide_cls = lm.C > 64 ? 1 : 0;
   return ALPACC_OK;
 }
 

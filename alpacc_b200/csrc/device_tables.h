@@ -9,7 +9,7 @@
 
 namespace alpacc {
 
-constexpr int kMaxLanes = 16;     // distinct live states a chunk may start with
+constexpr int kMaxLanes = 32;     // distinct live states a chunk may start with
 constexpr int kMaxMachine = 255;  // states of the minimised lexer automaton (u8)
 
 // The sequential lexer of backends/c/lexer.c run over encoded endomorphism
@@ -36,6 +36,23 @@ struct LexerMachine {
   // reaches live state s on a byte of class c0 followed by one of class c1
   std::vector<unsigned long long> img2;
 };
+
+// The lexer kernel's shared-memory form of the machine: rows of CP >= C
+// 32-bit entries (CP a power of two), entry(s, c) stored at
+// s * CP + (c ^ (s & swz)) = F(next) | code << 24, where F(x) = (x << shift) |
+// ((x & swz) << 2) is the byte offset of x's row (so F(s) ^ (c * 4) is the
+// byte offset of entry (s, c)), and code is what happens before the byte:
+// 0xFF no token boundary, 0xFE the token ending there is ignored, else its
+// terminal id.
+struct LexerTable {
+  std::vector<uint32_t> tab;   // [M * CP]
+  std::vector<uint16_t> cls4;  // [256] class * 4
+  int shift = 2;               // log2(CP) + 2
+  int swz = 0;                 // min(CP, 32) - 1
+  int wide_cls = 0;            // class * 4 does not fit a byte (C > 64)
+};
+
+int build_lexer_table(const LexerMachine &lm, LexerTable *out, std::string *why);
 
 // LLP pair table as a dense array indexed by the key's terminals in base NT
 // (NT = END + 1): entry = record index or 0xffffffff when the reference's

@@ -135,3 +135,84 @@ def test_pair_table_random_grammars(harness):
     L.pair_lookup.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
     for name, g, t in fuzz_grammars(16):
         assert _check_pairs(L, t) > 0, name
+
+
+@pytest.fixture(scope="module")
+def emu(tmp_path_factory):
+    so = str(tmp_path_factory.mktemp("emu") / "liblexer_emu.so")
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-shared", "-fPIC",
+                           "-I", os.path.join(REPO, "alpacc_b200", "csrc"), "-I", os.path.join(REPO, "include"),
+                           os.path.join(HERE, "native", "lexer_emu.cpp"),
+                           os.path.join(REPO, "alpacc_b200", "csrc", "device_tables.cpp"), "-o", so])
+    L = ctypes.CDLL(so)
+    L.lexer_emu.restype = ctypes.c_int
+    L.lexer_emu.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p,
+                            ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64), ctypes.c_void_p,
+                            ctypes.POINTER(ctypes.c_uint64)]
+    return L
+
+
+def _emu_vs_machine(L, M, t, inputs):
+    """The tile algorithm of the lexer kernel (emulated) against the machine
+    walked byte by byte: status and every lexeme."""
+    s, keep = native.make_tables(t)
+    states = ctypes.c_int(0)
+    stats = np.zeros(4, dtype=np.int64)
+    total = np.zeros(4, dtype=np.int64)
+    for d in inputs:
+        cap = len(d) + 1
+        want = np.zeros(3 * cap, dtype=np.uint64)
+        got = np.zeros(3 * cap, dtype=np.uint64)
+        cw, cg, lb = ctypes.c_uint64(0), ctypes.c_uint64(0), ctypes.c_uint64(0)
+        rw = M.machine_lex(ctypes.byref(s), d, len(d), want.ctypes.data, cap, ctypes.byref(cw), ctypes.byref(states))
+        rg = L.lexer_emu(ctypes.byref(s), d, len(d), 0, got.ctypes.data, cap, ctypes.byref(cg), stats.ctypes.data,
+                         ctypes.byref(lb))
+        total += stats
+        assert rg == rw, (t.name, len(d), d[:40], rg, rw)
+        if rw == native.OK:
+            assert cg.value == cw.value, (t.name, len(d))
+            assert np.array_equal(got[: 3 * cg.value], want[: 3 * cw.value]), (t.name, len(d), d[:40])
+    return total
+
+
+TILE = 14880
+
+
+@pytest.mark.parametrize("config", sorted(cases.CONFIGS))
+def test_lexer_tile_algorithm(harness, emu, config):
+    ins = cases.case_inputs(config, sizes=(1, 59, 60, 61, 3000, TILE - 1, TILE, TILE + 1, 3 * TILE + 7),
+                            seeds=(0,))
+    _emu_vs_machine(emu, harness, cases.tables(config, "both"), ins)
+
+
+def test_lexer_tile_algorithm_open_chunks(harness, emu):
+    """Inputs whose chunks never converge (a numeric array on one line is
+    valid both inside and outside a JSON string): per-lane chunk functions and
+    tiles without a constant chunk (transition vectors, look-back)."""
+    t = cases.tables("json_ext_i32")
+    rng = np.random.default_rng(7)
+    nums = b"[" + b", ".join(str(int(x)).encode() for x in rng.integers(0, 1000, 30000)) + b"]"
+    mixed = b'{"a": ' + nums + b', "b": "x y z"}'
+    bad = nums[:50000] + b"\x01" + nums[50000:]
+    stats = _emu_vs_machine(emu, harness, t, [nums, mixed, bad, nums[:TILE * 2 + 5] + b"]"])
+    assert stats[0] > 1000 and stats[2] > 0  # open chunks and look-back tiles were exercised
+
+
+def test_lexer_tile_algorithm_rejects_and_lengths(harness, emu):
+    from alpacc_b200 import workloads as W
+    t = cases.tables("json_ext_i32")
+    docs = [b'[1, "' + b"x" * k + b'", 2]' for k in (65533, 65534, 69998)]
+    docs += [b"[1," + b" " * 70000 + b"2]", W.json_doc(200000, 3)[:-3] + b"\x02\x03]", b'"' + b"a" * 40000]
+    _emu_vs_machine(emu, harness, t, docs)
+
+
+@pytest.mark.parametrize("nkw", [8, 24, 32])
+def test_lexer_tile_algorithm_keyword_lexers(harness, emu, nkw):
+    """Machines above 64 states (256-bit state sets) and many start lanes."""
+    t = generate_parts(keyword_grammar(nkw), "kw%d" % nkw, False, "both")
+    _emu_vs_machine(emu, harness, t, keyword_inputs(nkw, seed=nkw, sizes=(0, 1, 20, 300, 15000, 40000)))
+
+
+def test_lexer_tile_algorithm_random_grammars(harness, emu):
+    for name, g, t in fuzz_grammars(16):
+        _emu_vs_machine(emu, harness, t, g.inputs(0, sentences=(8, 300), noise=(500, 15000)))
