@@ -46,32 +46,22 @@ int upload_pairs(alpacc_gpu_grammar *g);
 
 int upload_tables(alpacc_gpu_grammar *g) {
   const LexerMachine &lm = g->hg.lex;
-  if (lm.M > 128) return ALPACC_E_UNSUPPORTED;  // 7-bit states in the transition entries
   if (g->hg.parts == ALPACC_PARTS_PARSER) return upload_pairs(g);
-  // transition entries at class * M + state: next state | produce(next) << 7
-  const size_t mc = (size_t)lm.M * lm.C;
-  std::vector<uint32_t> trw((mc + 3) / 4, 0);
-  for (int c = 0; c < lm.C; c++)
-    for (int m = 0; m < lm.M; m++) {
-      const size_t i = (size_t)c * lm.M + m;
-      const uint32_t nx = lm.trans[(size_t)m * lm.C + c];
-      const uint32_t e = nx | ((lm.flags[nx] & 1u) << 7);
-      trw[i >> 2] |= e << ((i & 3) * 8);
-    }
-  g->trans_word_count = (int)trw.size();
-  // copies of the byte-class and transition tables in shared memory: more
-  // copies mean fewer bank conflicts on data-dependent lookups, but fewer
-  // resident CTAs; measured on json_ext, occupancy wins - keep a CTA's tables
-  // within ~12 KB
-  int copies = 32;
-  while (copies > 1 && (size_t)copies * (trw.size() * 4 + 512) > 12 * 1024) copies >>= 1;
-  if (const char *e = getenv("ALPACC_LEX_COPIES")) {
-    int v = atoi(e);
-    if (v >= 1 && v <= 32 && (v & (v - 1)) == 0) copies = v;
+  LexerTable lt;
+  const int rc = build_lexer_table(lm, &lt, &g->last_error);
+  if (rc != ALPACC_OK) return rc;
+  g->tab_words = (int)lt.tab.size();
+  g->cp_shift = lt.shift;
+  g->swz = lt.swz;
+  g->wide_cls = lt.wide_cls;
+  g->lex_w4 = lm.M > 64 ? 1 : 0;
+  if (g->wide_cls) {
+    TRY(upload(g->lex_cls4, lt.cls4));
+  } else {
+    std::vector<uint8_t> c4(lt.cls4.begin(), lt.cls4.end());
+    TRY(upload(g->lex_cls4, c4));
   }
-  g->trans_rep = copies;
-  TRY(upload(g->cls_id, lm.cls));
-  TRY(upload(g->trans_words, trw));
+  TRY(upload(g->lex_tab, lt.tab));
   TRY(upload(g->lane_of, lm.lane_of));
   TRY(upload(g->img, lm.img));
   TRY(upload(g->img_cnt, lm.img_cnt));
@@ -119,15 +109,14 @@ void collect_stages(alpacc_gpu_grammar *g) {
   }
 }
 
-size_t lex_smem_bytes(const alpacc_gpu_grammar *g) { return lex_dyn_smem(g); }
-
 // The kernel attribute is per function, shared by every handle: only raise it.
 int ensure_lex_smem(size_t bytes) {
   static std::mutex mu;
   static size_t current = 0;
   std::lock_guard<std::mutex> lock(mu);
   if (bytes <= current) return ALPACC_OK;
-  if (cudaFuncSetAttribute(lex_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) {
+  if (cudaFuncSetAttribute(lex_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess ||
+      cudaFuncSetAttribute(lex_kernel_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) {
     cudaGetLastError();
     return ALPACC_E_CUDA;
   }
@@ -214,10 +203,35 @@ struct LexWindow {
   uint64_t index_base;
 };
 
-// The whole device path for d_in[0..n) (n bytes; n token ids for kRunParse).
-// Leaves counts in g->last_T / last_N.
-int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int mode = kRunBoth,
-               const LexWindow *win = nullptr) {
+// Per-call flags, tickets and counters: one region of the handle's `flags`
+// buffer, zeroed by one memset per call (byte offsets, 16-byte aligned).
+struct FlagLayout {
+  size_t lex_ticket = 0, st1_flag = 0, st2_flags = 0, pair_ticket = 0, pst_flags = 0;
+  size_t pse_ticket[2] = {}, pse_flags[2] = {}, queue_len[2] = {}, super_key[2] = {};
+  size_t total = 0;
+  size_t take(size_t bytes) {
+    const size_t off = total;
+    total += (std::max<size_t>(bytes, 16) + 15) & ~(size_t)15;
+    return off;
+  }
+};
+
+// Capacity (elements) of a parser-stage array whose exact size only the
+// device knows: the full bound when it is small; else the largest exact need
+// seen on this handle (with 1/8 slack), at least a floor. A device-side
+// overflow makes the call grow to the exact need and run again.
+uint64_t plan_cap(uint64_t bound, uint64_t need_seen) {
+  constexpr uint64_t kFull = 16ull << 20, kFloor = 16ull << 20;
+  if (bound <= kFull) return bound;
+  const uint64_t seen = need_seen + need_seen / 8;
+  return std::min(bound, std::max(seen, kFloor));
+}
+
+// The whole device path for d_in[0..n) (n bytes; n token ids for kRunParse),
+// launched without waiting for the host in between: each stage reads the
+// counts of the previous one from the device status. Leaves counts in
+// g->last_T / last_N.
+int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int mode, const LexWindow *win) {
   const HostGrammar &hg = g->hg;
   const alpacc_tables &tb = hg.t;
   const LexerMachine &lm = hg.lex;
@@ -225,191 +239,212 @@ int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int mode 
   const int term_w = (int)tb.terminal_size, idx_w = (int)tb.index_size, len_w = (int)tb.length_size;
   const int prod_w = (int)tb.production_size;
   if (n > (1ull << 31) - 1) return ALPACC_E_CAPACITY;
-  CK(cudaMemsetAsync(g->d_status, 0, sizeof(DeviceStatus), g->stream));
   g->launches = 0;
   for (int k = 0; k < alpacc_gpu_grammar::kStages; k++) g->stage_used[k] = false;
+
+  // ---- sizes: bounds from n, capacities for what only the device knows ----
+  const bool lexing = mode != kRunParse && n > 0;
+  const uint64_t lex_tiles = lexing ? (n + kLexData - 1) / kLexData : 0;
+  uint64_t piece_tiles = lex_tiles, pieces = lexing ? 1 : 0;
+  if (lexing && g->h_in) {  // host input: copied in pieces of ~16 MiB, each lexed as soon as it arrived
+    piece_tiles = kPieceTiles;
+    pieces = (lex_tiles + piece_tiles - 1) / piece_tiles;
+    if (pieces > (uint64_t)alpacc_gpu_grammar::kMaxPieces) {
+      piece_tiles = (lex_tiles + alpacc_gpu_grammar::kMaxPieces - 1) / alpacc_gpu_grammar::kMaxPieces;
+      pieces = (lex_tiles + piece_tiles - 1) / piece_tiles;
+    }
+  }
+  const bool parsing = mode != kRunLex;
+  const uint64_t T_ub = n;  // a token covers at least one byte; parser mode: exactly n ids
+  const uint64_t m_ub = T_ub + 2;
+  const uint64_t pair_tiles = parsing ? (m_ub + kPairTile - 1) / kPairTile : 0;
+  const uint64_t max_br = (uint64_t)std::max(pt.max_br, 1), max_pr = (uint64_t)std::max(pt.max_pr, 1);
+  const uint64_t br_cap = parsing ? plan_cap(m_ub * max_br, g->need_br) : 0;
+  const uint64_t pr_cap = parsing ? plan_cap(m_ub * max_pr, g->need_pr) : 0;
+  const uint64_t e_cap = std::max<uint64_t>(std::max(br_cap, pr_cap), 1);
+  const uint64_t pse_tiles = (e_cap + kPseTile - 1) / kPseTile;
+  const uint64_t super_n = (pse_tiles >> kPseSuperShift) + 1;
+
+  FlagLayout fl;
+  fl.lex_ticket = fl.take(16 + pieces * 4);
+  fl.st1_flag = fl.take(lex_tiles * 4);
+  fl.st2_flags = fl.take(lex_tiles * 4);
+  fl.pair_ticket = fl.take(16);
+  fl.pst_flags = fl.take(pair_tiles * 4);
+  for (int w = 0; w < 2; ++w) {
+    fl.pse_ticket[w] = fl.take(16);
+    fl.pse_flags[w] = fl.take(parsing ? pse_tiles * 4 : 0);
+    fl.queue_len[w] = fl.take(16);
+    fl.super_key[w] = fl.take(parsing ? super_n * 4 : 0);
+  }
+  TRY(grow(g->flags, fl.total));
+  uint8_t *fb = (uint8_t *)g->flags.p;
+  if (lexing) {
+    TRY(grow(g->st1_state, lex_tiles));
+    TRY(grow(g->st1_vec, lex_tiles * (uint64_t)lm.M));
+    TRY(grow(g->st2_agg, lex_tiles * 16));
+    TRY(grow(g->st2_inc, lex_tiles * 16));
+    // tokens: at most one per byte (n + 1 leaves room for what a rejected
+    // input's chunks may write before the reject is known)
+    TRY(grow(g->tok_ids, (n + 1) * term_w));
+    TRY(grow(g->tok_starts, (n + 1) * idx_w));
+    TRY(grow(g->tok_lens, (n + 1) * len_w));
+  }
+  if (parsing) {
+    TRY(grow(g->tok_ids, std::max<uint64_t>(T_ub, 1) * term_w));
+    TRY(grow(g->pst_agg, pair_tiles * 16));
+    TRY(grow(g->pst_inc, pair_tiles * 16));
+    TRY(grow(g->br, br_cap * 4));
+    TRY(grow(g->pr, pr_cap * 4));
+    TRY(grow(g->pse_agg, pse_tiles * 16));
+    TRY(grow(g->pse_inc, pse_tiles * 16));
+    TRY(grow(g->ch_h0, pse_tiles * kPseThreads * 4));
+    TRY(grow(g->ch_tc, pse_tiles * kPseThreads * 4));
+    TRY(grow(g->chunk_min, pse_tiles * kPseThreads * 4));
+    TRY(grow(g->tile_min, pse_tiles * 4));
+    TRY(grow(g->queue, e_cap * 8));
+    TRY(grow(g->node_prods, std::max<uint64_t>(pr_cap, 1) * prod_w));
+    TRY(grow(g->node_parents, std::max<uint64_t>(pr_cap, 1) * idx_w));
+    TRY(grow(g->token_parents, std::max<uint64_t>(T_ub, 1) * idx_w));
+  }
+
+  CK(cudaMemsetAsync(g->d_status, 0, sizeof(DeviceStatus), g->stream));
+  CK(cudaMemsetAsync(fb, 0, fl.total, g->stream));
   CK(cudaEventRecord(g->ev0, g->stream));
 
   // ---------------- lexer ----------------
-  uint64_t T = 0;
   if (mode == kRunParse) {
-    T = n;
-    // from pageable memory: staged before the call returns
+    const uint64_t T = n;  // from pageable memory: staged before the call returns
     CK(cudaMemcpyAsync(&g->d_status->num_tokens, &T, 8, cudaMemcpyHostToDevice, g->stream));
-  } else if (n > 0) {
-    const uint64_t tiles = (n + kLexData - 1) / kLexData;
-    // host input: copied in pieces of ~16 MiB, each piece's tiles lexed as soon as it arrived
-    uint64_t piece_tiles = tiles, pieces = 1;
-    if (g->h_in) {
-      piece_tiles = kPieceTiles;
-      pieces = (tiles + piece_tiles - 1) / piece_tiles;
-      if (pieces > (uint64_t)alpacc_gpu_grammar::kMaxPieces) {
-        piece_tiles = (tiles + alpacc_gpu_grammar::kMaxPieces - 1) / alpacc_gpu_grammar::kMaxPieces;
-        pieces = (tiles + piece_tiles - 1) / piece_tiles;
-      }
+  } else if (lexing) {
+    LexArgs a = lex_args(g, d_in, n, lex_tiles);
+    a.st1_flag = (unsigned *)(fb + fl.st1_flag);
+    a.st2.flags = (unsigned *)(fb + fl.st2_flags);
+    if (win) {
+      a.open_end = win->open_end;
+      a.index_base = win->index_base;
     }
-    TRY(grow(g->lex_ticket, 16 + pieces * 4));
-    TRY(grow(g->st1_flag, tiles * 4));
-    TRY(grow(g->st1_state, tiles));
-    TRY(grow(g->st1_vec, tiles * (uint64_t)lm.M));
-    TRY(grow(g->st2_flags, tiles * 4));
-    TRY(grow(g->st2_agg, tiles * 16));
-    TRY(grow(g->st2_inc, tiles * 16));
-    TRY(grow(g->tok_ids, n * term_w));
-    TRY(grow(g->tok_starts, n * idx_w));
-    TRY(grow(g->tok_lens, n * len_w));
-    // staged tokens: at most one per data byte of a tile, plus the final token of the last tile
-    const uint64_t cap = tiles * (uint64_t)kLexData + 16;
-    TRY(grow(g->stage_ids, cap));
-    TRY(grow(g->stage_starts, cap * 4));
-    TRY(grow(g->stage_ends, cap * 4));
-    TRY(grow(g->tile_cnt, tiles * 4));
-    TRY(grow(g->tile_pos, tiles * 4));
-    TRY(grow(g->tile_off, tiles * 8));
-    TRY(grow(g->tile_prev, tiles * 4));
-    CK(cudaMemsetAsync(g->lex_ticket.p, 0, 16 + pieces * 4, g->stream));
-    CK(cudaMemsetAsync(g->st1_flag.p, 0, tiles * 4, g->stream));
-    CK(cudaMemsetAsync(g->st2_flags.p, 0, tiles * 4, g->stream));
-    LexArgs a = lex_args(g, d_in, n, tiles);
-    if (win) a.open_end = win->open_end;
-    LexPlaceArgs pa = lex_place_args(g, a, tiles);
-    if (win) pa.index_base = win->index_base;
     stage_begin(g, 0);
     for (uint64_t k = 0; k < pieces; ++k) {
-      const uint64_t tb = k * piece_tiles, te = std::min(tiles, tb + piece_tiles);
+      const uint64_t t0 = k * piece_tiles, t1 = std::min(lex_tiles, t0 + piece_tiles);
       if (g->h_in) {
-        const uint64_t b0 = tb * kLexData, b1 = std::min<uint64_t>(n, te * kLexData);
+        const uint64_t b0 = t0 * kLexData, b1 = std::min<uint64_t>(n, t1 * kLexData);
         CK(cudaMemcpyAsync((uint8_t *)d_in + b0, g->h_in + b0, b1 - b0, cudaMemcpyHostToDevice, g->cstream));
         CK(cudaEventRecord(g->piece_ev[k], g->cstream));
         CK(cudaStreamWaitEvent(g->stream, g->piece_ev[k], 0));
       }
-      a.tile_begin = tb;
-      a.tile_end = te;
-      a.ticket = (unsigned *)g->lex_ticket.p + 4 + k;
-      const unsigned grid = (unsigned)std::min<uint64_t>(te - tb, (uint64_t)g->lex_grid);
-      lex_kernel<<<grid, kLexThreads, lex_smem_bytes(g), g->stream>>>(a);
-    ++g->launches;
-      CK(cudaGetLastError());
+      a.tile_begin = t0;
+      a.tile_end = t1;
+      a.ticket = (unsigned *)(fb + fl.lex_ticket) + 4 + k;
+      const unsigned grid = (unsigned)std::min<uint64_t>(t1 - t0, (uint64_t)g->lex_grid);
+      CK(launch_lex(g, a, grid, g->stream));
+      ++g->launches;
     }
-    lex_scan_kernel<<<1, kLexScanThreads, 0, g->stream>>>(pa);
-    ++g->launches;
-    CK(cudaGetLastError());
-    lex_place_kernel<<<(unsigned)std::min<uint64_t>(tiles, 148 * 8), 256, 0, g->stream>>>(pa);
-    ++g->launches;
     stage_end(g, 0);
-    CK(cudaGetLastError());
-    if (g->host_out) CK(cudaEventRecord(g->lex_done, g->stream));
-    int rc = sync_status(g);
-    if (rc) return rc;
-    if (g->h_status->reject) return ALPACC_REJECT;
-    T = g->h_status->num_tokens;
-    if (g->host_out) TRY(start_token_copy(g, T));
   }
-  if (mode == kRunLex) {
-    CK(cudaEventRecord(g->ev1, g->stream));
-    CK(cudaStreamSynchronize(g->stream));
-    float ms = 0;
-    if (cudaEventElapsedTime(&ms, g->ev0, g->ev1) == cudaSuccess) g->last_ms = ms;
-    collect_stages(g);
-    g->last_T = T;
-    g->last_N = 0;
-    return ALPACC_OK;
+  CK(cudaEventRecord(g->lex_done, g->stream));
+  // host calls: the lexer's status is read back on the copy stream while the
+  // parser runs, so that the token arrays can follow at once
+  if (g->host_out && parsing && lexing) {
+    CK(cudaStreamWaitEvent(g->cstream, g->lex_done, 0));
+    CK(cudaMemcpyAsync(g->h_lex_status, g->d_status, sizeof(DeviceStatus), cudaMemcpyDeviceToHost, g->cstream));
+    CK(cudaEventRecord(g->lex_status_ev, g->cstream));
   }
 
-  // ---------------- pair lookup ----------------
-  const uint64_t m = T + 2;
-  const uint64_t br_cap = m * (uint64_t)std::max(pt.max_br, 1);
-  const uint64_t pr_cap = m * (uint64_t)std::max(pt.max_pr, 1);
-  {
-    const uint64_t tiles = (m + kPairTile - 1) / kPairTile;
-    TRY(grow(g->pair_ticket, 16));
-    TRY(grow(g->pst_flags, tiles * 4));
-    TRY(grow(g->pst_agg, tiles * 16));
-    TRY(grow(g->pst_inc, tiles * 16));
-    TRY(grow(g->br, br_cap * 4));
-    TRY(grow(g->pr, pr_cap * 4));
-    TRY(grow(g->tok_ids, std::max<uint64_t>(T, 1) * term_w));
-    CK(cudaMemsetAsync(g->pair_ticket.p, 0, 16, g->stream));
-    CK(cudaMemsetAsync(g->pst_flags.p, 0, tiles * 4, g->stream));
+  if (parsing) {
+    // ---------------- pair lookup ----------------
     if (n == 0 && mode != kRunParse) CK(cudaMemsetAsync(&g->d_status->num_tokens, 0, 8, g->stream));
     PairArgs a = pair_args(g);
-    a.num_tiles = tiles;
+    a.tiles_cap = pair_tiles;
     a.br_cap = br_cap;
     a.pr_cap = pr_cap;
+    a.ticket = (unsigned *)(fb + fl.pair_ticket);
+    a.st.flags = (unsigned *)(fb + fl.pst_flags);
     stage_begin(g, 1);
-    pair_kernel<<<(unsigned)tiles, kPairThreads, 0, g->stream>>>(a);
+    pair_kernel<<<(unsigned)std::min<uint64_t>(pair_tiles, (uint64_t)g->pair_grid), kPairThreads, 0, g->stream>>>(a);
     ++g->launches;
     stage_end(g, 1);
     CK(cudaGetLastError());
-    int rc = sync_status(g);
-    if (rc) return rc;
-    if (g->h_status->reject) return ALPACC_REJECT;
-  }
-  const uint64_t B = g->h_status->num_brackets;
-  const uint64_t P = g->h_status->num_productions;
 
-  // ---------------- depth walks (the parent walk also writes the compacted tree) ----------------
-  const uint64_t Emax = std::max<uint64_t>(std::max(B, P), 1);
-  const uint64_t pse_tiles_max = (Emax + kPseTile - 1) / kPseTile;
-  TRY(grow(g->pse_ticket, 16));
-  TRY(grow(g->pse_flags, pse_tiles_max * 4));
-  TRY(grow(g->pse_agg, pse_tiles_max * 16));
-  TRY(grow(g->pse_inc, pse_tiles_max * 16));
-  TRY(grow(g->ch_h0, pse_tiles_max * kPseThreads * 4));
-  TRY(grow(g->ch_tc, pse_tiles_max * kPseThreads * 4));
-  TRY(grow(g->tile_min, pse_tiles_max * 4));
-  TRY(grow(g->chunk_min, pse_tiles_max * kPseThreads * 4));
-  TRY(grow(g->super_min, ((pse_tiles_max >> kPseSuperShift) + 1) * 4));
-  TRY(grow(g->queue, Emax * 8));
-  TRY(grow(g->queue_len, 16));
-  TRY(grow(g->node_prods, std::max<uint64_t>(P, 1) * prod_w));
-  TRY(grow(g->node_parents, std::max<uint64_t>(P, 1) * idx_w));
-  TRY(grow(g->token_parents, std::max<uint64_t>(T, 1) * idx_w));
-  const int walks = mode == kRunParse ? 1 : 2;  // the parser-mode result has no tree
-  for (int walk = 0; walk < walks; ++walk) {
-    const uint64_t E = walk == kPseBrackets ? B : P;
-    if (E == 0) continue;
-    const uint64_t tiles = (E + kPseTile - 1) / kPseTile;
-    CK(cudaMemsetAsync(g->pse_ticket.p, 0, 16, g->stream));
-    CK(cudaMemsetAsync(g->pse_flags.p, 0, tiles * 4, g->stream));
-    CK(cudaMemsetAsync(g->queue_len.p, 0, 16, g->stream));
-    CK(cudaMemsetAsync(g->super_min.p, 0x7f, ((tiles >> kPseSuperShift) + 1) * 4, g->stream));
-    PseArgs a = pse_args(g, walk, Emax);
-    a.num_tiles = tiles;
-    stage_begin(g, 2 + 2 * walk);
-    pse_tile_kernel<<<(unsigned)tiles, kPseThreads, 0, g->stream>>>(a);
-    ++g->launches;
-    stage_end(g, 2 + 2 * walk);
-    CK(cudaGetLastError());
-    stage_begin(g, 3 + 2 * walk);
-    pse_resolve_kernel<<<148 * 8, 256, 0, g->stream>>>(a);
-    ++g->launches;
-    stage_end(g, 3 + 2 * walk);
-    CK(cudaGetLastError());
+    // ------- depth walks (the parent walk also writes the compacted tree) -------
+    const int walks = mode == kRunParse ? 1 : 2;  // the parser-mode result has no tree
+    for (int walk = 0; walk < walks; ++walk) {
+      PseArgs pa = pse_args(g, walk, e_cap);
+      pa.elem_cap = walk == kPseBrackets ? br_cap : pr_cap;
+      pa.ticket = (unsigned *)(fb + fl.pse_ticket[walk]);
+      pa.st.flags = (unsigned *)(fb + fl.pse_flags[walk]);
+      pa.queue_len = (unsigned long long *)(fb + fl.queue_len[walk]);
+      pa.super_key = (uint32_t *)(fb + fl.super_key[walk]);
+      const uint64_t tiles = (pa.elem_cap + kPseTile - 1) / kPseTile;
+      stage_begin(g, 2 + 2 * walk);
+      pse_tile_kernel<<<(unsigned)std::max<uint64_t>(std::min<uint64_t>(tiles, (uint64_t)g->pse_grid), 1), kPseThreads,
+                        0, g->stream>>>(pa);
+      ++g->launches;
+      stage_end(g, 2 + 2 * walk);
+      CK(cudaGetLastError());
+      stage_begin(g, 3 + 2 * walk);
+      pse_resolve_kernel<<<148 * 8, 256, 0, g->stream>>>(pa);
+      ++g->launches;
+      stage_end(g, 3 + 2 * walk);
+      CK(cudaGetLastError());
+    }
+    if (mode == kRunParse) {  // parse_test's productions at production_t width
+      narrow_u32_kernel<<<(unsigned)std::max<uint64_t>(std::min<uint64_t>((pr_cap + 1023) / 1024, 148 * 8), 1), 256, 0,
+                          g->stream>>>((const uint32_t *)g->pr.p, g->node_prods.p, &g->d_status->num_productions,
+                                       pr_cap, prod_w);
+      ++g->launches;
+      CK(cudaGetLastError());
+    }
   }
-  if (mode == kRunParse && P > 0) {  // parse_test's productions at production_t width
-    narrow_u32_kernel<<<(unsigned)std::min<uint64_t>((P + 1023) / 1024, 148 * 8), 256, 0, g->stream>>>(
-        (const uint32_t *)g->pr.p, g->node_prods.p, P, prod_w);
-    ++g->launches;
-    CK(cudaGetLastError());
-  }
-  if (P == 0 || mode == kRunParse) CK(cudaMemsetAsync(&g->d_status->num_nodes, 0, 8, g->stream));
   CK(cudaEventRecord(g->ev1, g->stream));
+
+  // ---- host calls: the token arrays, copied while the parser runs ----
+  if (g->host_out && parsing && lexing) {
+    CK(cudaEventSynchronize(g->lex_status_ev));
+    const DeviceStatus &ls = *g->h_lex_status;
+    if (ls.error == 0 && !ls.reject) TRY(start_token_copy(g, ls.num_tokens));
+  }
   int rc = sync_status(g);
-  if (rc) return rc;
   float ms = 0;
   if (cudaEventElapsedTime(&ms, g->ev0, g->ev1) == cudaSuccess) g->last_ms = ms;
   collect_stages(g);
-  if (g->h_status->reject) return ALPACC_REJECT;
-  if (mode == kRunParse) {
-    g->last_T = T;
-    g->last_N = P;
+  const DeviceStatus &st = *g->h_status;
+  if (parsing) {  // exact needs of this input, for the capacities of later calls
+    g->need_br = std::max<uint64_t>(g->need_br, st.num_brackets);
+    g->need_pr = std::max<uint64_t>(g->need_pr, st.num_productions);
+  }
+  if (rc) return rc;
+  if (st.reject) return ALPACC_REJECT;
+  const uint64_t T = mode == kRunParse ? n : st.num_tokens;
+  if (g->host_out && mode == kRunLex) TRY(start_token_copy(g, T));
+  g->last_T = T;
+  if (mode == kRunLex) {
+    g->last_N = 0;
     return ALPACC_OK;
   }
-  if (P == 0 && T != 0) return ALPACC_REJECT;  // compact_tree: terminal count mismatch
-  g->last_T = T;
-  g->last_N = g->h_status->num_nodes;
+  if (mode == kRunParse) {
+    g->last_N = st.num_productions;
+    return ALPACC_OK;
+  }
+  if (st.num_productions == 0 && T != 0) return ALPACC_REJECT;  // compact_tree: terminal count mismatch
+  g->last_N = st.num_nodes;
   return ALPACC_OK;
+}
+
+// run_device_once, and once more with capacities grown to the exact needs
+// when a parser-stage array overflowed on the device (a first call on an
+// input larger than any before).
+int run_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int mode = kRunBoth,
+               const LexWindow *win = nullptr) {
+  int rc = run_device_once(g, d_in, n, mode, win);
+  if (rc == ALPACC_E_CAPACITY && n <= (1ull << 31) - 1) {
+    abandon_host_result(g);
+    const uint8_t *h_in = g->h_in;
+    g->h_in = nullptr;  // the input is on the device already
+    rc = run_device_once(g, d_in, n, mode, win);
+    g->h_in = h_in;
+  }
+  return rc;
 }
 
 void fill_device_result(alpacc_gpu_grammar *g, alpacc_result *out, int status) {
@@ -457,13 +492,15 @@ alpacc_gpu_grammar *alpacc_gpu_load(const alpacc_tables *tables, int device, uin
       }() ||
       cudaStreamCreateWithFlags(&g->cstream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&g->lex_done, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&g->lex_status_ev, cudaEventDisableTiming) != cudaSuccess ||
       [&] {
         for (auto &e : g->piece_ev)
           if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return true;
         return false;
       }() ||
       alpacc::dev_malloc(reinterpret_cast<void **>(&g->d_status), sizeof(DeviceStatus)) != cudaSuccess ||
-      cudaMallocHost(&g->h_status, sizeof(DeviceStatus)) != cudaSuccess) {
+      cudaMallocHost(&g->h_status, sizeof(DeviceStatus)) != cudaSuccess ||
+      cudaMallocHost(&g->h_lex_status, sizeof(DeviceStatus)) != cudaSuccess) {
     cudaGetLastError();
     *err = ALPACC_E_CUDA;
     alpacc_gpu_free(g);
@@ -471,16 +508,21 @@ alpacc_gpu_grammar *alpacc_gpu_load(const alpacc_tables *tables, int device, uin
   }
   std::memset(g->h_status, 0, sizeof(DeviceStatus));
   rc = upload_tables(g);
-  if (rc == ALPACC_OK) rc = ensure_lex_smem(lex_smem_bytes(g));
+  if (rc == ALPACC_OK) rc = ensure_lex_smem(lex_dyn_smem(g));
   if (rc == ALPACC_OK) {
     int per_sm = 0, sms = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lex_kernel, kLexThreads, lex_smem_bytes(g)) !=
-            cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || per_sm < 1) {
+    int pair_sm = 0, pse_sm = 0;
+    if (lex_occupancy(g, &per_sm) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pair_sm, pair_kernel, kPairThreads, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pse_sm, pse_tile_kernel, kPseThreads, 0) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || per_sm < 1 ||
+        pair_sm < 1 || pse_sm < 1) {
       cudaGetLastError();
       rc = ALPACC_E_CUDA;
     } else {
       g->lex_grid = per_sm * sms;
+      g->pair_grid = pair_sm * sms;
+      g->pse_grid = pse_sm * sms;
     }
   }
   if (rc == ALPACC_OK && max_input > 0) rc = grow(g->in, max_input + 16);
@@ -497,15 +539,14 @@ void alpacc_gpu_free(alpacc_gpu_grammar *g) {
   if (!g) return;
   cudaSetDevice(g->device);
   if (g->stream) cudaStreamSynchronize(g->stream);
-  DevBuf *bufs[] = {&g->cls_id, &g->trans_words, &g->lane_of, &g->img, &g->img_cnt, &g->img2, &g->sterm, &g->sflags,
+  DevBuf *bufs[] = {&g->lex_tab, &g->lex_cls4, &g->lane_of, &g->img, &g->img_cnt, &g->img2, &g->sterm, &g->sflags,
                     &g->dense, &g->rec, &g->stacks, &g->prods,
                     &g->arity, &g->is_term, &g->in, &g->lex_ticket, &g->st1_flag, &g->st1_state, &g->st1_vec,
                     &g->st2_flags, &g->st2_agg, &g->st2_inc, &g->tok_ids, &g->tok_starts, &g->tok_lens,
                     &g->pair_ticket, &g->pst_flags, &g->pst_agg, &g->pst_inc, &g->br, &g->pr, &g->pse_ticket,
                     &g->pse_flags, &g->pse_agg, &g->pse_inc, &g->ch_h0, &g->ch_tc, &g->tile_min,
-                    &g->chunk_min, &g->super_min, &g->queue, &g->queue_len, &g->node_prods, &g->node_parents,
-                    &g->token_parents, &g->stage_ids, &g->stage_starts, &g->stage_ends, &g->tile_cnt,
-                    &g->tile_pos, &g->tile_off, &g->tile_prev, &g->b_arrays, &g->b_desc, &g->b_status,
+                    &g->chunk_min, &g->super_key, &g->queue, &g->queue_len, &g->node_prods, &g->node_parents,
+                    &g->token_parents, &g->flags, &g->b_arrays, &g->b_desc, &g->b_status,
                     &g->b_pack, &g->b_packed};
   for (DevBuf *b : bufs) release(*b);
   if (g->cstream) cudaStreamSynchronize(g->cstream);
@@ -518,6 +559,8 @@ void alpacc_gpu_free(alpacc_gpu_grammar *g) {
   if (g->cstream) cudaStreamDestroy(g->cstream);
   if (g->d_status) cudaFree(g->d_status);
   if (g->h_status) cudaFreeHost(g->h_status);
+  if (g->h_lex_status) cudaFreeHost(g->h_lex_status);
+  if (g->lex_status_ev) cudaEventDestroy(g->lex_status_ev);
   if (g->ev0) cudaEventDestroy(g->ev0);
   if (g->ev1) cudaEventDestroy(g->ev1);
   for (auto &e : g->sev)
@@ -810,22 +853,19 @@ int alpacc_gpu_autotune(alpacc_gpu_grammar *g, const uint8_t *d_sample, uint64_t
   if (!g || (n > 0 && !d_sample) || g->hg.parts == ALPACC_PARTS_PARSER) return ALPACC_E_INVALID;
   const int run_mode = g->hg.parts == ALPACC_PARTS_LEXER ? kRunLex : kRunBoth;
   if (cudaSetDevice(g->device) != cudaSuccess) return ALPACC_E_CUDA;
-  const int keep = g->trans_rep;
-  const size_t per_copy = (size_t)g->trans_word_count * 4 + 512;
-  int best = keep;
+  int max_per_sm = 0, sms = 0;
+  if (lex_occupancy(g, &max_per_sm) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device) != cudaSuccess || max_per_sm < 1) {
+    cudaGetLastError();
+    return ALPACC_E_CUDA;
+  }
+  // the lexer's persistent grid: resident CTAs per SM from the occupancy
+  // limit down (fewer CTAs: less contention for shared-memory banks and the
+  // look-back; more: more latency hidden)
+  int best = max_per_sm;
   double best_ms = -1.0;
-  for (int c = 1; c <= 32; c <<= 1) {
-    if ((size_t)c * per_copy > 64 * 1024) break;  // shared memory per CTA stays modest
-    g->trans_rep = c;
-    int per_sm = 0, sms = 0;
-    if (ensure_lex_smem(lex_smem_bytes(g)) != ALPACC_OK ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lex_kernel, kLexThreads, lex_smem_bytes(g)) !=
-            cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device) != cudaSuccess || per_sm < 1) {
-      cudaGetLastError();
-      continue;
-    }
-    g->lex_grid = per_sm * sms;
+  for (int c = max_per_sm; c >= 1 && c >= max_per_sm - 4; --c) {
+    g->lex_grid = c * sms;
     double ms = 0;
     int ok = 1;
     for (int rep = 0; rep < 3 && ok; ++rep) {  // first run warms up
@@ -838,16 +878,7 @@ int alpacc_gpu_autotune(alpacc_gpu_grammar *g, const uint8_t *d_sample, uint64_t
       best = c;
     }
   }
-  g->trans_rep = best;
-  int per_sm = 0, sms = 0;
-  if (ensure_lex_smem(lex_smem_bytes(g)) != ALPACC_OK ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lex_kernel, kLexThreads, lex_smem_bytes(g)) !=
-          cudaSuccess ||
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device) != cudaSuccess || per_sm < 1) {
-    cudaGetLastError();
-    return ALPACC_E_CUDA;
-  }
-  g->lex_grid = per_sm * sms;
+  g->lex_grid = best * sms;
   if (choice) *choice = best;
   return best_ms < 0 ? ALPACC_E_CUDA : ALPACC_OK;
 }
@@ -858,7 +889,7 @@ void *alpacc_gpu_stream(alpacc_gpu_grammar *g) { return g ? (void *)g->stream : 
 int alpacc_gpu_info(const alpacc_gpu_grammar *g, int64_t *vals, int nvals) {
   if (!g || !vals) return ALPACC_E_INVALID;
   const int64_t v[] = {g->hg.lex.M, g->hg.lex.C, g->hg.lex.max_lanes, g->hg.lex.reachable, g->hg.lex.dead,
-                       g->hg.pairs.nt, (int64_t)g->hg.pairs.rec_ss.size(), g->trans_rep,
+                       g->hg.pairs.nt, (int64_t)g->hg.pairs.rec_ss.size(), g->lex_grid,
                        g->h_status ? g->h_status->lex_reject_reason : 0,
                        g->h_status ? g->h_status->parse_reject_reason : 0,
                        g->h_status ? g->h_status->timeout_site : 0};

@@ -100,13 +100,6 @@ int run_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offset
   BTRY(grow(g->st2_flags, std::max<uint64_t>(lex_tiles, 1) * 4));
   BTRY(grow(g->st2_agg, std::max<uint64_t>(lex_tiles, 1) * 16));
   BTRY(grow(g->st2_inc, std::max<uint64_t>(lex_tiles, 1) * 16));
-  BTRY(grow(g->stage_ids, lex_tiles * (uint64_t)kLexData + 16));
-  BTRY(grow(g->stage_starts, (lex_tiles * (uint64_t)kLexData + 16) * 4));
-  BTRY(grow(g->stage_ends, (lex_tiles * (uint64_t)kLexData + 16) * 4));
-  BTRY(grow(g->tile_cnt, std::max<uint64_t>(lex_tiles, 1) * 4));
-  BTRY(grow(g->tile_pos, std::max<uint64_t>(lex_tiles, 1) * 4));
-  BTRY(grow(g->tile_off, std::max<uint64_t>(lex_tiles, 1) * 8));
-  BTRY(grow(g->tile_prev, std::max<uint64_t>(lex_tiles, 1) * 4));
   BTRY(grow(g->tok_ids, T_cap * term_w));
   BTRY(grow(g->tok_starts, T_cap * idx_w));
   BTRY(grow(g->tok_lens, T_cap * len_w));
@@ -124,7 +117,7 @@ int run_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offset
   BTRY(grow(g->ch_tc, walk_ub * kPseThreads * 4));
   BTRY(grow(g->tile_min, walk_ub * 4));
   BTRY(grow(g->chunk_min, walk_ub * kPseThreads * 4));
-  BTRY(grow(g->super_min, ((walk_ub >> kPseSuperShift) + 1) * 4));
+  BTRY(grow(g->super_key, ((walk_ub >> kPseSuperShift) + 1) * 4));
   const uint64_t qcap = std::max(B_cap, P_cap);
   BTRY(grow(g->queue, qcap * 8));
   BTRY(grow(g->queue_len, 16));
@@ -153,6 +146,7 @@ int run_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offset
   if (total) BCK(cudaMemcpyAsync(g->in.p, bytes + base, total, cudaMemcpyHostToDevice, s));
   BCK(cudaMemsetAsync(g->lex_ticket.p, 0, 16, s));
   BCK(cudaMemsetAsync(g->st1_flag.p, 0, std::max<uint64_t>(lex_tiles, 1) * 4, s));
+  BCK(cudaMemsetAsync(g->st2_flags.p, 0, std::max<uint64_t>(lex_tiles, 1) * 4, s));
   BCK(cudaMemsetAsync(g->pair_ticket.p, 0, 16, s));
   BCK(cudaMemsetAsync(g->pst_flags.p, 0, pair_ub * 4, s));
   g->launches = 0;
@@ -162,12 +156,8 @@ int run_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offset
     LexArgs a = lex_args(g, (const uint8_t *)g->in.p, total, lex_tiles);
     a.batch = d_bd;
     a.status = bd.status;
-    const LexPlaceArgs pa = lex_place_args(g, a, lex_tiles);
-    lex_kernel<<<(unsigned)std::min<uint64_t>(lex_tiles, (uint64_t)g->lex_grid), kLexThreads, lex_dyn_smem(g), s>>>(a);
-    lex_scan_kernel<<<1, kLexScanThreads, 0, s>>>(pa);
-    lex_place_kernel<<<(unsigned)std::min<uint64_t>(lex_tiles, 148 * 8), 256, 0, s>>>(pa);
-    g->launches += 3;
-    BCK(cudaGetLastError());
+    BCK(launch_lex(g, a, (unsigned)std::min<uint64_t>(lex_tiles, (uint64_t)g->lex_grid), s));
+    g->launches += 1;
   }
   // ---- pairs ----
   batch_plan_kernel<<<1, 1024, 0, s>>>(bd, kPlanPairs, bd.pair_tile0, kPairTile);
@@ -188,7 +178,7 @@ int run_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offset
     BCK(cudaMemsetAsync(g->pse_ticket.p, 0, 16, s));
     BCK(cudaMemsetAsync(g->pse_flags.p, 0, ub * 4, s));
     BCK(cudaMemsetAsync(g->queue_len.p, 0, 16, s));
-    BCK(cudaMemsetAsync(g->super_min.p, 0x7f, ((ub >> kPseSuperShift) + 1) * 4, s));
+    BCK(cudaMemsetAsync(g->super_key.p, 0, ((ub >> kPseSuperShift) + 1) * 4, s));
     PseArgs pa = pse_args(g, mode, qcap);
     pa.batch = d_bd;
     pa.status = bd.status;

@@ -142,12 +142,68 @@ struct AddU64 {
 struct AddI64 {
   __device__ __forceinline__ long long operator()(long long a, long long b) const { return a + b; }
 };
+struct MaxI32 {
+  __device__ __forceinline__ int operator()(int a, int b) const { return a > b ? a : b; }
+};
 struct MaxI64 {
   __device__ __forceinline__ long long operator()(long long a, long long b) const { return a > b ? a : b; }
 };
 struct MinI64 {
   __device__ __forceinline__ long long operator()(long long a, long long b) const { return a < b ? a : b; }
 };
+
+// Two 32-bit exclusive scans over the block at once: a sum of `c` and a
+// maximum of `p` (identity 0 for both). `sa` and `sb` need (blockDim.x / 32)
+// elements each.
+__device__ __forceinline__ void block_exclusive_scan2(int *sa, int *sb, int c, int p, int *c_ex, int *p_ex,
+                                                      int *c_tot, int *p_tot) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  int ci = c, pi = p;
+#pragma unroll
+  for (int d = 1; d < kWarp; d <<= 1) {
+    const int oc = __shfl_up_sync(0xffffffffu, ci, d);
+    const int op = __shfl_up_sync(0xffffffffu, pi, d);
+    if (lane >= d) {
+      ci += oc;
+      pi = op > pi ? op : pi;
+    }
+  }
+  if (lane == kWarp - 1) {
+    sa[warp] = ci;
+    sb[warp] = pi;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    int wc = lane < nwarps ? sa[lane] : 0, wp = lane < nwarps ? sb[lane] : 0;
+#pragma unroll
+    for (int d = 1; d < kWarp; d <<= 1) {
+      const int oc = __shfl_up_sync(0xffffffffu, wc, d);
+      const int op = __shfl_up_sync(0xffffffffu, wp, d);
+      if (lane >= d) {
+        wc += oc;
+        wp = op > wp ? op : wp;
+      }
+    }
+    if (lane < nwarps) {
+      sa[lane] = wc;  // inclusive prefix of warp totals
+      sb[lane] = wp;
+    }
+  }
+  __syncthreads();
+  int ec = __shfl_up_sync(0xffffffffu, ci, 1), ep = __shfl_up_sync(0xffffffffu, pi, 1);
+  if (lane == 0) ec = ep = 0;
+  if (warp > 0) {
+    ec += sa[warp - 1];
+    ep = sb[warp - 1] > ep ? sb[warp - 1] : ep;
+  }
+  *c_ex = ec;
+  *p_ex = ep;
+  *c_tot = sa[nwarps - 1];
+  *p_tot = sb[nwarps - 1];
+  __syncthreads();
+}
 
 // A pair scanned component-wise (used for (count, position) and (brackets,
 // productions) carries).

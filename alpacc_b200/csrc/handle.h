@@ -79,22 +79,30 @@ struct alpacc_gpu_grammar {
   bool stage_used[kStages] = {};
   double stage_ms[kStages] = {};
   // tables
-  DevBuf cls_id, trans_words, lane_of, img, img_cnt, img2, sterm, sflags;
+  DevBuf lex_tab, lex_cls4, lane_of, img, img_cnt, img2, sterm, sflags;
   DevBuf dense, rec, stacks, prods, arity, is_term;
-  int trans_word_count = 0, trans_rep = 32;
+  // lexer table shape (build_lexer_table): entries, rows of 1 << (cp_shift - 2),
+  // column swizzle mask, u16 class table when classes exceed 64
+  int tab_words = 0, cp_shift = 2, swz = 0, wide_cls = 0;
+  int lex_w4 = 0;    // machine above 64 states: 256-bit state sets in pass 1
   int lex_grid = 0;  // persistent grid of lex_kernel
+  int pair_grid = 0, pse_grid = 0;  // resident CTAs of pair_kernel / pse_tile_kernel
+  // parser-stage capacities: the largest exact needs seen (brackets, productions)
+  uint64_t need_br = 0, need_pr = 0;
   int launches = 0;  // kernel launches of the last call
   int diag = 0;
   // status
   DeviceStatus *d_status = nullptr;
   DeviceStatus *h_status = nullptr;  // pinned
+  DeviceStatus *h_lex_status = nullptr;  // pinned: the status after the lexer (host calls)
+  cudaEvent_t lex_status_ev = nullptr;
   // scratch
   DevBuf in;                                   // device copy of host input
+  DevBuf flags;                                // per-call flags, tickets, counters (zeroed each call)
   DevBuf lex_ticket, st1_flag, st1_state, st1_vec, st2_flags, st2_agg, st2_inc;
-  DevBuf stage_ids, stage_starts, stage_ends, tile_cnt, tile_pos, tile_off, tile_prev;
   DevBuf tok_ids, tok_starts, tok_lens;
   DevBuf pair_ticket, pst_flags, pst_agg, pst_inc, br, pr;
-  DevBuf pse_ticket, pse_flags, pse_agg, pse_inc, ch_h0, ch_tc, tile_min, chunk_min, super_min, queue, queue_len;
+  DevBuf pse_ticket, pse_flags, pse_agg, pse_inc, ch_h0, ch_tc, tile_min, chunk_min, super_key, queue, queue_len;
   DevBuf node_prods, node_parents, token_parents;
   // batches: descriptor arrays, per-document statuses, packing ranges, packed results
   DevBuf b_arrays, b_desc, b_status, b_pack, b_packed;
@@ -177,7 +185,8 @@ inline void release_block(alpacc_gpu_grammar *g, PinnedBlock *b, bool tree) {
   cudaFreeHost(b);
 }
 
-// Dynamic shared memory of lex_kernel for this handle's tables.
+// Dynamic shared memory of lex_kernel for this handle's tables: the class
+// table, then the entries.
 inline size_t lex_dyn_smem(const alpacc_gpu_grammar *g) {
-  return ((256 * (size_t)g->trans_rep * 2 + 15) & ~(size_t)15) + (size_t)g->trans_word_count * g->trans_rep * 4;
+  return (g->wide_cls ? 512 : 256) + (size_t)g->tab_words * 4;
 }

@@ -54,23 +54,27 @@ constexpr int kLexChunk = kLexWords * 4;
 constexpr int kLexHalo = 8;
 constexpr int kLexLoad = kLexThreads * kLexChunk;               // bytes loaded per tile
 constexpr int kLexData = (kLexThreads - kLexHalo) * kLexChunk;  // new bytes per tile
+constexpr int kLexLanes = kMaxLanes;                            // start lanes of an open chunk
 
 struct LexArgs {
   const uint8_t *in;
   unsigned long long n;
   unsigned long long num_tiles;
-  // minimised machine
-  const uint8_t *cls_id;            // [256] byte -> class
-  const uint32_t *trans_words_ptr;  // [trans_words] u8 entries (next | produce << 7) at class * M + state
-  int trans_words;
-  int copies;                       // table copies in shared memory (power of two <= 32)
-  const uint8_t *lane_of;           // [C*M]
-  const uint8_t *img;               // [C*kMaxLanes]
+  // minimised machine in the form of build_lexer_table: entries
+  // F(next) | code << 24 in rows of 1 << (cp_shift - 2), columns swizzled by
+  // (state & swz)
+  const uint32_t *tab;              // [tab_words]
+  int tab_words;
+  const uint8_t *cls4;              // byte -> class * 4: u8[256], or u16[256] when wide_cls
+  int wide_cls;
+  int cp_shift, swz;
+  const uint8_t *lane_of;           // [C*M] slot of a start state in img of a class, 0xff dead
+  const uint8_t *img;               // [C*kLexLanes]
   const uint8_t *img_cnt;           // [C]
-  const unsigned long long *img2;   // [C*C] live states after two bytes, or null
+  const unsigned long long *img2;   // [C*C] live states after two bytes (M <= 64), or null
   const uint8_t *sterm;             // [M]
   const uint8_t *sflags;            // [M] bit0 produce, bit1 accept, bit2 kept
-  int M, C, dead, m0, ignore;
+  int M, C, dead, m0;
   unsigned long long len_max;
   // outputs (native widths)
   void *tok_ids, *tok_starts, *tok_lens;
@@ -81,47 +85,21 @@ struct LexArgs {
   uint8_t *st1_state;   // [tiles]
   uint8_t *st1_vec;     // [tiles * M]
   unsigned long long tile_begin, tile_end;  // this launch's tiles (tile_end 0: all num_tiles)
-  PairTileState st2;    // (kept-token count, last boundary position)
+  PairTileState st2;    // (kept-token count, last boundary)
   DeviceStatus *status;
   int diag;             // 1: accumulate diagnostic counters in status->scratch
-  // Staged output (when stage_ids is set): tile i writes its kept tokens at
-  // i * kLexData + k with their start (0 when the start lies before the tile)
-  // and end positions, and its (count, last boundary) to tile_cnt / tile_pos;
-  // lex_scan_kernel and lex_place_kernel then place them. No tile waits for
-  // another tile's count. Without staging, the tiles chain their counts by
-  // decoupled look-back (st2) and write the final arrays directly.
-  uint8_t *stage_ids;
-  uint32_t *stage_starts, *stage_ends;
-  uint32_t *tile_cnt, *tile_pos;
   const BatchDesc *batch;  // null: one document (in, n, status); else tiles are virtual (lex_tile0)
   // One window of a longer input (chunked lexing): the input continues after
   // byte n, so the token in progress at n is neither emitted nor judged; the
-  // window's last boundary is left in status->last_boundary. Staged path only.
+  // window's last boundary is left in status->last_boundary.
   int open_end;
-};
-
-__global__ void lex_kernel(LexArgs args);
-
-struct LexPlaceArgs {
-  unsigned long long num_tiles;
-  unsigned long long tile_data;  // data bytes per tile (staging stride)
-  unsigned long long n;
-  const uint32_t *tile_cnt, *tile_pos;
-  unsigned long long *tile_off;  // exclusive prefix of tile_cnt
-  uint32_t *tile_prev;           // last boundary before each tile (0: none)
-  const uint8_t *stage_ids;
-  const uint32_t *stage_starts, *stage_ends;
-  void *tok_ids, *tok_starts, *tok_lens;
-  int term_w, idx_w, len_w;
-  unsigned long long len_max;
-  DeviceStatus *status;
-  const BatchDesc *batch;  // null: one document; else counts restart at each document's first tile
   unsigned long long index_base;  // added to every token start (a window's offset in chunked lexing)
 };
 
-constexpr int kLexScanThreads = 1024;
-__global__ void lex_scan_kernel(LexPlaceArgs args);   // one CTA
-__global__ void lex_place_kernel(LexPlaceArgs args);  // CTAs over tiles
+// Machines of at most 64 states (one 64-bit state set in pass 1), and of up
+// to 255 states (four words).
+__global__ void lex_kernel(LexArgs args);
+__global__ void lex_kernel_wide(LexArgs args);
 
 // ---- pair lookup / stack-action expansion: 256 threads x 8 positions ----
 constexpr int kPairThreads = 256;
@@ -133,7 +111,7 @@ struct PairArgs {
   const void *tok_ids;      // lexer output, terminal ids (term_w bytes each)
   int term_w;
   const unsigned long long *num_tokens;  // device: T
-  unsigned long long num_tiles;          // tiles launched (upper bound)
+  unsigned long long tiles_cap;          // pair tiles the look-back state holds (ALPACC_E_CAPACITY beyond)
   int q, k, nt;
   int empty_t, start_t, end_t;
   const uint32_t *dense;    // [nt^(q+k)] record index or 0xffffffff
@@ -169,7 +147,7 @@ struct PseArgs {
   const uint32_t *elems;            // brackets (bit 31 = left) or productions
   const unsigned long long *count;  // device: number of elements
   const unsigned long long *num_tokens;
-  unsigned long long num_tiles;
+  unsigned long long elem_cap;      // elements the walk's arrays hold (ALPACC_E_CAPACITY beyond)
   const int32_t *arity;             // parents: per production
   const uint8_t *is_term;           // parents: terminal production flags
   int num_prods;                    // entries of arity / is_term
@@ -177,7 +155,7 @@ struct PseArgs {
   int32_t *ch_min;                  // [tiles * 256] minimum depth in each chunk (INT_MAX if empty)
   int32_t *ch_tc;                   // parents: [tiles * 256] terminal productions before each chunk
   int32_t *tile_min;                // [tiles]
-  int32_t *super_min;               // [ceil(tiles / 256)] minimum over each run of 256 tiles
+  uint32_t *super_key;              // [ceil(tiles / 256)] INT_MAX - minimum over each run of 256 tiles (0: none)
   unsigned long long *queue;        // elements whose answer lies in an earlier tile
   unsigned long long queue_cap;
   unsigned long long *queue_len;    // device counter
@@ -192,6 +170,7 @@ struct PseArgs {
 
 __global__ void pse_tile_kernel(PseArgs args);
 __global__ void pse_resolve_kernel(PseArgs args);
-__global__ void narrow_u32_kernel(const uint32_t *src, void *dst, unsigned long long count, int width);
+__global__ void narrow_u32_kernel(const uint32_t *src, void *dst, const unsigned long long *count,
+                                  unsigned long long cap, int width);
 
 }  // namespace alpacc

@@ -1,33 +1,38 @@
 // Data-parallel lexer for sm_100a: the sequential semantics of lex_string
-// (backends/c/lexer.c:39-97) computed tile-parallel.
+// (backends/c/lexer.c:39-97) computed tile-parallel in one kernel.
 //
 // The lexer runs a Moore machine over byte classes that device_tables.cpp
-// derives from TO_STATE / COMPOSE / ACCEPT: a transition entry holds the next
-// state (7 bits) and that state's produce flag (bit 7), indexed by
-// class * M + state. Persistent CTAs load the tables into shared memory once
-// - the byte-class table and the transition table are replicated (`copies`
-// of each, lane l reading copy l % copies) so data-dependent lookups from one
-// warp rarely meet in a bank - and then take tiles by ticket.
+// derives from TO_STATE / COMPOSE / ACCEPT. Its transition table lives in
+// shared memory as 32-bit entries (build_lexer_table): entry(s, c) =
+// F(next) | code << 24, where F(x) is the byte offset of state x's row (rows
+// of CP >= C entries, CP a power of two, columns swizzled by the row's low
+// state bits so that threads reading one class in different states meet in
+// different banks) and code says what happens before the byte: 0xFF no token
+// boundary, 0xFE the token that ends here is ignored, else its terminal id.
+// One step of the machine is then a class lookup, one LOP3 (address =
+// (entry & 0xFFFFFF) ^ class * 4) and one shared-memory load.
 //
-// A tile is 256 chunks of 60 bytes (15 words: an odd stride, so per-thread
-// walks are bank-conflict free). The first 8 chunks are a halo - the 480
-// bytes before the tile's 14880 data bytes - walked again so that the tile
+// A tile is 256 chunks of 60 bytes (15 words: an odd word stride, so per-thread
+// rows are bank-conflict free); the first 8 chunks are a halo repeating the
+// 480 bytes before the tile's 14880 data bytes, walked again so that the tile
 // can almost always derive its incoming state by itself.
 //
-// Pass 1: every chunk computes its transition function without knowing its
-//   start state by running the machine from every live state its first byte
-//   can lead to ("lanes") and merging lanes that meet. Once one lane is left
-//   (after a few bytes) the walk costs one lookup per byte and records the
-//   token boundaries it passes: a 64-bit mask, and the state before each
-//   boundary written over the consumed byte. Such a chunk maps every live
-//   start state to one end state ("constant").
-// Resolution: a chunk's start state follows from the nearest constant chunk
+// Pass 1 (each chunk, start state unknown): the set of live states after its
+//   first bytes is walked until it is one state (typically 1-4 bytes on JSON)
+//   and word aligned; from there a fully unrolled single-lane walk writes each
+//   byte's code over the consumed input word. Such a chunk maps every live
+//   start to one end state ("constant"). A chunk whose set never shrinks to
+//   one state ("open") instead walks each of its first byte's targets on its
+//   own and keeps the end state per start lane.
+// Resolution: each chunk's start state follows from the nearest constant chunk
 //   before it; only when no halo chunk is constant does the tile read its
-//   predecessor's published outgoing state (decoupled look-back, bounded).
-// Pass 2: each data chunk re-walks only the bytes before its lanes merged,
-//   from its true start, then counts kept tokens over the recorded
-//   boundaries; a (count, last boundary) carry is scanned across the tile and
-//   across tiles by decoupled look-back; tokens are written structure-of-arrays.
+//   predecessor's published outgoing state (bounded look-back).
+// Pass 2: each data chunk re-walks the bytes before its walk converged (all of
+//   an open or partial chunk) from its true start, writing their codes.
+// Output: boundary masks from the code words, a (token count, last boundary)
+//   block scan, a decoupled look-back over tiles (Merrill & Garland 2016) taken
+//   last, and the kept tokens written straight into the final
+//   structure-of-arrays outputs with the length_t check of lexer.c:68-72.
 //
 // Reference equivalents: backends/cuda/lexer.cu:437-760 (``lexer`` kernel) and
 // backends/cuda/scan.cu:181-400 (look-back).
@@ -49,24 +54,22 @@ __device__ __forceinline__ void store_uint(void *base, unsigned long long i, int
   }
 }
 
-constexpr int kNotConverged = 255;
+enum ChunkKind : uint8_t { kEmpty = 0, kConst = 1, kOpen = 2, kPartial = 3 };
+
+constexpr uint32_t kAddrMask = 0xFFFFFFu;  // F(next) bits of an entry
+constexpr uint8_t kNoBoundary = 0xFF, kIgnored = 0xFE;
 
 struct LexSmem {
-  uint32_t bytes[kLexThreads * kLexWords];  // the tile; recorded boundary states overwrite consumed bytes
-  uint8_t lst[kMaxLanes * kLexThreads];     // lane states, slot-major
-  uint8_t lrm[kMaxLanes * kLexThreads];     // original slot -> merged slot
-  uint16_t active[kLexThreads];
-  uint8_t c0[kLexThreads];      // class id of the chunk's first byte
-  uint8_t nbytes[kLexThreads];
-  uint8_t start[kLexThreads];   // true start state of data chunks
-  uint8_t cstate[kLexThreads];  // lane state just before the recorded part
-  uint8_t exact[kLexThreads];   // 1: lanes tracked per start state (lst/lrm valid)
-  uint8_t sterm[256];           // per machine state: terminal id
-  uint8_t sflags[256];          // bit1 accept, bit2 kept
-  uint8_t cls_id[256];          // byte -> class id (first byte of a chunk)
-  long long scan_tmp[kLexThreads / 32];
-  Pair64 pair_tmp[kLexThreads / 32];
+  uint32_t bytes[kLexThreads * kLexWords];  // the tile; codes replace the consumed words
+  uint8_t lend[kLexLanes * kLexThreads];    // open chunks: end state per start lane (lane-major)
+  uint8_t kind[kLexThreads];
+  uint8_t endst[kLexThreads];  // constant chunks: end state
+  uint8_t c0[kLexThreads];     // class of the chunk's first byte
+  uint8_t start[kLexThreads];  // true start state of data chunks
+  uint8_t sterm[256];          // per machine state: terminal id
+  uint8_t sflags[256];         // bit1 accept, bit2 kept
   int kconst[kLexThreads];
+  int scan_a[kLexThreads / 32], scan_b[kLexThreads / 32];
   unsigned tile;
   int s_in;
   int need_lookback;
@@ -74,72 +77,186 @@ struct LexSmem {
   long long cnt_prefix, pos_prefix;
 };
 
-struct Tabs {
-  const uint16_t *cls;    // [256 * copies] class * M
-  const uint32_t *trans;  // [words * copies] packed u8 entries
-  int copies;
-  int lane_copy;
+// The machine in shared memory: class table and entries, plus the shape
+// parameters that turn a state into its row offset and back.
+struct Tab {
+  const uint8_t *cls;  // [256] class * 4 (u8), or [512] bytes of u16 when wide
+  const uint8_t *ent;  // entries, addressed by byte offset
+  int wide;
+  int shift;           // F(x) >> shift == x
+  uint32_t swz;        // K - 1
 };
 
-__device__ __forceinline__ uint32_t cls_pre(const Tabs &tb, uint32_t b) {
-  return tb.cls[b * (uint32_t)tb.copies + (uint32_t)tb.lane_copy];
+__device__ __forceinline__ uint32_t cls4_of(const Tab &tb, uint32_t b) {
+  return tb.wide ? (uint32_t) reinterpret_cast<const uint16_t *>(tb.cls)[b] : (uint32_t)tb.cls[b];
 }
 
-// entry of (class premultiplied cp, state s): next state | produce << 7
-__device__ __forceinline__ uint32_t entry(const Tabs &tb, uint32_t cp, uint32_t s) {
-  const uint32_t i = cp + s;
-  const uint32_t w = tb.trans[(i >> 2) * (uint32_t)tb.copies + (uint32_t)tb.lane_copy];
-  return __byte_perm(w, 0, i & 3);
+__device__ __forceinline__ uint32_t row_of(const Tab &tb, uint32_t x) { return (x << tb.shift) | ((x & tb.swz) << 2); }
+
+__device__ __forceinline__ int state_of(const Tab &tb, uint32_t f) { return (int)((f & kAddrMask) >> tb.shift); }
+
+// One machine step: the entry for (state of f, class c4 / 4).
+__device__ __forceinline__ uint32_t step(const Tab &tb, uint32_t f, uint32_t c4) {
+  return *reinterpret_cast<const uint32_t *>(tb.ent + ((f & kAddrMask) ^ c4));
 }
 
-// f_t(x): the state after chunk t when it starts in state x. A chunk walked as
-// a state set is constant: every live start ends in its one state (a start
-// whose lane died instead is caught when the chunk is re-walked from its true
-// start, which then rejects the input).
+// f_t(x): the state after chunk t when it starts in state x. A constant chunk
+// maps every live start to its one end state (a start whose lane died instead
+// is caught when the chunk is re-walked from its true start, which then
+// rejects the input); an open chunk keeps the end state of each start lane.
+// A partial chunk (the input's last) is never followed by a non-empty chunk.
 __device__ __forceinline__ int eval_chunk(const LexArgs &a, const LexSmem *sm, int t, int x) {
-  if (sm->nbytes[t] == 0) return x;
+  const int kind = sm->kind[t];
+  if (kind == kEmpty) return x;
   const int dead = a.dead;
-  if (x == dead) return dead;
-  if (!sm->exact[t]) return sm->active[t] ? sm->lst[t] : dead;
+  if (x == dead || x < 0) return dead;
+  if (kind == kConst) return sm->endst[t];
+  if (kind == kPartial) return dead;
   const int slot = __ldg(a.lane_of + (size_t)sm->c0[t] * a.M + x);
   if (slot == 0xff) return dead;
-  const int r = sm->lrm[slot * kLexThreads + t];
-  if (!((sm->active[t] >> r) & 1)) return dead;
-  return sm->lst[r * kLexThreads + t];
-}
-
-__device__ __forceinline__ int const_value(const LexArgs &a, const LexSmem *sm, int k) {
-  const uint32_t act = sm->active[k];
-  if (!act) return a.dead;
-  return sm->lst[(__ffs(act) - 1) * kLexThreads + k];
+  return sm->lend[slot * kLexThreads + t];
 }
 
 struct CntPosOp {
   __device__ Pair64 operator()(Pair64 e, Pair64 l) const { return Pair64{e.a + l.a, e.b > l.b ? e.b : l.b}; }
 };
 
-}  // namespace
+// Bytes of `w` that differ from 0: 0x80 in such a byte, 0 elsewhere (exact, no
+// borrow between bytes).
+__device__ __forceinline__ uint32_t nonzero_bytes(uint32_t w) {
+  return (((w & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | w) & 0x80808080u;
+}
 
-__global__ void __launch_bounds__(kLexThreads, 6) lex_kernel(LexArgs args) {
-  extern __shared__ __align__(16) unsigned char dyn_smem[];
-  __shared__ __align__(16) LexSmem sm_static;
-  LexSmem *sm = &sm_static;
-  const LexArgs &a = args;
+// The four 0x80 flags of nonzero_bytes as a 4-bit mask (byte i -> bit i).
+__device__ __forceinline__ uint32_t movemask4(uint32_t x) { return ((x >> 7) * 0x10204080u) >> 28; }
+
+// The set walk of pass 1 over W 64-bit words of states.
+template <int W>
+struct StateSet {
+  unsigned long long w[W];
+  __device__ __forceinline__ void clear() {
+#pragma unroll
+    for (int i = 0; i < W; i++) w[i] = 0;
+  }
+  __device__ __forceinline__ void add(int s) {
+#pragma unroll
+    for (int i = 0; i < W; i++)
+      if ((s >> 6) == i) w[i] |= 1ull << (s & 63);
+  }
+  __device__ __forceinline__ int count() const {
+    int c = 0;
+#pragma unroll
+    for (int i = 0; i < W; i++) c += __popcll(w[i]);
+    return c;
+  }
+  __device__ __forceinline__ int first() const {
+#pragma unroll
+    for (int i = 0; i < W; i++)
+      if (w[i]) return 64 * i + __ffsll((long long)w[i]) - 1;
+    return -1;
+  }
+};
+
+// Pass 1 for a full chunk: returns the chunk kind; sets *jw_out (bytes walked
+// as a set, a multiple of 4: pass 2 re-walks them), the converged state at
+// that point (or -1), and the end state (constant) or the per-lane end states
+// in lend (open).
+template <int W>
+__device__ __forceinline__ int pass1_chunk(const LexArgs &a, const Tab &tb, LexSmem *sm, int t, int *jw_out,
+                                           int *end_out, int *conv_out) {
+  uint32_t *row = sm->bytes + t * kLexWords;
+  const uint8_t *rb = reinterpret_cast<const uint8_t *>(row);
+  const int dead = a.dead;
+  const int c0 = (int)(cls4_of(tb, rb[0]) >> 2);
+  sm->c0[t] = (uint8_t)c0;
+  StateSet<W> set;
+  set.clear();
+  int j;
+  if (W == 1 && a.img2) {  // the first two bytes at once
+    set.w[0] = __ldg(a.img2 + c0 * a.C + (int)(cls4_of(tb, rb[1]) >> 2));
+    j = 2;
+  } else {
+    const int cnt = __ldg(a.img_cnt + c0);
+    for (int l = 0; l < cnt; l++) set.add(__ldg(a.img + c0 * kLexLanes + l));
+    j = 1;
+  }
+  // walk the set until it is one state and the position is word aligned
+  int live = set.count();
+  while (j < kLexChunk && (live > 1 || (j & 3))) {
+    const uint32_t c4 = cls4_of(tb, rb[j]);
+    StateSet<W> ns;
+    ns.clear();
+#pragma unroll
+    for (int i = 0; i < W; i++)
+      for (unsigned long long m = set.w[i]; m; m &= m - 1) {
+        const int s = 64 * i + __ffsll((long long)m) - 1;
+        const int nx = state_of(tb, step(tb, row_of(tb, (uint32_t)s), c4));
+        if (nx != dead) ns.add(nx);
+      }
+    set = ns;
+    live = set.count();
+    ++j;
+  }
+  *conv_out = -1;
+  if (live == 0) {  // every live start dies in this chunk
+    *jw_out = j;
+    *end_out = dead;
+    return kConst;
+  }
+  if (live > 1) {  // open: the end state of each start lane, walked on its own
+    const int cnt = __ldg(a.img_cnt + c0);
+    for (int l = 0; l < cnt; l++) {
+      uint32_t f = row_of(tb, __ldg(a.img + c0 * kLexLanes + l));
+      for (int k = 1; k < kLexChunk; k++) f = step(tb, f, cls4_of(tb, rb[k]));
+      sm->lend[l * kLexThreads + t] = (uint8_t)state_of(tb, f);
+    }
+    *jw_out = kLexChunk;
+    *end_out = -1;
+    return kOpen;
+  }
+  const int s_conv = set.first();
+  *conv_out = s_conv;
+  *jw_out = j;
+  if (j >= kLexChunk) {
+    *end_out = s_conv;
+    return kConst;
+  }
+  // the unrolled walk from the converged state: codes of words >= j / 4
+  const uint32_t fconv = row_of(tb, (uint32_t)s_conv);
+  const int jw4 = j >> 2;
+  uint32_t f = fconv;
+#pragma unroll
+  for (int w = 0; w < kLexWords; ++w) {
+    if (w == jw4) f = fconv;
+    const uint32_t word = row[w];
+    const uint32_t e0 = step(tb, f, cls4_of(tb, __byte_perm(word, 0, 0x4440)));
+    const uint32_t e1 = step(tb, e0, cls4_of(tb, __byte_perm(word, 0, 0x4441)));
+    const uint32_t e2 = step(tb, e1, cls4_of(tb, __byte_perm(word, 0, 0x4442)));
+    const uint32_t e3 = step(tb, e2, cls4_of(tb, __byte_perm(word, 0, 0x4443)));
+    f = e3;
+    if (w >= jw4) row[w] = __byte_perm(__byte_perm(e0, e1, 0x0073), __byte_perm(e2, e3, 0x0073), 0x5410);
+  }
+  *end_out = state_of(tb, f);
+  return kConst;
+}
+
+template <int W>
+__device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_smem, LexSmem *sm) {
   const int t = threadIdx.x;
   const int lane = t & 31;
-  const int copies = a.copies;
 
   // ---- tables, once per CTA ----
-  uint16_t *s_cls = reinterpret_cast<uint16_t *>(dyn_smem);
-  uint32_t *s_trans = reinterpret_cast<uint32_t *>(dyn_smem + ((256 * copies * 2 + 15) & ~15));
-  for (int i = t; i < 256 * copies; i += kLexThreads) s_cls[i] = (uint16_t)(__ldg(a.cls_id + i / copies) * a.M);
-  for (int i = t; i < a.trans_words * copies; i += kLexThreads) s_trans[i] = __ldg(a.trans_words_ptr + i / copies);
+  const int cls_bytes = a.wide_cls ? 512 : 256;
+  uint8_t *s_cls = dyn_smem;
+  uint8_t *s_ent = dyn_smem + cls_bytes;
+  for (int i = t; i < cls_bytes / 4; i += kLexThreads)
+    reinterpret_cast<uint32_t *>(s_cls)[i] = __ldg(reinterpret_cast<const uint32_t *>(a.cls4) + i);
+  for (int i = t; i < a.tab_words; i += kLexThreads) reinterpret_cast<uint32_t *>(s_ent)[i] = __ldg(a.tab + i);
   for (int i = t; i < 256; i += kLexThreads) {
     sm->sterm[i] = i < a.M ? __ldg(a.sterm + i) : 0;
     sm->sflags[i] = i < a.M ? __ldg(a.sflags + i) : 0;
-    sm->cls_id[i] = __ldg(a.cls_id + i);
   }
-  const Tabs tb{s_cls, s_trans, copies, lane & (copies - 1)};
+  const Tab tb{s_cls, s_ent, a.wide_cls, a.cp_shift, (uint32_t)a.swz};
   const int dead = a.dead;
   const unsigned long long num_tiles = a.num_tiles;
   const unsigned long long tile_end = a.tile_end ? a.tile_end : num_tiles;
@@ -158,7 +275,7 @@ __global__ void __launch_bounds__(kLexThreads, 6) lex_kernel(LexArgs args) {
     // (virtual tile `tile` is local tile `lt` of `tiles_t`)
     const uint8_t *in_base = a.in;
     long long n = (long long)a.n;
-    unsigned long long lt = tile, tiles_t = num_tiles;
+    unsigned long long lt = tile, tiles_t = num_tiles, tok_base = 0;
     DeviceStatus *st = a.status;
     if (a.batch) {
       const BatchDesc &b = *a.batch;
@@ -168,6 +285,7 @@ __global__ void __launch_bounds__(kLexThreads, 6) lex_kernel(LexArgs args) {
       in_base = a.in + b.in_off[d];
       n = (long long)b.n[d];
       st = b.status + d;
+      tok_base = b.tok_off[d];  // the document's token region
     }
     const long long data0 = (long long)lt * kLexData;
     const long long load0 = data0 - (long long)kLexHalo * kLexChunk;
@@ -182,135 +300,46 @@ __global__ void __launch_bounds__(kLexThreads, 6) lex_kernel(LexArgs args) {
         if (aligned && g >= 0 && g + 16 <= n) {
           reinterpret_cast<uint4 *>(dst)[v] = __ldg(reinterpret_cast<const uint4 *>(in + g));
         } else {
-          for (int k = 0; k < 16; ++k) {
-            const long long p = g + k;
-            dst[16 * v + k] = (p >= 0 && p < n) ? in[p] : 0;
+          uint32_t wv[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            uint32_t x = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const long long p = g + 4 * q + k;
+              if (p >= 0 && p < n) x |= (uint32_t)in[p] << (8 * k);
+            }
+            wv[q] = x;
           }
+          reinterpret_cast<uint4 *>(dst)[v] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
         }
       }
     }
     const long long g0 = load0 + (long long)t * kLexChunk;
     int nb = 0;
     if (g0 >= 0 && g0 < n) nb = (int)min((long long)kLexChunk, n - g0);
-    sm->nbytes[t] = (uint8_t)nb;
     __syncthreads();
 
-    // ---- pass 1: the set of live states until it is a single state, then
-    // one lane recording boundaries ----
-    // The set walk (machines of at most 64 states) costs one lookup per live
-    // state per byte and merges equal states for free; it gives no per-start
-    // mapping, so a chunk whose set never shrinks to one state is walked again
-    // with lanes tracked per start state (slots in lst/lrm).
-    uint8_t *tb8 = reinterpret_cast<uint8_t *>(sm->bytes) + t * kLexChunk;
-    uint32_t active = 0;
-    unsigned long long bmask = 0;
-    int jconv = kNotConverged;
-    {
-      int c0 = 0;
-      bool exact = a.M > 64;
-      if (nb > 0) {
-        c0 = sm->cls_id[tb8[0]];
-        const int cnt = __ldg(a.img_cnt + c0);
-        int lconv = -1;
-        uint32_t s = 0;
-        int j = 1;
-        if (!exact) {
-          const unsigned long long live = dead >= 0 ? ~(1ull << dead) : ~0ull;
-          unsigned long long set = 0;
-          if (a.img2 && nb >= 2) {  // the first two bytes at once
-            set = __ldg(a.img2 + c0 * a.C + sm->cls_id[tb8[1]]);
-            j = 2;
-          } else {
-            for (int l = 0; l < cnt; l++) set |= 1ull << __ldg(a.img + c0 * kMaxLanes + l);
-          }
-          while (j < nb && __popcll(set) > 1) {
-            const uint32_t cp = cls_pre(tb, tb8[j]);
-            unsigned long long ns = 0;
-            for (unsigned long long m = set; m; m &= m - 1)
-              ns |= 1ull << (entry(tb, cp, (uint32_t)(__ffsll((long long)m) - 1)) & 0x7f);
-            set = ns & live;
-            ++j;
-          }
-          if (__popcll(set) > 1) {
-            exact = true;
-          } else if (set) {
-            lconv = 0;
-            s = (uint32_t)(__ffsll((long long)set) - 1);
-            active = 1;
-          }  // else every lane died: active = 0, not converged
-        }
-        if (exact) {
-          active = cnt ? ((1u << cnt) - 1u) : 0u;
-          for (int l = 0; l < cnt; l++) {
-            sm->lst[l * kLexThreads + t] = __ldg(a.img + c0 * kMaxLanes + l);
-            sm->lrm[l * kLexThreads + t] = (uint8_t)l;
-          }
-          j = 1;
-          while (j < nb && __popc(active) > 1) {
-            const uint32_t cp = cls_pre(tb, tb8[j]);
-            for (uint32_t m = active; m; m &= m - 1) {
-              const int l = __ffs(m) - 1;
-              const int s2 = (int)(entry(tb, cp, sm->lst[l * kLexThreads + t]) & 0x7f);
-              if (s2 == dead) active &= ~(1u << l);
-              else sm->lst[l * kLexThreads + t] = (uint8_t)s2;
-            }
-            if (__popc(active) > 1) {
-              for (uint32_t m1 = active; m1; m1 &= m1 - 1) {
-                const int l1 = __ffs(m1) - 1;
-                if (!((active >> l1) & 1)) continue;
-                const int s1 = sm->lst[l1 * kLexThreads + t];
-                for (uint32_t m2 = active & ~((2u << l1) - 1u); m2; m2 &= m2 - 1) {
-                  const int l2 = __ffs(m2) - 1;
-                  if (sm->lst[l2 * kLexThreads + t] == s1) {
-                    active &= ~(1u << l2);
-                    for (int k = 0; k < cnt; k++)
-                      if (sm->lrm[k * kLexThreads + t] == l2) sm->lrm[k * kLexThreads + t] = (uint8_t)l1;
-                  }
-                }
-              }
-            }
-            ++j;
-          }
-          if (__popc(active) == 1) {
-            lconv = __ffs(active) - 1;
-            s = sm->lst[lconv * kLexThreads + t];
-          }
-        }
-        if (lconv >= 0) {
-          jconv = j;
-          sm->cstate[t] = (uint8_t)s;
-          // the hot loop: one class lookup and one transition per byte. The
-          // dead state is absorbing and never produces, so a lane that dies
-          // records nothing further and needs no test inside the loop.
-#pragma unroll 4
-          for (; j < nb; ++j) {
-            const uint32_t e = entry(tb, cls_pre(tb, tb8[j]), s);
-            if (e & 0x80) {
-              bmask |= 1ull << j;
-              tb8[j] = (uint8_t)s;  // state of the token ending before byte j
-            }
-            s = e & 0x7f;
-          }
-          if ((int)s == dead) active = 0;
-          else sm->lst[lconv * kLexThreads + t] = (uint8_t)s;
-        }
-      }
-      sm->active[t] = (uint16_t)active;
-      sm->c0[t] = (uint8_t)c0;
-      sm->exact[t] = exact ? 1 : 0;
-      if (a.diag) {
-        const unsigned w = __reduce_add_sync(0xffffffffu, (unsigned)(jconv == kNotConverged ? nb : jconv));
-        if (lane == 0) atomicAdd(&st->scratch[3], (unsigned long long)w);
-      }
+    // ---- pass 1 ----
+    int jw = nb, end = -1, conv = -1, kind = kEmpty;
+    if (nb == kLexChunk) {
+      kind = pass1_chunk<W>(a, tb, sm, t, &jw, &end, &conv);
+    } else if (nb > 0) {
+      kind = kPartial;  // the input's last chunk: walked whole in pass 2
+    }
+    sm->kind[t] = (uint8_t)kind;
+    sm->endst[t] = (uint8_t)(end < 0 ? 0 : end);
+    if (a.diag) {
+      const unsigned w = __reduce_add_sync(0xffffffffu, (unsigned)(kind == kConst ? jw : nb));
+      if (lane == 0) atomicAdd(&st->scratch[3], (unsigned long long)w);
     }
     __syncthreads();
 
     // ---- resolution: nearest constant chunk before each chunk ----
-    const bool is_const = nb > 0 && __popc(active) <= 1;
-    long long ktot;
-    const long long kex = block_exclusive_scan<long long>(is_const ? (long long)t : -1ll, MaxI64(), -1ll,
-                                                          sm->scan_tmp, &ktot);
-    sm->kconst[t] = (int)kex;
+    const bool is_const = kind == kConst;
+    int ktot;
+    const int kex = block_exclusive_scan<int>(is_const ? t : -1, MaxI32(), -1, sm->scan_a, &ktot);
+    sm->kconst[t] = kex;
     if (t == kLexHalo) sm->need_lookback = kex < 0 ? 1 : 0;
     if (t == 0) sm->out_published = 0;
     if (a.diag) {
@@ -321,8 +350,8 @@ __global__ void __launch_bounds__(kLexThreads, 6) lex_kernel(LexArgs args) {
     if (ktot >= 0) {
       // the outgoing state does not depend on the incoming one: publish now
       if (t == 0) {
-        int x = const_value(a, sm, (int)ktot);
-        for (int jj = (int)ktot + 1; jj < kLexThreads; ++jj) x = eval_chunk(a, sm, jj, x);
+        int x = sm->endst[ktot];
+        for (int jj = ktot + 1; jj < kLexThreads; ++jj) x = eval_chunk(a, sm, jj, x);
         a.st1_state[tile] = (uint8_t)(x < 0 ? 0 : x);
         __threadfence();
         st_release_u32(a.st1_flag + tile, 2u);
@@ -379,7 +408,7 @@ __global__ void __launch_bounds__(kLexThreads, 6) lex_kernel(LexArgs args) {
       const int k = sm->kconst[t];
       int x, from;
       if (k >= 0) {
-        x = const_value(a, sm, k);
+        x = sm->endst[k];
         from = k + 1;
       } else {
         x = sm->s_in;
@@ -401,76 +430,55 @@ __global__ void __launch_bounds__(kLexThreads, 6) lex_kernel(LexArgs args) {
       st_release_u32(a.st1_flag + tile, 2u);
     }
 
-    // ---- pass 2a: re-walk the pre-merge bytes from the true start ----
+    // ---- pass 2: the bytes walked as a set (all of an open or partial
+    // chunk) again from the true start, writing their codes ----
     long long cnt = 0, lastb = 0;
-    bool final_tok = false, final_kept = false;
-    int final_term = 0;
+    unsigned long long bmask = 0;
+    bool final_kept = false;
+    int x_end = 0;
+    uint32_t *row = sm->bytes + t * kLexWords;
+    uint8_t *rb = reinterpret_cast<uint8_t *>(row);
     if (t >= kLexHalo && nb > 0) {
-      int x = sm->start[t];
-      bool died = (x == dead);
-      const int jc = jconv == kNotConverged ? nb : jconv;
-      for (int j = 0; j < jc && !died; ++j) {
-        const uint32_t e = entry(tb, cls_pre(tb, tb8[j]), (uint32_t)x);
-        if (g0 + j >= 1 && (e & 0x80)) {
-          bmask |= 1ull << j;
-          tb8[j] = (uint8_t)x;
+      const int x0 = sm->start[t];
+      bool died = x0 == dead;
+      uint32_t f = row_of(tb, (uint32_t)(x0 < 0 ? 0 : x0));
+      if (!died) {
+        for (int j = 0; j < jw; ++j) {
+          const uint32_t e = step(tb, f, cls4_of(tb, rb[j]));
+          rb[j] = (g0 + j >= 1) ? (uint8_t)(e >> 24) : kNoBoundary;
+          f = e;
         }
-        x = (int)(e & 0x7f);
-        if (x == dead) died = true;
+        died = state_of(tb, f) == dead;
       }
-      if (!died && jconv != kNotConverged) {
-        if (x != sm->cstate[t]) atomicCAS(&st->error, 0, -1 /* lanes disagree: internal error */);
-        if (!active) died = true;  // the merged lane died further on
-        else x = sm->lst[(__ffs(active) - 1) * kLexThreads + t];
+      if (kind == kConst) {
+        // the walk from the true start must meet the converged lane
+        if (!died && conv >= 0 && state_of(tb, f) != conv) atomicCAS(&st->error, 0, -1 /* internal error */);
+        x_end = died ? dead : end;
+      } else {
+        x_end = died ? dead : state_of(tb, f);
       }
-      if (died) record_reject(st, &st->lex_reject_reason, 1);
-      for (unsigned long long m = bmask; m; m &= m - 1) {
-        const int j = __ffsll((long long)m) - 1;
-        if (sm->sflags[tb8[j]] & 4) ++cnt;
+      if (x_end == dead) record_reject(st, &st->lex_reject_reason, 1);
+      // ---- boundaries (all) and kept-token count from the code words ----
+#pragma unroll
+      for (int w = 0; w < kLexWords; ++w) {
+        const uint32_t cw = row[w];
+        bmask |= (unsigned long long)movemask4(nonzero_bytes(~cw)) << (4 * w);
+        // kept: code < 0xFE, i.e. (code | 1) != 0xFF; bytes past nb do not count
+        const uint32_t kb = nonzero_bytes(~(cw | 0x01010101u));
+        if (4 * w + 4 <= nb) cnt += __popc(kb);
+        else if (4 * w < nb) cnt += __popc(kb & (0xFFFFFFFFu >> (8 * (4 * w + 4 - nb))));
       }
+      if (nb < 64) bmask &= (1ull << nb) - 1;
       if (bmask) lastb = g0 + 63 - __clzll((long long)bmask);
       if (g0 + nb == n && !a.open_end) {  // this chunk holds the last byte of the input
-        final_tok = true;
-        final_term = sm->sterm[x];
-        final_kept = (sm->sflags[x] & 4) != 0;
+        final_kept = x_end != dead && (sm->sflags[x_end] & 4) != 0;
         if (final_kept) ++cnt;
-        if (!(sm->sflags[x] & 2) || died) record_reject(st, &st->lex_reject_reason, 2);
+        if (x_end == dead || !(sm->sflags[x_end] & 2)) record_reject(st, &st->lex_reject_reason, 2);
       }
     }
-    // ---- (count, last boundary) carry ----
-    Pair64 cp_tot;
-    const Pair64 cp_ex = block_exclusive_scan_pair(Pair64{cnt, lastb}, CntPosOp(), Pair64{0, 0}, sm->pair_tmp, &cp_tot);
-    const long long cnt_ex = cp_ex.a, pos_ex = cp_ex.b;
-    const long long cnt_tot = cp_tot.a, pos_tot = cp_tot.b;
-    if (a.stage_ids) {
-      // ---- staged: tile-local offsets, no wait on other tiles ----
-      if (t == 0) {
-        a.tile_cnt[tile] = (uint32_t)cnt_tot;
-        a.tile_pos[tile] = (uint32_t)pos_tot;
-      }
-      if (t >= kLexHalo && nb > 0) {
-        unsigned long long out = tile * (unsigned long long)kLexData + (unsigned long long)cnt_ex;
-        long long tok_start = pos_ex;  // 0: the token starts before this tile
-        for (unsigned long long m = bmask; m; m &= m - 1) {
-          const int j = __ffsll((long long)m) - 1;
-          const long long p = g0 + j;
-          const int s = tb8[j];
-          if (sm->sflags[s] & 4) {
-            a.stage_ids[out] = sm->sterm[s];
-            a.stage_starts[out] = (uint32_t)tok_start;
-            a.stage_ends[out] = (uint32_t)p;
-            ++out;
-          }
-          tok_start = p;
-        }
-        if (final_tok && final_kept) {
-          a.stage_ids[out] = (uint8_t)final_term;
-          a.stage_starts[out] = (uint32_t)tok_start;
-          a.stage_ends[out] = (uint32_t)n;
-        }
-      }
-      continue;
-    }
+    // ---- (count, last boundary) carry: block scan, then across tiles ----
+    int cnt_tot, pos_tot, cnt_ex, pos_ex;
+    block_exclusive_scan2(sm->scan_a, sm->scan_b, (int)cnt, (int)lastb, &cnt_ex, &pos_ex, &cnt_tot, &pos_tot);
     if (t < kWarp) {
       const Pair64 agg{cnt_tot, pos_tot};
       Pair64 prefix{0, 0};
@@ -483,36 +491,40 @@ __global__ void __launch_bounds__(kLexThreads, 6) lex_kernel(LexArgs args) {
         publish_pair(a.st2, (long long)tile, inc, true);
         sm->cnt_prefix = prefix.a;
         sm->pos_prefix = prefix.b;
-        if (lt + 1 == tiles_t) st->num_tokens = (unsigned long long)inc.a;
+        if (lt + 1 == tiles_t) {
+          st->num_tokens = (unsigned long long)inc.a;
+          st->last_boundary = (unsigned long long)inc.b;
+        }
       }
     }
     __syncthreads();
 
-    // ---- pass 2b: write this chunk's kept tokens ----
+    // ---- the kept tokens, straight into the outputs ----
     if (t >= kLexHalo && nb > 0) {
-      unsigned long long out = (unsigned long long)(sm->cnt_prefix + cnt_ex);
-      long long tok_start = sm->pos_prefix > pos_ex ? sm->pos_prefix : pos_ex;
+      unsigned long long out = tok_base + (unsigned long long)(sm->cnt_prefix + cnt_ex);
+      long long prev = sm->pos_prefix > pos_ex ? sm->pos_prefix : pos_ex;  // 0: the token starts at byte 0
       const unsigned long long len_max = a.len_max;
+      const unsigned long long base = a.index_base;
       bool too_long = false;
       for (unsigned long long m = bmask; m; m &= m - 1) {
         const int j = __ffsll((long long)m) - 1;
         const long long p = g0 + j;
-        const int s = tb8[j];
-        if (sm->sflags[s] & 4) {
-          const unsigned long long len = (unsigned long long)(p - tok_start);
-          if (len > len_max) too_long = true;
-          store_uint(a.tok_ids, out, a.term_w, (unsigned long long)sm->sterm[s]);
-          store_uint(a.tok_starts, out, a.idx_w, (unsigned long long)tok_start);
+        const uint32_t code = rb[j];
+        if (code < kIgnored) {
+          const unsigned long long len = (unsigned long long)(p - prev);
+          too_long |= len > len_max;
+          store_uint(a.tok_ids, out, a.term_w, code);
+          store_uint(a.tok_starts, out, a.idx_w, base + (unsigned long long)prev);
           store_uint(a.tok_lens, out, a.len_w, len);
           ++out;
         }
-        tok_start = p;
+        prev = p;
       }
-      if (final_tok && final_kept) {
-        const unsigned long long len = (unsigned long long)(n - tok_start);
-        if (len > len_max) too_long = true;
-        store_uint(a.tok_ids, out, a.term_w, (unsigned long long)final_term);
-        store_uint(a.tok_starts, out, a.idx_w, (unsigned long long)tok_start);
+      if (final_kept) {
+        const unsigned long long len = (unsigned long long)(n - prev);
+        too_long |= len > len_max;
+        store_uint(a.tok_ids, out, a.term_w, sm->sterm[x_end]);
+        store_uint(a.tok_starts, out, a.idx_w, base + (unsigned long long)prev);
         store_uint(a.tok_lens, out, a.len_w, len);
       }
       if (too_long) record_reject(st, &st->lex_reject_reason, 3);
@@ -520,100 +532,18 @@ __global__ void __launch_bounds__(kLexThreads, 6) lex_kernel(LexArgs args) {
   }
 }
 
-// ---------------------------------------------------------------------------
-// Placement of staged tokens
-// ---------------------------------------------------------------------------
+}  // namespace
 
-// Exclusive (count, last boundary) prefix over the tiles, by one CTA; also the
-// total token count. In a batch the prefix restarts at each document's first
-// tile (a segmented scan: the flag bit kSeg marks a segment start) and the
-// offsets are placed in the document's token region.
-constexpr long long kSeg = 1ll << 62;
-
-struct SegCntPosOp {
-  __device__ Pair64 operator()(Pair64 l, Pair64 r) const {
-    if (r.b & kSeg) return r;
-    const long long lp = l.b & ~kSeg;
-    return Pair64{l.a + r.a, (lp > r.b ? lp : r.b) | (l.b & kSeg)};
-  }
-};
-
-__global__ void __launch_bounds__(kLexScanThreads) lex_scan_kernel(LexPlaceArgs a) {
-  __shared__ Pair64 tmp[kLexScanThreads / 32];
-  const int t = threadIdx.x;
-  constexpr int kPer = 16;
-  const BatchDesc *bd = a.batch;
-  // segment start of tile i (a batch document's first tile) and its document
-  auto seg_doc = [&](unsigned long long i, bool *start) -> int {
-    if (!bd) {
-      *start = i == 0;
-      return 0;
-    }
-    const int d = batch_doc(bd->lex_tile0, bd->docs, i);
-    *start = bd->lex_tile0[d] == i;
-    return d;
-  };
-  Pair64 carry{0, 0};
-  for (unsigned long long base = 0; base < a.num_tiles; base += (unsigned long long)kLexScanThreads * kPer) {
-    const unsigned long long i0 = base + (unsigned long long)t * kPer;
-    Pair64 loc{0, 0};
-    for (int k = 0; k < kPer && i0 + k < a.num_tiles; ++k) {
-      bool start;
-      seg_doc(i0 + k, &start);
-      const Pair64 v{(long long)a.tile_cnt[i0 + k], (long long)a.tile_pos[i0 + k] | (start ? kSeg : 0)};
-      loc = SegCntPosOp()(loc, v);
-    }
-    Pair64 tot;
-    const Pair64 ex = block_exclusive_scan_pair(loc, SegCntPosOp(), Pair64{0, 0}, tmp, &tot);
-    Pair64 run = SegCntPosOp()(carry, ex);
-    for (int k = 0; k < kPer && i0 + k < a.num_tiles; ++k) {
-      bool start;
-      const int d = seg_doc(i0 + k, &start);
-      if (start) run = Pair64{0, 0};
-      const unsigned long long region = bd ? bd->tok_off[d] : 0;
-      a.tile_off[i0 + k] = region + (unsigned long long)run.a;
-      a.tile_prev[i0 + k] = (uint32_t)(run.b & ~kSeg);
-      run = Pair64{run.a + (long long)a.tile_cnt[i0 + k],
-                   ((run.b & ~kSeg) > (long long)a.tile_pos[i0 + k] ? (run.b & ~kSeg) : (long long)a.tile_pos[i0 + k])};
-      // the document's token count, at its last tile
-      if (bd && i0 + k + 1 == bd->lex_tile0[d + 1]) bd->status[d].num_tokens = (unsigned long long)run.a;
-    }
-    carry = SegCntPosOp()(carry, tot);
-  }
-  if (t == 0 && !bd) {
-    a.status->num_tokens = (unsigned long long)(carry.a);
-    a.status->last_boundary = (unsigned long long)(carry.b & ~kSeg);
-  }
+__global__ void __launch_bounds__(kLexThreads, 5) lex_kernel(LexArgs args) {
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  __shared__ __align__(16) LexSmem sm;
+  lex_body<1>(args, dyn_smem, &sm);
 }
 
-// Each CTA copies whole tiles' staged tokens to their final places; a token
-// whose start lies before its tile takes the last boundary before the tile.
-__global__ void __launch_bounds__(256) lex_place_kernel(LexPlaceArgs a) {
-  bool too_long = false;
-  DeviceStatus *st = a.status;
-  for (unsigned long long tile = blockIdx.x; tile < a.num_tiles; tile += gridDim.x) {
-    DeviceStatus *sd = a.batch ? a.batch->status + batch_doc(a.batch->lex_tile0, a.batch->docs, tile) : a.status;
-    if (sd != st) {
-      if (too_long) record_reject(st, &st->lex_reject_reason, 3);
-      too_long = false;
-      st = sd;
-    }
-    const unsigned c = a.tile_cnt[tile];
-    const unsigned long long off = a.tile_off[tile];
-    const uint32_t prev = a.tile_prev[tile];
-    const unsigned long long base = tile * (unsigned long long)a.tile_data;
-    for (unsigned i = threadIdx.x; i < c; i += blockDim.x) {
-      const uint32_t s0 = a.stage_starts[base + i];
-      const uint32_t start = s0 > prev ? s0 : prev;
-      const uint32_t end = a.stage_ends[base + i];
-      const unsigned long long len = end - start;
-      if (len > a.len_max) too_long = true;
-      store_uint(a.tok_ids, off + i, a.term_w, a.stage_ids[base + i]);
-      store_uint(a.tok_starts, off + i, a.idx_w, a.index_base + start);
-      store_uint(a.tok_lens, off + i, a.len_w, len);
-    }
-  }
-  if (too_long) record_reject(st, &st->lex_reject_reason, 3);
+__global__ void __launch_bounds__(kLexThreads, 5) lex_kernel_wide(LexArgs args) {
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  __shared__ __align__(16) LexSmem sm;
+  lex_body<4>(args, dyn_smem, &sm);
 }
 
 }  // namespace alpacc

@@ -32,6 +32,7 @@
 #include "../../include/alpacc_b200.h"
 #include "handle.h"
 #include "kernels.h"
+#include "pipeline.h"
 
 using namespace alpacc;
 
@@ -129,31 +130,10 @@ int lex_noalloc_on_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n
     cudaGetLastError();
     return ALPACC_E_CUDA;
   }
-  LexArgs a{};
-  a.in = d_in;
-  a.n = n;
-  a.num_tiles = tiles;
-  a.cls_id = (const uint8_t *)g->cls_id.p;
-  a.trans_words_ptr = (const uint32_t *)g->trans_words.p;
-  a.trans_words = g->trans_word_count;
-  a.copies = g->trans_rep;
-  a.lane_of = (const uint8_t *)g->lane_of.p;
-  a.img = (const uint8_t *)g->img.p;
-  a.img_cnt = (const uint8_t *)g->img_cnt.p;
-  a.sterm = (const uint8_t *)g->sterm.p;
-  a.sflags = (const uint8_t *)g->sflags.p;
-  a.M = lm.M;
-  a.C = lm.C;
-  a.dead = lm.dead;
-  a.m0 = lm.m0;
-  a.ignore = hg.ignore;
-  a.len_max = hg.len_max;
+  LexArgs a = lex_args(g, d_in, n, tiles);  // the handle's tables; working memory and outputs below
   a.tok_ids = d_token_ids;
   a.tok_starts = d_token_starts;
   a.tok_lens = d_token_lengths;
-  a.term_w = (int)hg.t.terminal_size;
-  a.idx_w = (int)hg.t.index_size;
-  a.len_w = (int)hg.t.length_size;
   a.ticket = reinterpret_cast<unsigned *>(base + kOffTicket);
   a.st1_flag = reinterpret_cast<unsigned *>(base + kOffSt1Flag);
   a.st1_state = base + kOffSt1State;
@@ -164,8 +144,7 @@ int lex_noalloc_on_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n
   a.status = status;
   a.diag = 0;
   const unsigned grid = (unsigned)(tiles < (unsigned long long)g->lex_grid ? tiles : (unsigned long long)g->lex_grid);
-  lex_kernel<<<grid, kLexThreads, lex_dyn_smem(g), g->stream>>>(a);
-  if (cudaGetLastError() != cudaSuccess) return ALPACC_E_CUDA;
+  if (launch_lex(g, a, grid, g->stream) != cudaSuccess) return ALPACC_E_CUDA;
   DeviceStatus h;
   if (cudaMemcpyAsync(&h, status, sizeof h, cudaMemcpyDeviceToHost, g->stream) != cudaSuccess ||
       cudaStreamSynchronize(g->stream) != cudaSuccess) {

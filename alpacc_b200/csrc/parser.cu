@@ -69,12 +69,24 @@ __global__ void __launch_bounds__(kPairThreads, 5) pair_kernel(PairArgs a) {
   __shared__ __align__(16) uint32_t s_out[kPairOut];     // output window
   const int t = threadIdx.x;
   const int L = a.q + a.k;
+  unsigned long long total;
+  if (a.batch) {
+    total = a.batch->pair_tile0[a.batch->docs];
+  } else {
+    // the lexer rejected: nothing to expand (one read, shared by the CTA:
+    // this kernel's own rejects may land meanwhile)
+    if (__syncthreads_or(t == 0 && *reinterpret_cast<volatile int *>(&a.status->reject) != 0)) return;
+    total = (*a.num_tokens + 2 + kPairTile - 1) / kPairTile;
+    if (total > a.tiles_cap) {
+      if (t == 0 && blockIdx.x == 0) atomicCAS(&a.status->error, 0, -4 /* ALPACC_E_CAPACITY */);
+      return;
+    }
+  }
   for (;;) {
   __syncthreads();  // the previous tile's shared data is consumed
   if (t == 0) s_tile = atomicAdd(a.ticket, 1u);
   __syncthreads();
   const unsigned long long tile = s_tile;  // virtual tile in a batch
-  const unsigned long long total = a.batch ? a.batch->pair_tile0[a.batch->docs] : a.num_tiles;
   if (tile >= total) break;
   // this tile's document
   unsigned long long lt = tile;
@@ -311,8 +323,19 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
       s_arity[i] = __ldg(a.arity + i);
       s_is_term[i] = __ldg(a.is_term + i);
     }
-  const unsigned long long total =
-      !a.batch ? a.num_tiles : (parents ? a.batch->pr_tile0 : a.batch->br_tile0)[a.batch->docs];
+  unsigned long long total;
+  if (a.batch) {
+    total = (parents ? a.batch->pr_tile0 : a.batch->br_tile0)[a.batch->docs];
+  } else {
+    // already rejected: nothing to find (one read, shared by the CTA)
+    if (__syncthreads_or(t == 0 && *reinterpret_cast<volatile int *>(&a.status->reject) != 0)) return;
+    const unsigned long long E = *a.count;
+    if (E > a.elem_cap) {
+      if (t == 0 && blockIdx.x == 0) atomicCAS(&a.status->error, 0, -4 /* ALPACC_E_CAPACITY */);
+      return;
+    }
+    total = (E + kPseTile - 1) / kPseTile;
+  }
   for (;;) {
   __syncthreads();  // the previous tile's shared data is consumed
   if (t == 0) s_tile = atomicAdd(a.ticket, 1u);
@@ -543,7 +566,7 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
     for (int w = 1; w < kPseWarps; ++w) r = sm.wmin[w] < r ? sm.wmin[w] : r;
     const int32_t tm = r + off;  // the tile holds at least one element
     a.tile_min[tile] = tm;
-    atomicMin(a.super_min + (tile >> kPseSuperShift), tm);
+    atomicMax(a.super_key + (tile >> kPseSuperShift), (uint32_t)((long long)INT_MAX - (long long)tm));
   }
   if (parents) {
 #pragma unroll
@@ -571,6 +594,18 @@ __device__ __forceinline__ long long warp_latest_le(const int32_t *arr, long lon
   for (long long base = hi; base >= lo; base -= 32) {
     const long long idx = base - lane;
     const int32_t v = idx >= lo ? arr[idx] : INT_MAX;
+    const unsigned b = __ballot_sync(0xffffffffu, v <= qv);
+    if (b) return base - (__ffs(b) - 1);
+  }
+  return -1;
+}
+
+// The same over super-tile keys (INT_MAX - minimum; 0: no tile).
+__device__ __forceinline__ long long warp_latest_le_key(const uint32_t *keys, long long hi, long long lo, int32_t qv,
+                                                        int lane) {
+  for (long long base = hi; base >= lo; base -= 32) {
+    const long long idx = base - lane;
+    const long long v = idx >= lo ? (long long)INT_MAX - (long long)keys[idx] : (long long)INT_MAX;
     const unsigned b = __ballot_sync(0xffffffffu, v <= qv);
     if (b) return base - (__ffs(b) - 1);
   }
@@ -611,6 +646,8 @@ __device__ __forceinline__ long long terminal_count(const PseArgs &a, const PseD
 // latest chunk of that tile, then the latest element of that chunk (depths
 // recomputed from the chunk's start depth).
 __global__ void pse_resolve_kernel(PseArgs a) {
+  // the walk did not complete (no kernel sets an error word while this one runs)
+  if (!a.batch && *reinterpret_cast<volatile int *>(&a.status->error)) return;
   const unsigned long long qn = *a.queue_len;
   const bool parents = a.mode == kPseParents;
   const int lane = threadIdx.x & 31;
@@ -640,7 +677,8 @@ __global__ void pse_resolve_kernel(PseArgs a) {
     const long long sup0 = (tile >> kPseSuperShift) << kPseSuperShift;
     long long tt = warp_latest_le(a.tile_min, tile - 1, sup0 > first ? sup0 : first, qv, lane);
     if (tt < 0 && sup0 > first) {
-      const long long sp = warp_latest_le(a.super_min, (sup0 >> kPseSuperShift) - 1, first >> kPseSuperShift, qv, lane);
+      const long long sp =
+          warp_latest_le_key(a.super_key, (sup0 >> kPseSuperShift) - 1, first >> kPseSuperShift, qv, lane);
       if (sp >= 0) {
         const long long lo = sp << kPseSuperShift;
         tt = warp_latest_le(a.tile_min, ((sp + 1) << kPseSuperShift) - 1, lo > first ? lo : first, qv, lane);
@@ -700,7 +738,9 @@ __global__ void __launch_bounds__(1024) batch_plan_kernel(BatchDesc b, int kind,
 // consecutive ids per step.
 // ---------------------------------------------------------------------------
 
-__global__ void narrow_u32_kernel(const uint32_t *src, void *dst, unsigned long long count, int width) {
+__global__ void narrow_u32_kernel(const uint32_t *src, void *dst, const unsigned long long *count_p,
+                                  unsigned long long cap, int width) {
+  const unsigned long long count = *count_p < cap ? *count_p : cap;
   const unsigned long long quads = (count + 3) / 4;
   for (unsigned long long q = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; q < quads;
        q += (unsigned long long)gridDim.x * blockDim.x) {

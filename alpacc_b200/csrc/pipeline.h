@@ -18,10 +18,12 @@ inline LexArgs lex_args(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, 
   a.in = d_in;
   a.n = n;
   a.num_tiles = tiles;
-  a.cls_id = (const uint8_t *)g->cls_id.p;
-  a.trans_words_ptr = (const uint32_t *)g->trans_words.p;
-  a.trans_words = g->trans_word_count;
-  a.copies = g->trans_rep;
+  a.tab = (const uint32_t *)g->lex_tab.p;
+  a.tab_words = g->tab_words;
+  a.cls4 = (const uint8_t *)g->lex_cls4.p;
+  a.wide_cls = g->wide_cls;
+  a.cp_shift = g->cp_shift;
+  a.swz = g->swz;
   a.lane_of = (const uint8_t *)g->lane_of.p;
   a.img = (const uint8_t *)g->img.p;
   a.img_cnt = (const uint8_t *)g->img_cnt.p;
@@ -32,7 +34,6 @@ inline LexArgs lex_args(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, 
   a.C = lm.C;
   a.dead = lm.dead;
   a.m0 = lm.m0;
-  a.ignore = hg.ignore;
   a.len_max = hg.len_max;
   a.tok_ids = g->tok_ids.p;
   a.tok_starts = g->tok_starts.p;
@@ -48,36 +49,21 @@ inline LexArgs lex_args(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, 
                         (unsigned long long *)g->st2_inc.p};
   a.status = g->d_status;
   a.diag = g->diag;
-  a.stage_ids = (uint8_t *)g->stage_ids.p;
-  a.stage_starts = (uint32_t *)g->stage_starts.p;
-  a.stage_ends = (uint32_t *)g->stage_ends.p;
-  a.tile_cnt = (uint32_t *)g->tile_cnt.p;
-  a.tile_pos = (uint32_t *)g->tile_pos.p;
   return a;
 }
 
-inline LexPlaceArgs lex_place_args(alpacc_gpu_grammar *g, const LexArgs &a, uint64_t tiles) {
-  LexPlaceArgs pa{};
-  pa.num_tiles = tiles;
-  pa.tile_data = kLexData;
-  pa.n = a.n;
-  pa.tile_cnt = a.tile_cnt;
-  pa.tile_pos = a.tile_pos;
-  pa.tile_off = (unsigned long long *)g->tile_off.p;
-  pa.tile_prev = (uint32_t *)g->tile_prev.p;
-  pa.stage_ids = a.stage_ids;
-  pa.stage_starts = a.stage_starts;
-  pa.stage_ends = a.stage_ends;
-  pa.tok_ids = a.tok_ids;
-  pa.tok_starts = a.tok_starts;
-  pa.tok_lens = a.tok_lens;
-  pa.term_w = a.term_w;
-  pa.idx_w = a.idx_w;
-  pa.len_w = a.len_w;
-  pa.len_max = a.len_max;
-  pa.status = a.status;
-  pa.batch = a.batch;
-  return pa;
+// The lexer kernel for this handle's machine.
+inline cudaError_t launch_lex(const alpacc_gpu_grammar *g, const LexArgs &a, unsigned grid, cudaStream_t s) {
+  if (g->lex_w4) lex_kernel_wide<<<grid, kLexThreads, lex_dyn_smem(g), s>>>(a);
+  else lex_kernel<<<grid, kLexThreads, lex_dyn_smem(g), s>>>(a);
+  return cudaGetLastError();
+}
+
+// Resident CTAs of that kernel per SM.
+inline cudaError_t lex_occupancy(const alpacc_gpu_grammar *g, int *per_sm) {
+  return g->lex_w4 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, lex_kernel_wide, kLexThreads,
+                                                                   lex_dyn_smem(g))
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, lex_kernel, kLexThreads, lex_dyn_smem(g));
 }
 
 inline PairArgs pair_args(alpacc_gpu_grammar *g) {
@@ -120,7 +106,7 @@ inline PseArgs pse_args(alpacc_gpu_grammar *g, int mode, unsigned long long queu
   a.ch_min = (int32_t *)g->chunk_min.p;
   a.ch_tc = (int32_t *)g->ch_tc.p;
   a.tile_min = (int32_t *)g->tile_min.p;
-  a.super_min = (int32_t *)g->super_min.p;
+  a.super_key = (uint32_t *)g->super_key.p;
   a.queue = (unsigned long long *)g->queue.p;
   a.queue_cap = queue_cap;
   a.queue_len = (unsigned long long *)g->queue_len.p;

@@ -240,7 +240,7 @@ class Parser:
     def info(self) -> dict:
         vals = (ctypes.c_int64 * 16)()
         n = lib().alpacc_gpu_info(self._h, vals, 16)
-        keys = ["M", "C", "max_lanes", "reachable", "dead", "nt", "records", "trans_rep", "lex_reject_reason",
+        keys = ["M", "C", "max_lanes", "reachable", "dead", "nt", "records", "lex_grid", "lex_reject_reason",
                 "parse_reject_reason", "timeout_site"]
         return dict(zip(keys, [vals[i] for i in range(min(n, len(keys)))]))
 
@@ -407,8 +407,8 @@ class Parser:
         """Tokens, brackets, productions, nodes of the last call."""
         vals = (ctypes.c_int64 * 9)()
         lib().alpacc_gpu_counts(self._h, vals, 9)
-        return {"T": vals[0], "B": vals[1], "P": vals[2], "N": vals[3], "vector_tiles": vals[4],
-                "const_chunks": vals[5], "chain_evals": vals[6], "multi_lane_bytes": vals[7], "launches": vals[8]}
+        return {"T": vals[0], "B": vals[1], "P": vals[2], "N": vals[3], "lookback_tiles": vals[4],
+                "const_chunks": vals[5], "chain_evals": vals[6], "set_walk_bytes": vals[7], "launches": vals[8]}
 
     def set_diagnostics(self, on: bool):
         lib().alpacc_gpu_set_diagnostics(self._h, 1 if on else 0)

@@ -168,7 +168,7 @@ def ours_batch(a, rank, world, local_rank, dist):
     pin.numpy()[:] = np.frombuffer(buf, dtype=np.uint8)
     offs = np.ascontiguousarray(offs, dtype=np.int64)
     d_all = pin.to(dev)
-    choice = parser.autotune(d_all.data_ptr(), total)  # lexer table copies for this grammar
+    choice = parser.autotune(d_all.data_ptr(), total)  # the lexer's resident CTAs per SM for this grammar
     ext = torch.cuda.ExternalStream(parser.stream_handle(), device=dev)
     count = len(offs) - 1
 
@@ -217,7 +217,7 @@ def ours_batch(a, rank, world, local_rank, dist):
         "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u8", "data": "synthetic (seeded JSON generator, log-normal lengths)",
         "config": dict(workload_config(total, world, "batch"), documents=count, accepted=int(accepted),
-                       autotune_lexer_table_copies=choice),
+                       autotune_lexer_ctas_per_sm=choice),
         "per_input": {"value": job_throughput(world, total, 1, per_ms), "unit": "GB/s", "ms": per_ms,
                       "what": "one alpacc_gpu_parse per document, same host buffers"},
         "speedup_vs_per_input": (job_throughput(world, total, a.steps, ms) / job_throughput(world, total, 1, per_ms)),

@@ -303,10 +303,10 @@ double alpacc_gpu_last_ms(alpacc_gpu_grammar *g);
 
 /*
  * Autotuner (no counterpart in the reference, whose CUDA backend takes its
- * launch shapes from per-architecture tables): parses the device-resident
- * sample with each candidate number of shared-memory copies of the lexer's
- * tables (more copies: fewer bank conflicts; fewer: more resident CTAs) and
- * keeps the fastest for this handle's grammar. *choice receives it.
+ * launch shapes from per-architecture tables, backends/cuda/lexer.cu:101-193):
+ * parses the device-resident sample with each candidate number of resident
+ * lexer CTAs per SM (from the occupancy limit down) and keeps the fastest for
+ * this handle's grammar. *choice receives it.
  */
 int alpacc_gpu_autotune(alpacc_gpu_grammar *g, const uint8_t *d_sample, uint64_t n, int *choice);
 
@@ -326,8 +326,9 @@ const char *alpacc_gpu_last_error(const alpacc_gpu_grammar *g);
    bracket walk, bracket resolve, parent walk, parent resolve, compaction. */
 int alpacc_gpu_stage_ms(const alpacc_gpu_grammar *g, double *out, int n);
 /* Tokens, brackets, productions and tree nodes of the last call, then four
-   lexer diagnostic counters (collected when diagnostics are on): tiles without
-   a constant chunk, constant chunks, chain evaluations, multi-lane bytes; then
+   lexer diagnostic counters (collected when diagnostics are on): tiles that
+   read their incoming state from the previous tile, constant chunks, chunk
+   evaluations chained to find start states, bytes walked as state sets; then
    the number of kernels the call launched. */
 int alpacc_gpu_counts(const alpacc_gpu_grammar *g, int64_t *vals, int n);
 void alpacc_gpu_set_diagnostics(alpacc_gpu_grammar *g, int on);
