@@ -405,6 +405,7 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
     if (ls.error == 0 && !ls.reject) TRY(start_token_copy(g, ls.num_tokens));
   }
   int rc = sync_status(g);
+  if (rc == ALPACC_OK && g->h_status->overflow) rc = ALPACC_E_CAPACITY;  // grown and run again by run_device
   float ms = 0;
   if (cudaEventElapsedTime(&ms, g->ev0, g->ev1) == cudaSuccess) g->last_ms = ms;
   collect_stages(g);

@@ -196,9 +196,9 @@ int run_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offset
   std::vector<uint64_t> T(D, 0), N(D, 0);
   uint64_t Tt = 0, Nt = 0;
   for (int d = 0; d < D; d++) {
-    if (st[d].error != 0) {
+    if (st[d].error != 0 || st[d].overflow) {  // the regions are upper bounds: an overflow is an internal error
       g->last_error = "batch document failed";
-      return st[d].error;
+      return st[d].error != 0 ? st[d].error : ALPACC_E_CAPACITY;
     }
     const uint64_t P = st[d].num_productions;
     T[d] = st[d].num_tokens;

@@ -33,7 +33,7 @@ struct DeviceStatus {
   int reject;        // 1 when the input is rejected
   int error;         // ALPACC_E_* (negative) on an internal failure
   int timeout_site;  // TimeoutSite of the first wait that ran out
-  int reserved;
+  int overflow;      // 1 when a scratch array was too small (the host grows it and runs again)
   unsigned long long num_tokens;
   unsigned long long num_brackets;
   unsigned long long num_productions;
@@ -71,6 +71,13 @@ __device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned l
 __device__ __forceinline__ void record_timeout(DeviceStatus *st, int site) {
   atomicCAS(&st->timeout_site, 0, site);
   atomicCAS(&st->error, 0, -5 /* ALPACC_E_TIMEOUT */);
+}
+
+// A scratch array of the call is too small. Unlike an error, this does not
+// stop the look-backs, so the counts the kernels publish stay exact and the
+// host can size the retry from them.
+__device__ __forceinline__ void record_overflow(DeviceStatus *st) {
+  if (*reinterpret_cast<volatile int *>(&st->overflow) == 0) atomicExch(&st->overflow, 1);
 }
 
 __device__ __forceinline__ void record_reject(DeviceStatus *st, int *reason, int why) {

@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(kPairThreads, 5) pair_kernel(PairArgs a) {
     if (__syncthreads_or(t == 0 && *reinterpret_cast<volatile int *>(&a.status->reject) != 0)) return;
     total = (*a.num_tokens + 2 + kPairTile - 1) / kPairTile;
     if (total > a.tiles_cap) {
-      if (t == 0 && blockIdx.x == 0) atomicCAS(&a.status->error, 0, -4 /* ALPACC_E_CAPACITY */);
+      if (t == 0 && blockIdx.x == 0) record_overflow(a.status);
       return;
     }
   }
@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(kPairThreads, 5) pair_kernel(PairArgs a) {
   __syncthreads();
   const long long pre_b = s_prefix_b, pre_p = s_prefix_p;
   if ((unsigned long long)(pre_b + tb) > br_cap || (unsigned long long)(pre_p + tp) > pr_cap) {
-    if (t == 0) atomicCAS(&st->error, 0, -4 /* ALPACC_E_CAPACITY */);
+    if (t == 0) record_overflow(st);
     continue;
   }
   // ---- brackets (pass 0) and productions (pass 1) through the output window ----
@@ -327,11 +327,14 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   if (a.batch) {
     total = (parents ? a.batch->pr_tile0 : a.batch->br_tile0)[a.batch->docs];
   } else {
-    // already rejected: nothing to find (one read, shared by the CTA)
-    if (__syncthreads_or(t == 0 && *reinterpret_cast<volatile int *>(&a.status->reject) != 0)) return;
+    // already rejected, or the pair stage overflowed: nothing to find (one
+    // read, shared by the CTA)
+    if (__syncthreads_or(t == 0 && (*reinterpret_cast<volatile int *>(&a.status->reject) != 0 ||
+                                    *reinterpret_cast<volatile int *>(&a.status->overflow) != 0)))
+      return;
     const unsigned long long E = *a.count;
     if (E > a.elem_cap) {
-      if (t == 0 && blockIdx.x == 0) atomicCAS(&a.status->error, 0, -4 /* ALPACC_E_CAPACITY */);
+      if (t == 0 && blockIdx.x == 0) record_overflow(a.status);
       return;
     }
     total = (E + kPseTile - 1) / kPseTile;
@@ -526,7 +529,7 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
       for (int j = 0; j < kPseItems; ++j)
         if (ans[j] == -1) {
           if (qi < a.queue_cap) a.queue[qi] = ((unsigned long long)doc << 40) | (unsigned long long)(c0 + j);
-          else atomicCAS(&st->error, 0, -4 /* ALPACC_E_CAPACITY */);
+          else record_overflow(st);
           ++qi;
         }
     }
@@ -646,8 +649,10 @@ __device__ __forceinline__ long long terminal_count(const PseArgs &a, const PseD
 // latest chunk of that tile, then the latest element of that chunk (depths
 // recomputed from the chunk's start depth).
 __global__ void pse_resolve_kernel(PseArgs a) {
-  // the walk did not complete (no kernel sets an error word while this one runs)
-  if (!a.batch && *reinterpret_cast<volatile int *>(&a.status->error)) return;
+  // the walk did not complete (no kernel sets these words while this one runs)
+  if (!a.batch && (*reinterpret_cast<volatile int *>(&a.status->error) ||
+                   *reinterpret_cast<volatile int *>(&a.status->overflow)))
+    return;
   const unsigned long long qn = *a.queue_len;
   const bool parents = a.mode == kPseParents;
   const int lane = threadIdx.x & 31;
