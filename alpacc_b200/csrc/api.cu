@@ -73,7 +73,12 @@ int upload_tables(alpacc_gpu_grammar *g) {
 
 int upload_pairs(alpacc_gpu_grammar *g) {
   const PairTable &pt = g->hg.pairs;
-  TRY(upload(g->dense, pt.dense));
+  if (pt.hashed) {
+    TRY(upload(g->ht_key, pt.ht_key));
+    TRY(upload(g->ht_rec, pt.ht_rec));
+  } else {
+    TRY(upload(g->dense, pt.dense));
+  }
   // records packed as ss | ps << 24 | nb << 48 | np << 56 (spans checked < 2^24 on load)
   std::vector<unsigned long long> rec(pt.rec_ss.size());
   for (size_t i = 0; i < rec.size(); i++)
@@ -541,7 +546,7 @@ void alpacc_gpu_free(alpacc_gpu_grammar *g) {
   cudaSetDevice(g->device);
   if (g->stream) cudaStreamSynchronize(g->stream);
   DevBuf *bufs[] = {&g->lex_tab, &g->lex_cls4, &g->lane_of, &g->img, &g->img_cnt, &g->img2, &g->sterm, &g->sflags,
-                    &g->dense, &g->rec, &g->stacks, &g->prods,
+                    &g->dense, &g->ht_key, &g->ht_rec, &g->rec, &g->stacks, &g->prods,
                     &g->arity, &g->is_term, &g->in, &g->lex_ticket, &g->st1_flag, &g->st1_state, &g->st1_vec,
                     &g->st2_flags, &g->st2_agg, &g->st2_inc, &g->tok_ids, &g->tok_starts, &g->tok_lens,
                     &g->pair_ticket, &g->pst_flags, &g->pst_agg, &g->pst_inc, &g->br, &g->pr, &g->pse_ticket,
@@ -893,7 +898,7 @@ int alpacc_gpu_info(const alpacc_gpu_grammar *g, int64_t *vals, int nvals) {
                        g->hg.pairs.nt, (int64_t)g->hg.pairs.rec_ss.size(), g->lex_grid,
                        g->h_status ? g->h_status->lex_reject_reason : 0,
                        g->h_status ? g->h_status->parse_reject_reason : 0,
-                       g->h_status ? g->h_status->timeout_site : 0};
+                       g->h_status ? g->h_status->timeout_site : 0, g->hg.pairs.hashed ? 1 : 0};
   const int nv = (int)(sizeof(v) / sizeof(v[0]));
   for (int i = 0; i < nvals && i < nv; i++) vals[i] = v[i];
   return nv;

@@ -2,6 +2,7 @@
 #include "device_tables.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <unordered_map>
@@ -235,6 +236,9 @@ int build_lexer_table(const LexerMachine &lm, LexerTable *out, std::string *why)
   return ALPACC_OK;
 }
 
+static int build_pairs_hashed(const alpacc_tables *t, PairTable *pt, std::string *why);
+static int build_pair_arrays(const alpacc_tables *t, PairTable *pt, std::string *why);
+
 static int build_pairs(const alpacc_tables *t, PairTable *pt, std::string *why) {
   const int q = (int)t->q, k = (int)t->k;
   const int L = q + k;
@@ -244,14 +248,19 @@ static int build_pairs(const alpacc_tables *t, PairTable *pt, std::string *why) 
   pt->k = k;
   if (L <= 0 || L > 8) { *why = "q + k must be in 1..8"; return ALPACC_E_UNSUPPORTED; }
   uint64_t dense = 1;
-  for (int i = 0; i < L; i++) {
+  bool fits = true;
+  for (int i = 0; i < L && fits; i++) {
     dense *= (uint64_t)nt;
-    if (dense > (1ull << 26)) { *why = "pair key space too large for the dense table"; return ALPACC_E_UNSUPPORTED; }
+    fits = dense <= kDenseLimit;
   }
-  pt->dense_size = dense;
-  pt->dense.assign(dense, 0xffffffffu);
   const uint64_t H = t->hash_table_size;
   const uint32_t tw = t->terminal_size;
+  // ALPACC_PAIR_LOOKUP=hashed selects the hashed form for any key space (a
+  // diagnostic switch: it lets the probe replay be checked on every grammar)
+  const char *force = getenv("ALPACC_PAIR_LOOKUP");
+  if (!fits || (force && strcmp(force, "hashed") == 0)) return build_pairs_hashed(t, pt, why);
+  pt->dense_size = dense;
+  pt->dense.assign(dense, 0xffffffffu);
   // every key the table holds, looked up exactly as lookup_key does
   std::vector<uint64_t> key(L), probe_key(L);
   for (uint64_t slot = 0; slot < H; slot++) {
@@ -291,6 +300,55 @@ static int build_pairs(const alpacc_tables *t, PairTable *pt, std::string *why) 
     pt->max_br = std::max(pt->max_br, (int)(se - ss));
     pt->max_pr = std::max(pt->max_pr, (int)(pe - ps));
   }
+  return build_pair_arrays(t, pt, why);
+}
+
+// The hashed form: every valid slot of the reference's table, with its own
+// record when its spans are usable.
+static int build_pairs_hashed(const alpacc_tables *t, PairTable *pt, std::string *why) {
+  const int L = pt->q + pt->k;
+  const uint64_t H = t->hash_table_size;
+  const uint32_t tw = t->terminal_size;
+  if (H == 0 || H > (1ull << 31)) { *why = "hash table size out of range"; return ALPACC_E_UNSUPPORTED; }
+  pt->hashed = true;
+  pt->max_iters = t->max_iters;
+  pt->ht_key.assign(H, 0);
+  pt->ht_rec.assign(H, kEmptySlot);
+  for (uint64_t slot = 0; slot < H; slot++) {
+    if (!t->hash_table_is_valid[slot]) continue;
+    unsigned long long packed = 0;
+    for (int j = 0; j < L; j++) {
+      const uint64_t v = read_uint(t->hash_table_keys, slot * L + j, tw);
+      if (v > 255) { *why = "terminal ids above 255 are not supported"; return ALPACC_E_UNSUPPORTED; }
+      packed |= (unsigned long long)v << (8 * j);
+    }
+    pt->ht_key[slot] = packed;
+    const int64_t ss = t->hash_table_stacks_span[2 * slot], se = t->hash_table_stacks_span[2 * slot + 1];
+    const int64_t ps = t->hash_table_productions_span[2 * slot], pe = t->hash_table_productions_span[2 * slot + 1];
+    if (ss < 0 || se < 0 || ps < 0 || pe < 0) {  // lookup_key returns false for this key
+      pt->ht_rec[slot] = kMissingKey;
+      continue;
+    }
+    if (se < ss || pe < ps || (uint64_t)se > t->stacks_size || (uint64_t)pe > t->productions_size) {
+      *why = "hash table span out of range";
+      return ALPACC_E_INVALID;
+    }
+    if (se - ss > 255 || pe - ps > 255) { *why = "more than 255 brackets or productions per pair"; return ALPACC_E_UNSUPPORTED; }
+    if (ss >= (1 << 24) || ps >= (1 << 24)) { *why = "stack or production table too large"; return ALPACC_E_UNSUPPORTED; }
+    pt->ht_rec[slot] = (uint32_t)pt->rec_ss.size();
+    pt->rec_ss.push_back((uint32_t)ss);
+    pt->rec_ps.push_back((uint32_t)ps);
+    pt->rec_nb.push_back((uint8_t)(se - ss));
+    pt->rec_np.push_back((uint8_t)(pe - ps));
+    pt->max_br = std::max(pt->max_br, (int)(se - ss));
+    pt->max_pr = std::max(pt->max_pr, (int)(pe - ps));
+  }
+  return build_pair_arrays(t, pt, why);
+}
+
+// Stack actions, productions and the per-production arities and flags, for
+// either form of the table.
+static int build_pair_arrays(const alpacc_tables *t, PairTable *pt, std::string *why) {
   const uint32_t bw = t->bracket_size;
   const uint64_t top = 1ull << (8 * bw - 1);
   pt->stacks.resize(t->stacks_size);

@@ -54,14 +54,28 @@ struct LexerTable {
 
 int build_lexer_table(const LexerMachine &lm, LexerTable *out, std::string *why);
 
-// LLP pair table as a dense array indexed by the key's terminals in base NT
-// (NT = END + 1): entry = record index or 0xffffffff when the reference's
-// lookup_key (backends/c/parser.c:17-45) would fail for that key.
+// LLP pair table, in one of two forms. Dense (key spaces up to 2^26): an
+// array indexed by the key's terminals in base NT (NT = END + 1), entry =
+// record index or 0xffffffff when the reference's lookup_key
+// (backends/c/parser.c:17-45) would fail for that key. Hashed (larger key
+// spaces, or forced): the reference's own open-addressing table, probed on
+// the device exactly as lookup_key probes it - FNV-1a over the key's
+// terminals, linear probing up to MAX_ITERS slots, the first slot holding the
+// key decides - with the key's terminals packed 8 bits each into a u64 and per
+// slot a record index, kEmptySlot (not a valid slot: probing goes on) or
+// kMissingKey (the key is there but a span is negative: lookup fails).
+constexpr uint32_t kEmptySlot = 0xffffffffu, kMissingKey = 0xfffffffeu;
+constexpr uint64_t kDenseLimit = 1ull << 26;
+
 struct PairTable {
   int nt = 0;                     // terminal ids 0..nt-1
   int q = 0, k = 0;
   uint64_t dense_size = 0;
-  std::vector<uint32_t> dense;    // [nt^(q+k)]
+  std::vector<uint32_t> dense;    // [nt^(q+k)], empty in the hashed form
+  bool hashed = false;
+  uint64_t max_iters = 0;
+  std::vector<unsigned long long> ht_key;  // [HASH_TABLE_SIZE] packed key terminals
+  std::vector<uint32_t> ht_rec;            // [HASH_TABLE_SIZE] record index, kEmptySlot or kMissingKey
   // record r: STACKS[rec_ss[r] .. +rec_nb[r]) and PRODUCTIONS[rec_ps[r] .. +rec_np[r])
   std::vector<uint32_t> rec_ss, rec_ps;
   std::vector<uint8_t> rec_nb, rec_np;

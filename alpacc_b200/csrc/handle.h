@@ -80,7 +80,7 @@ struct alpacc_gpu_grammar {
   double stage_ms[kStages] = {};
   // tables
   DevBuf lex_tab, lex_cls4, lane_of, img, img_cnt, img2, sterm, sflags;
-  DevBuf dense, rec, stacks, prods, arity, is_term;
+  DevBuf dense, ht_key, ht_rec, rec, stacks, prods, arity, is_term;
   // lexer table shape (build_lexer_table): entries, rows of 1 << (cp_shift - 2),
   // column swizzle mask, u16 class table when classes exceed 64
   int tab_words = 0, cp_shift = 2, swz = 0, wide_cls = 0;

@@ -114,7 +114,10 @@ struct PairArgs {
   unsigned long long tiles_cap;          // pair tiles the look-back state holds (ALPACC_E_CAPACITY beyond)
   int q, k, nt;
   int empty_t, start_t, end_t;
-  const uint32_t *dense;    // [nt^(q+k)] record index or 0xffffffff
+  const uint32_t *dense;    // [nt^(q+k)] record index or 0xffffffff; null: the hashed form below
+  const unsigned long long *ht_key;  // hashed form: [ht_size] key terminals packed 8 bits each
+  const uint32_t *ht_rec;            // hashed form: [ht_size] record, kEmptySlot or kMissingKey
+  unsigned long long ht_size, max_iters;
   const unsigned long long *rec;  // ss | ps << 24 | nb << 48 | np << 56
   const uint32_t *stacks;   // bit31 left
   const uint32_t *prods;

@@ -132,14 +132,38 @@ __global__ void __launch_bounds__(kPairThreads, 5) pair_kernel(PairArgs a) {
     const int li = j * kPairThreads + t;
     uint32_t r = 0xffffffffu;
     if (tile0 + li < m) {
-      unsigned long long d = 0;
       bool bad = false;
-      for (int x = 0; x < L; ++x) {
-        const unsigned term = s_term[li + x];
-        bad |= term == 0xffffu;  // keeps the table index in bounds
-        d = d * (unsigned long long)a.nt + term;
+      if (a.dense) {
+        unsigned long long d = 0;
+        for (int x = 0; x < L; ++x) {
+          const unsigned term = s_term[li + x];
+          bad |= term == 0xffffu;  // keeps the table index in bounds
+          d = d * (unsigned long long)a.nt + term;
+        }
+        r = bad ? 0xffffffffu : __ldg(a.dense + d);
+      } else {
+        // lookup_key (parser.c:30-45): FNV-1a over the key's terminals, linear
+        // probing from hash % size for at most MAX_ITERS slots; the first slot
+        // holding the key decides
+        unsigned long long h = 14695981039346656037ull, key = 0;
+        for (int x = 0; x < L; ++x) {
+          const unsigned term = s_term[li + x];
+          bad |= term == 0xffffu;  // an id outside the grammar is never a key
+          h = (h ^ (unsigned long long)term) * 1099511628211ull;
+          key |= (unsigned long long)(term & 0xffu) << (8 * x);
+        }
+        if (!bad) {
+          h %= a.ht_size;
+          for (unsigned long long it = 0; it < a.max_iters; ++it) {
+            const uint32_t rr = __ldg(a.ht_rec + h);
+            if (rr != kEmptySlot && __ldg(a.ht_key + h) == key) {
+              r = rr == kMissingKey ? 0xffffffffu : rr;
+              break;
+            }
+            h = h + 1 == a.ht_size ? 0 : h + 1;
+          }
+        }
       }
-      r = bad ? 0xffffffffu : __ldg(a.dense + d);
       if (r == 0xffffffffu) missing = true;
     }
     s_rec[li] = r;

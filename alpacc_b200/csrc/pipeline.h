@@ -79,7 +79,11 @@ inline PairArgs pair_args(alpacc_gpu_grammar *g) {
   a.empty_t = (int)tb.empty_terminal;
   a.start_t = (int)tb.start_terminal;
   a.end_t = (int)tb.end_terminal;
-  a.dense = (const uint32_t *)g->dense.p;
+  a.dense = pt.hashed ? nullptr : (const uint32_t *)g->dense.p;
+  a.ht_key = (const unsigned long long *)g->ht_key.p;
+  a.ht_rec = (const uint32_t *)g->ht_rec.p;
+  a.ht_size = pt.ht_key.size();
+  a.max_iters = pt.max_iters;
   a.rec = (const unsigned long long *)g->rec.p;
   a.stacks = (const uint32_t *)g->stacks.p;
   a.prods = (const uint32_t *)g->prods.p;

@@ -72,7 +72,27 @@ extern "C" int pair_lookup(const alpacc_tables *t, const uint64_t *keys, uint64_
       if (v >= (uint64_t)pt.nt) bad = true;
       d = d * (uint64_t)pt.nt + (bad ? 0 : v);
     }
-    const uint32_t r = bad ? 0xffffffffu : pt.dense[d];
+    uint32_t r = 0xffffffffu;
+    if (!pt.hashed) {
+      r = bad ? 0xffffffffu : pt.dense[d];
+    } else if (!bad) {  // the device's probe of the hashed form
+      uint64_t h = 14695981039346656037ull;
+      unsigned long long packed = 0;
+      for (int j = 0; j < L; j++) {
+        h = (h ^ keys[i * L + j]) * 1099511628211ull;
+        packed |= (unsigned long long)keys[i * L + j] << (8 * j);
+      }
+      const uint64_t H = pt.ht_key.size();
+      h %= H;
+      for (uint64_t it = 0; it < pt.max_iters; it++) {
+        const uint32_t rr = pt.ht_rec[h];
+        if (rr != alpacc::kEmptySlot && pt.ht_key[h] == packed) {
+          r = rr == alpacc::kMissingKey ? 0xffffffffu : rr;
+          break;
+        }
+        h = h + 1 == H ? 0 : h + 1;
+      }
+    }
     int64_t *o = out + 5 * i;
     if (r == 0xffffffffu) {
       o[0] = 0;

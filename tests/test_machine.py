@@ -129,6 +129,20 @@ def test_pair_table_matches_lookup_key(harness, config):
     assert _check_pairs(L, cases.tables(config)) > 0
 
 
+@pytest.mark.parametrize("config", ["json_ext_i32", "arithmetic_i64", "sexp_i64", "paper_grammar_i64"])
+def test_hashed_pair_table_matches_lookup_key(harness, config, monkeypatch):
+    """The hashed form (used for key spaces above 2^26, forced here with
+    ALPACC_PAIR_LOOKUP=hashed): the device's probe of the reference's own
+    open-addressing table, restated in the harness, against lookup_key."""
+    monkeypatch.setenv("ALPACC_PAIR_LOOKUP", "hashed")
+    L = harness
+    L.pair_lookup.restype = ctypes.c_int
+    L.pair_lookup.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
+    assert _check_pairs(L, cases.tables(config)) > 0
+    for name, g, t in list(fuzz_grammars(6)):
+        assert _check_pairs(L, t) > 0, name
+
+
 def test_pair_table_random_grammars(harness):
     L = harness
     L.pair_lookup.restype = ctypes.c_int
