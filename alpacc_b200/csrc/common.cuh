@@ -149,6 +149,9 @@ struct AddU64 {
 struct AddI64 {
   __device__ __forceinline__ long long operator()(long long a, long long b) const { return a + b; }
 };
+struct AddI32 {
+  __device__ __forceinline__ int operator()(int a, int b) const { return a + b; }
+};
 struct MaxI32 {
   __device__ __forceinline__ int operator()(int a, int b) const { return a > b ? a : b; }
 };

@@ -21,14 +21,18 @@
 //   first bytes is walked until it is one state (typically 1-4 bytes on JSON)
 //   and word aligned; from there a fully unrolled single-lane walk writes each
 //   byte's code over the consumed input word. Such a chunk maps every live
-//   start to one end state ("constant"). A chunk whose set never shrinks to
-//   one state ("open") instead walks each of its first byte's targets on its
-//   own and keeps the end state per start lane.
+//   start to one end state ("constant"). A chunk whose set is not one state
+//   after 16 bytes ("open") instead has each of its first byte's targets
+//   walked on its own - one job per lane, spread over the whole CTA so that no
+//   thread walks several lanes while the others wait - keeping the end state
+//   per start lane and, for the first 64 jobs, the lane's codes.
 // Resolution: each chunk's start state follows from the nearest constant chunk
 //   before it; only when no halo chunk is constant does the tile read its
 //   predecessor's published outgoing state (bounded look-back).
-// Pass 2: each data chunk re-walks the bytes before its walk converged (all of
-//   an open or partial chunk) from its true start, writing their codes.
+// Pass 2: each data chunk re-walks the bytes before its walk converged from
+//   its true start, writing their codes; an open chunk copies its true lane's
+//   codes (or walks the chunk again when its lanes had no code slots), a
+//   partial chunk (the input's last) is walked whole.
 // Output: boundary masks from the code words, a (token count, last boundary)
 //   block scan, a decoupled look-back over tiles (Merrill & Garland 2016) taken
 //   last, and the kept tokens written straight into the final
@@ -58,6 +62,15 @@ enum ChunkKind : uint8_t { kEmpty = 0, kConst = 1, kOpen = 2, kPartial = 3 };
 
 constexpr uint32_t kAddrMask = 0xFFFFFFu;  // F(next) bits of an entry
 constexpr uint8_t kNoBoundary = 0xFF, kIgnored = 0xFE;
+// Bytes a chunk walks as a state set before it counts as open: bounds how long
+// one late-converging chunk can hold its warp in the set walk.
+constexpr int kSetWalk = 16;
+// Lane walks of open chunks run as jobs spread over the CTA, one lane per
+// thread; the first kCodeJobs keep their codes, so the chunk's pass 2 copies
+// the true lane's codes instead of walking again.
+constexpr int kLexJobs = kLexThreads;
+constexpr int kCodeJobs = 64;
+constexpr uint16_t kNoJobs = 0xffff;
 
 struct LexSmem {
   uint32_t bytes[kLexThreads * kLexWords];  // the tile; codes replace the consumed words
@@ -66,6 +79,10 @@ struct LexSmem {
   uint8_t endst[kLexThreads];  // constant chunks: end state
   uint8_t c0[kLexThreads];     // class of the chunk's first byte
   uint8_t start[kLexThreads];  // true start state of data chunks
+  uint16_t jfirst[kLexThreads];  // open chunks: first lane job, or kNoJobs (its thread walks its lanes)
+  uint8_t jt[kLexJobs], jl[kLexJobs];  // lane job: chunk, lane
+  uint32_t jcodes[kCodeJobs * kLexWords];  // codes of bytes 1..59 of the first lane jobs
+  int njobs;
   uint8_t sterm[256];          // per machine state: terminal id
   uint8_t sflags[256];         // bit1 accept, bit2 kept
   int kconst[kLexThreads];
@@ -143,6 +160,17 @@ struct StateSet {
     for (int i = 0; i < W; i++)
       if ((s >> 6) == i) w[i] |= 1ull << (s & 63);
   }
+  // more than one state (no population count for a single word)
+  __device__ __forceinline__ bool many() const {
+    if (W == 1) return (w[0] & (w[0] - 1)) != 0;
+    return count() > 1;
+  }
+  __device__ __forceinline__ bool empty() const {
+    unsigned long long o = 0;
+#pragma unroll
+    for (int i = 0; i < W; i++) o |= w[i];
+    return o == 0;
+  }
   __device__ __forceinline__ int count() const {
     int c = 0;
 #pragma unroll
@@ -180,9 +208,10 @@ __device__ __forceinline__ int pass1_chunk(const LexArgs &a, const Tab &tb, LexS
     for (int l = 0; l < cnt; l++) set.add(__ldg(a.img + c0 * kLexLanes + l));
     j = 1;
   }
-  // walk the set until it is one state and the position is word aligned
-  int live = set.count();
-  while (j < kLexChunk && (live > 1 || (j & 3))) {
+  // walk the set until it is one state and the position is word aligned, at
+  // most kSetWalk bytes
+  bool many = set.many();
+  while (j < kSetWalk && (many || (j & 3))) {
     const uint32_t c4 = cls4_of(tb, rb[j]);
     StateSet<W> ns;
     ns.clear();
@@ -194,22 +223,16 @@ __device__ __forceinline__ int pass1_chunk(const LexArgs &a, const Tab &tb, LexS
         if (nx != dead) ns.add(nx);
       }
     set = ns;
-    live = set.count();
+    many = set.many();
     ++j;
   }
   *conv_out = -1;
-  if (live == 0) {  // every live start dies in this chunk
+  if (set.empty()) {  // every live start dies in this chunk
     *jw_out = j;
     *end_out = dead;
     return kConst;
   }
-  if (live > 1) {  // open: the end state of each start lane, walked on its own
-    const int cnt = __ldg(a.img_cnt + c0);
-    for (int l = 0; l < cnt; l++) {
-      uint32_t f = row_of(tb, __ldg(a.img + c0 * kLexLanes + l));
-      for (int k = 1; k < kLexChunk; k++) f = step(tb, f, cls4_of(tb, rb[k]));
-      sm->lend[l * kLexThreads + t] = (uint8_t)state_of(tb, f);
-    }
+  if (many) {  // open: its start lanes are walked one by one as CTA-wide jobs
     *jw_out = kLexChunk;
     *end_out = -1;
     return kOpen;
@@ -238,6 +261,34 @@ __device__ __forceinline__ int pass1_chunk(const LexArgs &a, const Tab &tb, LexS
   }
   *end_out = state_of(tb, f);
   return kConst;
+}
+
+// One lane of an open chunk: bytes 1..59 of chunk tc's row walked from lane
+// l's state (the state byte 0 leads to), end state into lend; with `codes`,
+// the codes of bytes 1..59 (byte 0 left 0xFF).
+__device__ __forceinline__ void walk_lane(const LexArgs &a, const Tab &tb, LexSmem *sm, int tc, int l,
+                                          uint32_t *codes) {
+  const uint32_t *row = sm->bytes + tc * kLexWords;
+  uint32_t f = row_of(tb, __ldg(a.img + sm->c0[tc] * kLexLanes + l));
+  {
+    const uint32_t word = row[0];
+    const uint32_t e1 = step(tb, f, cls4_of(tb, __byte_perm(word, 0, 0x4441)));
+    const uint32_t e2 = step(tb, e1, cls4_of(tb, __byte_perm(word, 0, 0x4442)));
+    const uint32_t e3 = step(tb, e2, cls4_of(tb, __byte_perm(word, 0, 0x4443)));
+    f = e3;
+    if (codes) codes[0] = __byte_perm(__byte_perm(0xFF000000u, e1, 0x0073), __byte_perm(e2, e3, 0x0073), 0x5410);
+  }
+#pragma unroll 2
+  for (int w = 1; w < kLexWords; ++w) {
+    const uint32_t word = row[w];
+    const uint32_t e0 = step(tb, f, cls4_of(tb, __byte_perm(word, 0, 0x4440)));
+    const uint32_t e1 = step(tb, e0, cls4_of(tb, __byte_perm(word, 0, 0x4441)));
+    const uint32_t e2 = step(tb, e1, cls4_of(tb, __byte_perm(word, 0, 0x4442)));
+    const uint32_t e3 = step(tb, e2, cls4_of(tb, __byte_perm(word, 0, 0x4443)));
+    f = e3;
+    if (codes) codes[w] = __byte_perm(__byte_perm(e0, e1, 0x0073), __byte_perm(e2, e3, 0x0073), 0x5410);
+  }
+  sm->lend[l * kLexThreads + tc] = (uint8_t)state_of(tb, f);
 }
 
 template <int W>
@@ -332,6 +383,28 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
     if (a.diag) {
       const unsigned w = __reduce_add_sync(0xffffffffu, (unsigned)(kind == kConst ? jw : nb));
       if (lane == 0) atomicAdd(&st->scratch[3], (unsigned long long)w);
+    }
+    // ---- open chunks: one job per start lane, spread over the CTA ----
+    {
+      const int lanes = kind == kOpen ? (int)__ldg(a.img_cnt + sm->c0[t]) : 0;
+      int njobs;
+      const int jex = block_exclusive_scan<int>(lanes, AddI32(), 0, sm->scan_a, &njobs);
+      if (kind == kOpen) {
+        if (jex + lanes <= kLexJobs) {
+          sm->jfirst[t] = (uint16_t)jex;
+          for (int l = 0; l < lanes; ++l) {
+            sm->jt[jex + l] = (uint8_t)t;
+            sm->jl[jex + l] = (uint8_t)l;
+          }
+        } else {
+          sm->jfirst[t] = kNoJobs;
+        }
+      }
+      __syncthreads();
+      if (t < njobs && t < kLexJobs)
+        walk_lane(a, tb, sm, sm->jt[t], sm->jl[t], t < kCodeJobs ? sm->jcodes + t * kLexWords : nullptr);
+      if (kind == kOpen && sm->jfirst[t] == kNoJobs)  // beyond the job slots: this thread walks its lanes
+        for (int l = 0; l < lanes; ++l) walk_lane(a, tb, sm, t, l, nullptr);
     }
     __syncthreads();
 
@@ -442,6 +515,19 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
       const int x0 = sm->start[t];
       bool died = x0 == dead;
       uint32_t f = row_of(tb, (uint32_t)(x0 < 0 ? 0 : x0));
+      int slot = 0xff;
+      if (kind == kOpen && !died) {
+        slot = __ldg(a.lane_of + (size_t)sm->c0[t] * a.M + x0);
+        const int job = slot == 0xff || sm->jfirst[t] == kNoJobs ? kCodeJobs : sm->jfirst[t] + slot;
+        if (job < kCodeJobs) {  // the true lane's codes, walked already: copy them
+          const uint32_t e0 = step(tb, f, cls4_of(tb, rb[0]));
+          const uint32_t *src = sm->jcodes + job * kLexWords;
+#pragma unroll
+          for (int w = 0; w < kLexWords; ++w) row[w] = src[w];
+          rb[0] = g0 >= 1 ? (uint8_t)(e0 >> 24) : kNoBoundary;
+          jw = 0;  // nothing left to walk
+        }
+      }
       if (!died) {
         for (int j = 0; j < jw; ++j) {
           const uint32_t e = step(tb, f, cls4_of(tb, rb[j]));
@@ -454,21 +540,26 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
         // the walk from the true start must meet the converged lane
         if (!died && conv >= 0 && state_of(tb, f) != conv) atomicCAS(&st->error, 0, -1 /* internal error */);
         x_end = died ? dead : end;
+      } else if (kind == kOpen && jw == 0) {
+        x_end = slot == 0xff ? dead : sm->lend[slot * kLexThreads + t];
       } else {
         x_end = died ? dead : state_of(tb, f);
       }
       if (x_end == dead) record_reject(st, &st->lex_reject_reason, 1);
-      // ---- boundaries (all) and kept-token count from the code words ----
+      // ---- boundaries (all) and kept boundaries (code < 0xFE, i.e.
+      // (code | 1) != 0xFF) from the code words ----
+      unsigned long long kmask = 0;
 #pragma unroll
       for (int w = 0; w < kLexWords; ++w) {
         const uint32_t cw = row[w];
         bmask |= (unsigned long long)movemask4(nonzero_bytes(~cw)) << (4 * w);
-        // kept: code < 0xFE, i.e. (code | 1) != 0xFF; bytes past nb do not count
-        const uint32_t kb = nonzero_bytes(~(cw | 0x01010101u));
-        if (4 * w + 4 <= nb) cnt += __popc(kb);
-        else if (4 * w < nb) cnt += __popc(kb & (0xFFFFFFFFu >> (8 * (4 * w + 4 - nb))));
+        kmask |= (unsigned long long)movemask4(nonzero_bytes(~(cw | 0x01010101u))) << (4 * w);
       }
-      if (nb < 64) bmask &= (1ull << nb) - 1;
+      if (nb < 64) {  // bytes past the input do not count
+        bmask &= (1ull << nb) - 1;
+        kmask &= (1ull << nb) - 1;
+      }
+      cnt = __popcll(kmask);
       if (bmask) lastb = g0 + 63 - __clzll((long long)bmask);
       if (g0 + nb == n && !a.open_end) {  // this chunk holds the last byte of the input
         final_kept = x_end != dead && (sm->sflags[x_end] & 4) != 0;

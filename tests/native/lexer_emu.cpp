@@ -2,7 +2,8 @@
 // of alpacc_b200/csrc/lexer.cu - the same shared-memory table
 // (build_lexer_table), tile and chunk geometry, pass 1 (state-set walk to a
 // word-aligned convergence point, unrolled single-lane walk writing codes over
-// the consumed words, per-lane end states of open chunks), resolution from the
+// the consumed words, per-lane end states of chunks whose set is not one
+// state after 16 bytes ("open"), with the true lane's codes), resolution from the
 // nearest constant chunk or the previous tile's published outgoing state /
 // transition vector, pass 2 (re-walk of the bytes walked as a set from the
 // true start), the boundary and kept masks computed with the kernel's byte
@@ -22,6 +23,7 @@
 namespace {
 
 constexpr int kThreads = 256, kWords = 15, kChunk = 60, kHalo = 8;
+constexpr int kSetWalk = 16;  // bytes a chunk walks as a state set before it counts as open
 constexpr int kLoad = kThreads * kChunk, kData = (kThreads - kHalo) * kChunk;
 enum { kEmpty = 0, kConst = 1, kOpen = 2, kPartial = 3 };
 
@@ -100,7 +102,7 @@ extern "C" int lexer_emu(const alpacc_tables *t, const uint8_t *in, uint64_t n, 
       }
       auto live_count = [&] { return (int)std::count(set.begin(), set.end(), 1); };
       int live = live_count();
-      while (j < kChunk && (live > 1 || (j & 3))) {
+      while (j < kSetWalk && (live > 1 || (j & 3))) {
         std::vector<char> ns(lm.M, 0);
         for (int s = 0; s < lm.M; s++)
           if (set[s]) {
