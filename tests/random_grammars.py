@@ -191,6 +191,25 @@ class RandomGrammar:
             stack.extend(reversed(rhs))
         return "".join(out)
 
+    def token_sentence(self, rng, budget: int) -> list:
+        """A random derivation as terminal ids (parser-mode input): the
+        terminals are declared first and in order, so terminal i has id i."""
+        out = []
+        stack = [self.nts[0]]
+        by_lhs = {nt: [rhs for lhs, rhs in self.prods if lhs == nt] for nt in self.nts}
+        steps = 0
+        while stack and steps < 200000:
+            steps += 1
+            s = stack.pop()
+            if s in self.regex:
+                out.append(self.terminals.index(s))
+                continue
+            opts = by_lhs[s]
+            if len(out) > budget or len(stack) > budget:
+                opts = sorted(opts, key=lambda r: sum(x in self.nts for x in r))[:1]
+            stack.extend(reversed(opts[int(rng.integers(0, len(opts)))]))
+        return out
+
     def inputs(self, seed: int = 0, exhaustive: int = 4, sentences=(8, 64, 2000, 20000),
                noise=(100, 15000, 40000)) -> list:
         rng = np.random.default_rng(seed)
@@ -232,6 +251,34 @@ def fuzz_grammars(count: int, first_seed: int = 0):
             continue
         found += 1
         yield name, g, t
+
+
+def big_keyspace_grammar():
+    """A random LLP(3, 3) grammar with 18 terminals (21 terminal ids with the
+    ignore and sentinel ids): its (q + k)-terminal key space, 21^6 = 85.8M
+    keys, exceeds the 2^26 keys of the dense pair table, so the loader keeps
+    the reference's hash table and the device probes it as lookup_key does.
+    Returns (name, grammar, combined tables)."""
+    from alpacc_b200.grammar.tables import generate_parts
+    g = RandomGrammar(0, 3, 3, num_chars=4, num_terminals=18, num_nonterminals=2, num_productions=3, size=20)
+    name = "big0_q3k3"
+    return name, g, generate_parts(g.text(), name, False, "both")
+
+
+def token_sentences(g, seed: int = 0, budgets=(4, 16, 300, 5000)) -> list:
+    """Parser-mode inputs of a random grammar: derivations as terminal-id bytes
+    (accepted), each also with one id changed (mostly rejected)."""
+    rng = np.random.default_rng(seed)
+    out = [b""]
+    for b in budgets:
+        for _ in range(3):
+            ids = g.token_sentence(rng, b)
+            out.append(bytes(ids))
+            if ids:
+                m = list(ids)
+                m[int(rng.integers(0, len(m)))] = int(rng.integers(0, len(g.terminals) + 3))
+                out.append(bytes(m))
+    return out
 
 
 # C's keywords: a lexer whose machine grows with every keyword that shares

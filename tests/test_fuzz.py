@@ -67,3 +67,16 @@ def test_keyword_lexers_all_modes(nkw):
     assert 0 < _check(t, name, ins) < len(ins)
     _check(generate_parts(text, name, False, "lexer"), name + "_lexer", ins)
     _check(generate_parts(text, name, False, "parser"), name + "_parser", cases.token_inputs_for(t, ins))
+
+
+def test_key_space_beyond_dense_table_vs_reference():
+    """The oversized-key-space grammar (hashed pair table on the device): the
+    oracle against the reference's programs built from its tables."""
+    if REFERENCE is None:
+        pytest.skip("reference sources not present")
+    from tests.random_grammars import big_keyspace_grammar
+    name, g, t = big_keyspace_grammar()
+    from tests.random_grammars import token_sentences
+    ins = g.inputs(0, sentences=(8, 64, 2000), noise=(100, 15000))
+    _check(t, name, ins)  # lexed random strings: mostly rejected, every record compared
+    assert _check(generate_parts(g.text(), name, False, "parser"), name + "_parser", token_sentences(g)) > 0

@@ -143,6 +143,17 @@ def test_hashed_pair_table_matches_lookup_key(harness, config, monkeypatch):
         assert _check_pairs(L, t) > 0, name
 
 
+def test_pair_table_key_space_beyond_dense(harness):
+    """A key space above 2^26 keys takes the hashed form without forcing."""
+    from tests.random_grammars import big_keyspace_grammar
+    L = harness
+    L.pair_lookup.restype = ctypes.c_int
+    L.pair_lookup.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
+    name, g, t = big_keyspace_grammar()
+    assert (t.end_terminal + 1) ** (t.q + t.k) > (1 << 26)
+    assert _check_pairs(L, t) > 0
+
+
 def test_pair_table_random_grammars(harness):
     L = harness
     L.pair_lookup.restype = ctypes.c_int
