@@ -48,8 +48,6 @@ __global__ void pack_ranges_kernel(const uint8_t *src, uint8_t *dst, const unsig
   }
 }
 
-constexpr int kPairCtas = 148 * 5;  // persistent grids of the batch path (resident CTAs)
-constexpr int kPseCtas = 148 * 4;
 
 int run_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offsets, uint32_t count,
               alpacc_result *outs) {
@@ -165,7 +163,8 @@ int run_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offset
     PairArgs pa = pair_args(g);
     pa.batch = d_bd;
     pa.status = bd.status;
-    pair_kernel<<<(unsigned)std::min<uint64_t>(pair_ub, kPairCtas), kPairThreads, 0, s>>>(pa);
+    pair_kernel<<<(unsigned)std::min<uint64_t>(pair_ub, (uint64_t)g->pair_grid), kPairThreads, pair_smem_bytes(g),
+                  s>>>(pa);
   }
   batch_plan_kernel<<<1, 1024, 0, s>>>(bd, kPlanBrackets, bd.br_tile0, kPseTile);
   batch_plan_kernel<<<1, 1024, 0, s>>>(bd, kPlanParents, bd.pr_tile0, kPseTile);
@@ -182,7 +181,7 @@ int run_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offset
     PseArgs pa = pse_args(g, mode, qcap);
     pa.batch = d_bd;
     pa.status = bd.status;
-    pse_tile_kernel<<<(unsigned)std::min<uint64_t>(ub, kPseCtas), kPseThreads, 0, s>>>(pa);
+    pse_tile_kernel<<<(unsigned)std::min<uint64_t>(ub, (uint64_t)g->pse_grid), kPseThreads, 0, s>>>(pa);
     pse_resolve_kernel<<<148 * 8, 256, 0, s>>>(pa);
     g->launches += 2;
     BCK(cudaGetLastError());

@@ -69,6 +69,22 @@ __global__ void __launch_bounds__(kPairThreads, 5) pair_kernel(PairArgs a) {
   __shared__ __align__(16) uint32_t s_out[kPairOut];     // output window
   const int t = threadIdx.x;
   const int L = a.q + a.k;
+  // records, stack actions and productions: staged in shared memory once per
+  // CTA when they are small, so the per-element gathers stay on chip
+  extern __shared__ __align__(16) unsigned char pair_dyn[];
+  const unsigned long long *rec = a.rec;
+  const uint32_t *stacks = a.stacks, *prods = a.prods;
+  if (a.smem_tables) {
+    unsigned long long *s_r = reinterpret_cast<unsigned long long *>(pair_dyn);
+    uint32_t *s_s = reinterpret_cast<uint32_t *>(s_r + a.n_rec);
+    uint32_t *s_p = s_s + a.n_stacks;
+    for (int i = t; i < a.n_rec; i += kPairThreads) s_r[i] = __ldg(a.rec + i);
+    for (int i = t; i < a.n_stacks; i += kPairThreads) s_s[i] = __ldg(a.stacks + i);
+    for (int i = t; i < a.n_prods; i += kPairThreads) s_p[i] = __ldg(a.prods + i);
+    rec = s_r;
+    stacks = s_s;
+    prods = s_p;
+  }
   unsigned long long total;
   if (a.batch) {
     total = a.batch->pair_tile0[a.batch->docs];
@@ -167,7 +183,7 @@ __global__ void __launch_bounds__(kPairThreads, 5) pair_kernel(PairArgs a) {
       if (r == 0xffffffffu) missing = true;
     }
     s_rec[li] = r;
-    s_cnt[li] = r == 0xffffffffu ? (uint16_t)0 : (uint16_t)(__ldg(a.rec + r) >> 48);
+    s_cnt[li] = r == 0xffffffffu ? (uint16_t)0 : (uint16_t)(rec[r] >> 48);
   }
   if (missing) record_reject(st, &st->parse_reject_reason, 1);
   __syncthreads();
@@ -216,7 +232,7 @@ __global__ void __launch_bounds__(kPairThreads, 5) pair_kernel(PairArgs a) {
   for (int pass = 0; pass < 2; ++pass) {
     const long long total = pass == 0 ? tb : tp;
     const long long base = pass == 0 ? (ex >> 32) : (ex & 0xffffffffll);
-    const uint32_t *src = pass == 0 ? a.stacks : a.prods;
+    const uint32_t *src = pass == 0 ? stacks : prods;
     uint32_t *dst = pass == 0 ? br_base + pre_b : pr_base + pre_p;
     for (long long w0 = 0; w0 < total; w0 += kPairOut) {
       long long o = base;
@@ -224,11 +240,11 @@ __global__ void __launch_bounds__(kPairThreads, 5) pair_kernel(PairArgs a) {
       for (int j = 0; j < kPairItems; ++j) {
         const int c = pass == 0 ? (cnt[j] & 0xff) : (cnt[j] >> 8);
         if (c == 0) continue;
-        const unsigned long long rc = __ldg(a.rec + s_rec[t * kPairItems + j]);
+        const unsigned long long rc = rec[s_rec[t * kPairItems + j]];
         const uint32_t sidx = (uint32_t)((pass == 0 ? rc : rc >> 24) & 0xffffffu);
         for (int x = 0; x < c; ++x) {
           const long long q = o + x - w0;
-          if (q >= 0 && q < kPairOut) s_out[q] = __ldg(src + sidx + x);
+          if (q >= 0 && q < kPairOut) s_out[q] = src[sidx + x];
         }
         o += c;
       }
