@@ -65,12 +65,10 @@ constexpr uint8_t kNoBoundary = 0xFF, kIgnored = 0xFE;
 // Bytes a chunk walks as a state set before it counts as open: bounds how long
 // one late-converging chunk can hold its warp in the set walk.
 constexpr int kSetWalk = 16;
-// Lane walks of open chunks run as jobs spread over the CTA, one lane per
-// thread; the first kCodeJobs keep their codes, so the chunk's pass 2 copies
-// the true lane's codes instead of walking again.
-constexpr int kLexJobs = kLexThreads;
+// Lane walks of open chunks run as jobs spread over the CTA (rounds of one
+// lane per thread); the first kCodeJobs keep their codes, so the chunk's
+// pass 2 copies the true lane's codes instead of walking again.
 constexpr int kCodeJobs = 64;
-constexpr uint16_t kNoJobs = 0xffff;
 
 struct LexSmem {
   uint32_t bytes[kLexThreads * kLexWords];  // the tile; codes replace the consumed words
@@ -79,10 +77,8 @@ struct LexSmem {
   uint8_t endst[kLexThreads];  // constant chunks: end state
   uint8_t c0[kLexThreads];     // class of the chunk's first byte
   uint8_t start[kLexThreads];  // true start state of data chunks
-  uint16_t jfirst[kLexThreads];  // open chunks: first lane job, or kNoJobs (its thread walks its lanes)
-  uint8_t jt[kLexJobs], jl[kLexJobs];  // lane job: chunk, lane
+  uint16_t jfirst[kLexThreads];  // first lane job of each chunk (jobs of earlier chunks; none for closed ones)
   uint32_t jcodes[kCodeJobs * kLexWords];  // codes of bytes 1..59 of the first lane jobs
-  int njobs;
   uint8_t sterm[256];          // per machine state: terminal id
   uint8_t sflags[256];         // bit1 accept, bit2 kept
   int kconst[kLexThreads];
@@ -389,22 +385,19 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
       const int lanes = kind == kOpen ? (int)__ldg(a.img_cnt + sm->c0[t]) : 0;
       int njobs;
       const int jex = block_exclusive_scan<int>(lanes, AddI32(), 0, sm->scan_a, &njobs);
-      if (kind == kOpen) {
-        if (jex + lanes <= kLexJobs) {
-          sm->jfirst[t] = (uint16_t)jex;
-          for (int l = 0; l < lanes; ++l) {
-            sm->jt[jex + l] = (uint8_t)t;
-            sm->jl[jex + l] = (uint8_t)l;
-          }
-        } else {
-          sm->jfirst[t] = kNoJobs;
-        }
-      }
+      sm->jfirst[t] = (uint16_t)jex;  // non-decreasing over the chunks (at most 256 x 32 jobs)
       __syncthreads();
-      if (t < njobs && t < kLexJobs)
-        walk_lane(a, tb, sm, sm->jt[t], sm->jl[t], t < kCodeJobs ? sm->jcodes + t * kLexWords : nullptr);
-      if (kind == kOpen && sm->jfirst[t] == kNoJobs)  // beyond the job slots: this thread walks its lanes
-        for (int l = 0; l < lanes; ++l) walk_lane(a, tb, sm, t, l, nullptr);
+      for (int job = t; job < njobs; job += kLexThreads) {
+        // the job's chunk: the last chunk whose first job is <= job (a chunk
+        // without lanes shares its successor's first job, so it is skipped)
+        int lo = 0, hi = kLexThreads - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if ((int)sm->jfirst[mid] <= job) lo = mid;
+          else hi = mid - 1;
+        }
+        walk_lane(a, tb, sm, lo, job - (int)sm->jfirst[lo], job < kCodeJobs ? sm->jcodes + job * kLexWords : nullptr);
+      }
     }
     __syncthreads();
 
@@ -518,7 +511,7 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
       int slot = 0xff;
       if (kind == kOpen && !died) {
         slot = __ldg(a.lane_of + (size_t)sm->c0[t] * a.M + x0);
-        const int job = slot == 0xff || sm->jfirst[t] == kNoJobs ? kCodeJobs : sm->jfirst[t] + slot;
+        const int job = slot == 0xff ? kCodeJobs : (int)sm->jfirst[t] + slot;
         if (job < kCodeJobs) {  // the true lane's codes, walked already: copy them
           const uint32_t e0 = step(tb, f, cls4_of(tb, rb[0]));
           const uint32_t *src = sm->jcodes + job * kLexWords;

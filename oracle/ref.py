@@ -72,12 +72,15 @@ class RefOracle:
         first = bytearray()
 
         def sink(_user, p, nbytes):
-            data = ctypes.string_at(p, nbytes)
+            # a write can be several GB (stdio hands large fwrite calls to the
+            # sink whole): hash it in place, without a bytes copy (ctypes'
+            # string_at takes a C int size)
+            skip = 0
             if len(first) < head:
-                k = min(head - len(first), nbytes)
-                first.extend(data[:k])
-                data = data[k:]
-            h.update(data)
+                skip = min(head - len(first), nbytes)
+                first.extend((ctypes.c_char * skip).from_address(p))
+            if nbytes > skip:
+                h.update((ctypes.c_char * (nbytes - skip)).from_address(p + skip))
             size[0] += nbytes
 
         cb = _SINK(sink)
