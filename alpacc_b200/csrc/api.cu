@@ -338,6 +338,11 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
     CK(cudaMemcpyAsync(&g->d_status->num_tokens, &T, 8, cudaMemcpyHostToDevice, g->stream));
   } else if (lexing) {
     LexArgs a = lex_args(g, d_in, n, lex_tiles);
+    if (g->diag) {
+      TRY(grow(g->diag_cycles, 64));
+      CK(cudaMemsetAsync(g->diag_cycles.p, 0, 64, g->stream));
+      a.phase_cycles = (unsigned long long *)g->diag_cycles.p;
+    }
     a.st1_flag = (unsigned *)(fb + fl.st1_flag);
     a.st2.flags = (unsigned *)(fb + fl.st2_flags);
     if (win) {
@@ -427,6 +432,8 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
   }
   int rc = sync_status(g);
   if (rc == ALPACC_OK && g->h_status->overflow) rc = ALPACC_E_CAPACITY;  // grown and run again by run_device
+  if (g->diag && lexing && cudaMemcpy(g->phase_cycles, g->diag_cycles.p, 64, cudaMemcpyDeviceToHost) != cudaSuccess)
+    cudaGetLastError();
   float ms = 0;
   if (cudaEventElapsedTime(&ms, g->ev0, g->ev1) == cudaSuccess) g->last_ms = ms;
   collect_stages(g);
@@ -570,7 +577,7 @@ void alpacc_gpu_free(alpacc_gpu_grammar *g) {
                     &g->pair_ticket, &g->pst_flags, &g->pst_agg, &g->pst_inc, &g->br, &g->pr, &g->pse_ticket,
                     &g->pse_flags, &g->pse_agg, &g->pse_inc, &g->ch_h0, &g->ch_tc, &g->tile_min,
                     &g->chunk_min, &g->super_key, &g->queue, &g->queue_len, &g->node_prods, &g->node_parents,
-                    &g->token_parents, &g->flags, &g->b_arrays, &g->b_desc, &g->b_status,
+                    &g->token_parents, &g->flags, &g->diag_cycles, &g->b_arrays, &g->b_desc, &g->b_status,
                     &g->b_pack, &g->b_packed};
   for (DevBuf *b : bufs) release(*b);
   if (g->cstream) cudaStreamSynchronize(g->cstream);
@@ -928,13 +935,16 @@ uint64_t alpacc_device_allocations(void) { return alpacc::g_device_allocs.load(s
 
 int alpacc_gpu_counts(const alpacc_gpu_grammar *g, int64_t *vals, int n) {
   if (!g || !vals || !g->h_status) return ALPACC_E_INVALID;
-  const int64_t v[9] = {(int64_t)g->h_status->num_tokens, (int64_t)g->h_status->num_brackets,
-                        (int64_t)g->h_status->num_productions, (int64_t)g->h_status->num_nodes,
-                        (int64_t)g->h_status->scratch[0], (int64_t)g->h_status->scratch[1],
-                        (int64_t)g->h_status->scratch[2], (int64_t)g->h_status->scratch[3],
-                        (int64_t)g->launches};
-  for (int i = 0; i < n && i < 9; i++) vals[i] = v[i];
-  return 9;
+  const int64_t v[17] = {(int64_t)g->h_status->num_tokens, (int64_t)g->h_status->num_brackets,
+                         (int64_t)g->h_status->num_productions, (int64_t)g->h_status->num_nodes,
+                         (int64_t)g->h_status->scratch[0], (int64_t)g->h_status->scratch[1],
+                         (int64_t)g->h_status->scratch[2], (int64_t)g->h_status->scratch[3],
+                         (int64_t)g->launches,
+                         (int64_t)g->phase_cycles[0], (int64_t)g->phase_cycles[1], (int64_t)g->phase_cycles[2],
+                         (int64_t)g->phase_cycles[3], (int64_t)g->phase_cycles[4], (int64_t)g->phase_cycles[5],
+                         (int64_t)g->phase_cycles[6], (int64_t)g->phase_cycles[7]};
+  for (int i = 0; i < n && i < 17; i++) vals[i] = v[i];
+  return 17;
 }
 
 void alpacc_gpu_set_diagnostics(alpacc_gpu_grammar *g, int on) {

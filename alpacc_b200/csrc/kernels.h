@@ -88,6 +88,11 @@ struct LexArgs {
   PairTileState st2;    // (kept-token count, last boundary)
   DeviceStatus *status;
   int diag;             // 1: accumulate diagnostic counters in status->scratch
+  // diagnostics: SM cycles of each barrier-delimited phase summed over tiles
+  // (thread 0's clock): 0 load, 1 pass 1, 2 lane jobs, 3 constant-chunk scan,
+  // 4 start states, 5 pass 2 + masks + count scan, 6 count look-back,
+  // 7 token writes; null when off
+  unsigned long long *phase_cycles;
   const BatchDesc *batch;  // null: one document (in, n, status); else tiles are virtual (lex_tile0)
   // One window of a longer input (chunked lexing): the input continues after
   // byte n, so the token in progress at n is neither emitted nor judged; the

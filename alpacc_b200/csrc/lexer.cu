@@ -307,6 +307,15 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
   const int dead = a.dead;
   const unsigned long long num_tiles = a.num_tiles;
   const unsigned long long tile_end = a.tile_end ? a.tile_end : num_tiles;
+  unsigned long long *pcyc = a.phase_cycles;
+  long long tp = clock64();
+// diagnostics: thread 0 adds the cycles since the previous mark to phase k
+#define LEX_PHASE(k)                                                  \
+  if (pcyc && t == 0) {                                               \
+    const long long now_ = clock64();                                 \
+    atomicAdd(pcyc + (k), (unsigned long long)(now_ - tp));           \
+    tp = now_;                                                        \
+  }
 
   for (unsigned long long round = 0;; ++round) {
     if (round > tile_end - a.tile_begin) {  // every round takes a new ticket: cannot happen
@@ -314,6 +323,7 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
       break;
     }
     __syncthreads();  // tables ready / previous tile fully consumed
+    LEX_PHASE(7);
     if (t == 0) sm->tile = atomicAdd(a.ticket, 1u);
     __syncthreads();
     const unsigned long long tile = a.tile_begin + sm->tile;
@@ -366,6 +376,7 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
     int nb = 0;
     if (g0 >= 0 && g0 < n) nb = (int)min((long long)kLexChunk, n - g0);
     __syncthreads();
+    LEX_PHASE(0);
 
     // ---- pass 1 ----
     int jw = nb, end = -1, conv = -1, kind = kEmpty;
@@ -385,6 +396,7 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
       const int lanes = kind == kOpen ? (int)__ldg(a.img_cnt + sm->c0[t]) : 0;
       int njobs;
       const int jex = block_exclusive_scan<int>(lanes, AddI32(), 0, sm->scan_a, &njobs);
+      LEX_PHASE(1);
       sm->jfirst[t] = (uint16_t)jex;  // non-decreasing over the chunks (at most 256 x 32 jobs)
       __syncthreads();
       for (int job = t; job < njobs; job += kLexThreads) {
@@ -400,6 +412,7 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
       }
     }
     __syncthreads();
+    LEX_PHASE(2);
 
     // ---- resolution: nearest constant chunk before each chunk ----
     const bool is_const = kind == kConst;
@@ -413,6 +426,7 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
       if (t == 0) atomicAdd(&st->scratch[1], (unsigned long long)nconst);
     }
     __syncthreads();
+    LEX_PHASE(3);
     if (ktot >= 0) {
       // the outgoing state does not depend on the incoming one: publish now
       if (t == 0) {
@@ -489,6 +503,7 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
       if (lane == 0) atomicAdd(&st->scratch[2], (unsigned long long)w);
     }
     __syncthreads();
+    LEX_PHASE(4);
     if (t == 0 && !sm->out_published) {
       const int x = eval_chunk(a, sm, kLexThreads - 1, sm->start[kLexThreads - 1]);
       a.st1_state[tile] = (uint8_t)(x < 0 ? 0 : x);
@@ -563,6 +578,7 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
     // ---- (count, last boundary) carry: block scan, then across tiles ----
     int cnt_tot, pos_tot, cnt_ex, pos_ex;
     block_exclusive_scan2(sm->scan_a, sm->scan_b, (int)cnt, (int)lastb, &cnt_ex, &pos_ex, &cnt_tot, &pos_tot);
+    LEX_PHASE(5);
     if (t < kWarp) {
       const Pair64 agg{cnt_tot, pos_tot};
       Pair64 prefix{0, 0};
@@ -582,6 +598,7 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
       }
     }
     __syncthreads();
+    LEX_PHASE(6);
 
     // ---- the kept tokens, straight into the outputs ----
     if (t >= kLexHalo && nb > 0) {
@@ -617,6 +634,8 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
 }
 
 }  // namespace
+
+#undef LEX_PHASE
 
 __global__ void __launch_bounds__(kLexThreads, 5) lex_kernel(LexArgs args) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];

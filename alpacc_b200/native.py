@@ -405,10 +405,13 @@ class Parser:
 
     def counts(self) -> dict:
         """Tokens, brackets, productions, nodes of the last call."""
-        vals = (ctypes.c_int64 * 9)()
-        lib().alpacc_gpu_counts(self._h, vals, 9)
+        vals = (ctypes.c_int64 * 17)()
+        lib().alpacc_gpu_counts(self._h, vals, 17)
         return {"T": vals[0], "B": vals[1], "P": vals[2], "N": vals[3], "lookback_tiles": vals[4],
-                "const_chunks": vals[5], "chain_evals": vals[6], "set_walk_bytes": vals[7], "launches": vals[8]}
+                "const_chunks": vals[5], "chain_evals": vals[6], "set_walk_bytes": vals[7], "launches": vals[8],
+                "lexer_phase_cycles": {k: vals[9 + i] for i, k in enumerate(
+                    ("load", "pass1", "lane_jobs", "const_scan", "start_states", "pass2_masks_scan",
+                     "count_lookback", "token_writes"))}}
 
     def set_diagnostics(self, on: bool):
         lib().alpacc_gpu_set_diagnostics(self._h, 1 if on else 0)

@@ -335,7 +335,10 @@ int alpacc_gpu_stage_ms(const alpacc_gpu_grammar *g, double *out, int n);
    lexer diagnostic counters (collected when diagnostics are on): tiles that
    read their incoming state from the previous tile, constant chunks, chunk
    evaluations chained to find start states, bytes walked as state sets; then
-   the number of kernels the call launched. */
+   the number of kernels the call launched; then (diagnostics on) the SM
+   cycles thread 0 of the lexer's CTAs spent in each phase, summed over tiles:
+   load, pass 1, lane jobs, constant-chunk scan, start states, pass 2 with the
+   masks and the count scan, the count look-back, the token writes. */
 int alpacc_gpu_counts(const alpacc_gpu_grammar *g, int64_t *vals, int n);
 void alpacc_gpu_set_diagnostics(alpacc_gpu_grammar *g, int on);
 /* Number of device allocations (cudaMalloc) this library has made in the
