@@ -129,21 +129,6 @@ int ensure_lex_smem(size_t bytes) {
   return ALPACC_OK;
 }
 
-// pair_kernel may stage its small tables in dynamic shared memory above the
-// default 48 KB per CTA: allow kPairSmemTables once.
-int ensure_pair_smem() {
-  static std::mutex mu;
-  static bool done = false;
-  std::lock_guard<std::mutex> lock(mu);
-  if (done) return ALPACC_OK;
-  if (cudaFuncSetAttribute(pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPairSmemTables) != cudaSuccess) {
-    cudaGetLastError();
-    return ALPACC_E_CUDA;
-  }
-  done = true;
-  return ALPACC_OK;
-}
-
 constexpr uint64_t kPieceTiles = (16u << 20) / kLexData;  // tiles per host-to-device piece (~16 MiB)
 
 // Token arrays of the current host call: copied on cstream once the lexer
@@ -386,8 +371,7 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
     a.ticket = (unsigned *)(fb + fl.pair_ticket);
     a.st.flags = (unsigned *)(fb + fl.pst_flags);
     stage_begin(g, 1);
-    pair_kernel<<<(unsigned)std::min<uint64_t>(pair_tiles, (uint64_t)g->pair_grid), kPairThreads, pair_smem_bytes(g),
-                  g->stream>>>(a);
+    pair_kernel<<<(unsigned)std::min<uint64_t>(pair_tiles, (uint64_t)g->pair_grid), kPairThreads, 0, g->stream>>>(a);
     ++g->launches;
     stage_end(g, 1);
     CK(cudaGetLastError());
@@ -542,9 +526,7 @@ alpacc_gpu_grammar *alpacc_gpu_load(const alpacc_tables *tables, int device, uin
     int per_sm = 0, sms = 0;
     int pair_sm = 0, pse_sm = 0;
     if (lex_occupancy(g, &per_sm) != cudaSuccess ||
-        ensure_pair_smem() != ALPACC_OK ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pair_sm, pair_kernel, kPairThreads, pair_smem_bytes(g)) !=
-            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pair_sm, pair_kernel, kPairThreads, 0) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pse_sm, pse_tile_kernel, kPseThreads, 0) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || per_sm < 1 ||
         pair_sm < 1 || pse_sm < 1) {

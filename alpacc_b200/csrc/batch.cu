@@ -163,8 +163,7 @@ int run_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offset
     PairArgs pa = pair_args(g);
     pa.batch = d_bd;
     pa.status = bd.status;
-    pair_kernel<<<(unsigned)std::min<uint64_t>(pair_ub, (uint64_t)g->pair_grid), kPairThreads, pair_smem_bytes(g),
-                  s>>>(pa);
+    pair_kernel<<<(unsigned)std::min<uint64_t>(pair_ub, (uint64_t)g->pair_grid), kPairThreads, 0, s>>>(pa);
   }
   batch_plan_kernel<<<1, 1024, 0, s>>>(bd, kPlanBrackets, bd.br_tile0, kPseTile);
   batch_plan_kernel<<<1, 1024, 0, s>>>(bd, kPlanParents, bd.pr_tile0, kPseTile);

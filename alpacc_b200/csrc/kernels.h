@@ -110,8 +110,7 @@ __global__ void lex_kernel_wide(LexArgs args);
 constexpr int kPairThreads = 256;
 constexpr int kPairItems = 8;
 constexpr int kPairTile = kPairThreads * kPairItems;
-constexpr int kPairOut = 4096;  // output window of pair_kernel (elements)
-constexpr int kPairSmemTables = 24 * 1024;  // record / stack / production tables staged up to this size
+constexpr int kPairOut = 6144;  // output window of pair_kernel (elements)
 
 struct PairArgs {
   const void *tok_ids;      // lexer output, terminal ids (term_w bytes each)
@@ -127,9 +126,6 @@ struct PairArgs {
   const unsigned long long *rec;  // ss | ps << 24 | nb << 48 | np << 56
   const uint32_t *stacks;   // bit31 left
   const uint32_t *prods;
-  // sizes of rec / stacks / prods; when smem_tables is set they are copied
-  // into the kernel's dynamic shared memory (records, then stacks, then prods)
-  int n_rec, n_stacks, n_prods, smem_tables;
   uint32_t *br_out;         // brackets (capacity br_cap)
   uint32_t *pr_out;         // productions (capacity pr_cap)
   unsigned long long br_cap, pr_cap;

@@ -69,22 +69,8 @@ __global__ void __launch_bounds__(kPairThreads, 5) pair_kernel(PairArgs a) {
   __shared__ __align__(16) uint32_t s_out[kPairOut];     // output window
   const int t = threadIdx.x;
   const int L = a.q + a.k;
-  // records, stack actions and productions: staged in shared memory once per
-  // CTA when they are small, so the per-element gathers stay on chip
-  extern __shared__ __align__(16) unsigned char pair_dyn[];
   const unsigned long long *rec = a.rec;
   const uint32_t *stacks = a.stacks, *prods = a.prods;
-  if (a.smem_tables) {
-    unsigned long long *s_r = reinterpret_cast<unsigned long long *>(pair_dyn);
-    uint32_t *s_s = reinterpret_cast<uint32_t *>(s_r + a.n_rec);
-    uint32_t *s_p = s_s + a.n_stacks;
-    for (int i = t; i < a.n_rec; i += kPairThreads) s_r[i] = __ldg(a.rec + i);
-    for (int i = t; i < a.n_stacks; i += kPairThreads) s_s[i] = __ldg(a.stacks + i);
-    for (int i = t; i < a.n_prods; i += kPairThreads) s_p[i] = __ldg(a.prods + i);
-    rec = s_r;
-    stacks = s_s;
-    prods = s_p;
-  }
   unsigned long long total;
   if (a.batch) {
     total = a.batch->pair_tile0[a.batch->docs];

@@ -66,15 +66,6 @@ inline cudaError_t lex_occupancy(const alpacc_gpu_grammar *g, int *per_sm) {
                    : cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, lex_kernel, kLexThreads, lex_dyn_smem(g));
 }
 
-// Dynamic shared memory of pair_kernel: the record, stack and production
-// tables when they fit kPairSmemTables, else none (they are read from global
-// memory).
-inline size_t pair_smem_bytes(const alpacc_gpu_grammar *g) {
-  const PairTable &pt = g->hg.pairs;
-  const size_t b = pt.rec_ss.size() * 8 + pt.stacks.size() * 4 + pt.prods.size() * 4;
-  return b <= (size_t)kPairSmemTables ? b : 0;
-}
-
 inline PairArgs pair_args(alpacc_gpu_grammar *g) {
   const alpacc_tables &tb = g->hg.t;
   const PairTable &pt = g->hg.pairs;
@@ -95,10 +86,6 @@ inline PairArgs pair_args(alpacc_gpu_grammar *g) {
   a.max_iters = pt.max_iters;
   a.rec = (const unsigned long long *)g->rec.p;
   a.stacks = (const uint32_t *)g->stacks.p;
-  a.n_rec = (int)pt.rec_ss.size();
-  a.n_stacks = (int)pt.stacks.size();
-  a.n_prods = (int)pt.prods.size();
-  a.smem_tables = pair_smem_bytes(g) > 0;
   a.prods = (const uint32_t *)g->prods.p;
   a.br_out = (uint32_t *)g->br.p;
   a.pr_out = (uint32_t *)g->pr.p;
