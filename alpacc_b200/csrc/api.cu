@@ -121,7 +121,10 @@ int ensure_lex_smem(size_t bytes) {
   std::lock_guard<std::mutex> lock(mu);
   if (bytes <= current) return ALPACC_OK;
   if (cudaFuncSetAttribute(lex_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess ||
-      cudaFuncSetAttribute(lex_kernel_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) {
+      cudaFuncSetAttribute(lex_kernel_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess ||
+      cudaFuncSetAttribute(lex_direct_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess ||
+      cudaFuncSetAttribute(lex_direct_kernel_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
+          cudaSuccess) {
     cudaGetLastError();
     return ALPACC_E_CUDA;
   }
@@ -285,6 +288,11 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
   TRY(grow(g->flags, fl.total));
   uint8_t *fb = (uint8_t *)g->flags.p;
   if (lexing) {
+    TRY(grow(g->codes, lex_tiles * (uint64_t)kLexData));
+    TRY(grow(g->tile_cnt, lex_tiles * 4));
+    TRY(grow(g->tile_pos, lex_tiles * 4));
+    TRY(grow(g->tile_off, lex_tiles * 8));
+    TRY(grow(g->tile_prev, lex_tiles * 4));
     TRY(grow(g->st1_state, lex_tiles));
     TRY(grow(g->st1_vec, lex_tiles * (uint64_t)lm.M));
     TRY(grow(g->st2_agg, lex_tiles * 16));
@@ -350,6 +358,8 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
       CK(launch_lex(g, a, grid, g->stream));
       ++g->launches;
     }
+    CK(launch_lex_emit(lex_emit_args(g, a), g->stream));
+    g->launches += 2;
     stage_end(g, 0);
   }
   CK(cudaEventRecord(g->lex_done, g->stream));
@@ -559,7 +569,8 @@ void alpacc_gpu_free(alpacc_gpu_grammar *g) {
                     &g->pair_ticket, &g->pst_flags, &g->pst_agg, &g->pst_inc, &g->br, &g->pr, &g->pse_ticket,
                     &g->pse_flags, &g->pse_agg, &g->pse_inc, &g->ch_h0, &g->ch_tc, &g->tile_min,
                     &g->chunk_min, &g->super_key, &g->queue, &g->queue_len, &g->node_prods, &g->node_parents,
-                    &g->token_parents, &g->flags, &g->diag_cycles, &g->b_arrays, &g->b_desc, &g->b_status,
+                    &g->token_parents, &g->flags, &g->diag_cycles, &g->codes, &g->tile_cnt, &g->tile_pos,
+                    &g->tile_off, &g->tile_prev, &g->b_arrays, &g->b_desc, &g->b_status,
                     &g->b_pack, &g->b_packed};
   for (DevBuf *b : bufs) release(*b);
   if (g->cstream) cudaStreamSynchronize(g->cstream);

@@ -96,6 +96,11 @@ int run_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offset
   BTRY(grow(g->st1_state, std::max<uint64_t>(lex_tiles, 1)));
   BTRY(grow(g->st1_vec, std::max<uint64_t>(lex_tiles, 1) * (uint64_t)lm.M));
   BTRY(grow(g->st2_flags, std::max<uint64_t>(lex_tiles, 1) * 4));
+  BTRY(grow(g->codes, std::max<uint64_t>(lex_tiles, 1) * (uint64_t)kLexData));
+  BTRY(grow(g->tile_cnt, std::max<uint64_t>(lex_tiles, 1) * 4));
+  BTRY(grow(g->tile_pos, std::max<uint64_t>(lex_tiles, 1) * 4));
+  BTRY(grow(g->tile_off, std::max<uint64_t>(lex_tiles, 1) * 8));
+  BTRY(grow(g->tile_prev, std::max<uint64_t>(lex_tiles, 1) * 4));
   BTRY(grow(g->st2_agg, std::max<uint64_t>(lex_tiles, 1) * 16));
   BTRY(grow(g->st2_inc, std::max<uint64_t>(lex_tiles, 1) * 16));
   BTRY(grow(g->tok_ids, T_cap * term_w));
@@ -155,7 +160,8 @@ int run_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offset
     a.batch = d_bd;
     a.status = bd.status;
     BCK(launch_lex(g, a, (unsigned)std::min<uint64_t>(lex_tiles, (uint64_t)g->lex_grid), s));
-    g->launches += 1;
+    BCK(launch_lex_emit(lex_emit_args(g, a), s));
+    g->launches += 3;
   }
   // ---- pairs ----
   batch_plan_kernel<<<1, 1024, 0, s>>>(bd, kPlanPairs, bd.pair_tile0, kPairTile);

@@ -42,6 +42,8 @@ struct DeviceStatus {
   int parse_reject_reason;  // 1 missing pair, 2 bracket mismatch, 3 unbalanced, 4 terminal count
   unsigned long long scratch[4];
   unsigned long long last_boundary;  // last token boundary of the input (single-document lexer)
+  int final_kept;    // the input's last token (ending at byte n) is kept: its terminal in final_term
+  int final_term;
 };
 
 // Upper bound on spin iterations of one wait; with the back-off below this is

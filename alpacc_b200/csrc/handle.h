@@ -102,6 +102,7 @@ struct alpacc_gpu_grammar {
   DevBuf diag_cycles;                          // diagnostics: lexer phase cycles
   unsigned long long phase_cycles[8] = {};     // of the last call
   DevBuf lex_ticket, st1_flag, st1_state, st1_vec, st2_flags, st2_agg, st2_inc;
+  DevBuf codes, tile_cnt, tile_pos, tile_off, tile_prev;  // staged lexer output
   DevBuf tok_ids, tok_starts, tok_lens;
   DevBuf pair_ticket, pst_flags, pst_agg, pst_inc, br, pr;
   DevBuf pse_ticket, pse_flags, pse_agg, pse_inc, ch_h0, ch_tc, tile_min, chunk_min, super_key, queue, queue_len;

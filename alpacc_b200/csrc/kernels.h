@@ -99,12 +99,42 @@ struct LexArgs {
   // window's last boundary is left in status->last_boundary.
   int open_end;
   unsigned long long index_base;  // added to every token start (a window's offset in chunked lexing)
+  // Staged output (lex_kernel, lex_kernel_wide): each tile writes the codes of
+  // its data bytes to codes[tile * kLexData ...] and its (kept-token count,
+  // last boundary) to tile_cnt / tile_pos; lex_scan_kernel and lex_emit_kernel
+  // then write the tokens, so no tile waits for another's count. The direct
+  // kernels (lex_direct_kernel, lex_direct_kernel_wide) chain the counts by
+  // decoupled look-back (st2) and write the tokens themselves.
+  uint8_t *codes;
+  uint32_t *tile_cnt, *tile_pos;
 };
 
 // Machines of at most 64 states (one 64-bit state set in pass 1), and of up
-// to 255 states (four words).
+// to 255 states (four words); staged and direct output.
 __global__ void lex_kernel(LexArgs args);
 __global__ void lex_kernel_wide(LexArgs args);
+__global__ void lex_direct_kernel(LexArgs args);
+__global__ void lex_direct_kernel_wide(LexArgs args);
+
+struct LexEmitArgs {
+  const uint8_t *codes;             // [tiles * kLexData] codes of every data byte (lex_kernel)
+  unsigned long long n;
+  unsigned long long num_tiles;
+  const uint32_t *tile_cnt, *tile_pos;
+  unsigned long long *tile_off;     // exclusive prefix of tile_cnt (token index, in the document's region)
+  uint32_t *tile_prev;              // last boundary before each tile (0: none)
+  void *tok_ids, *tok_starts, *tok_lens;
+  int term_w, idx_w, len_w;
+  unsigned long long len_max;
+  unsigned long long index_base;
+  int open_end;
+  DeviceStatus *status;
+  const BatchDesc *batch;           // null: one document; else counts restart at each document's first tile
+};
+
+constexpr int kLexScanThreads = 1024;
+__global__ void lex_scan_kernel(LexEmitArgs args);  // one CTA
+__global__ void lex_emit_kernel(LexEmitArgs args);  // CTAs over tiles
 
 // ---- pair lookup / stack-action expansion: 256 threads x 8 positions ----
 constexpr int kPairThreads = 256;

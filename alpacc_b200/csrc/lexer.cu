@@ -33,10 +33,15 @@
 //   its true start, writing their codes; an open chunk copies its true lane's
 //   codes (or walks the chunk again when its lanes had no code slots), a
 //   partial chunk (the input's last) is walked whole.
-// Output: boundary masks from the code words, a (token count, last boundary)
-//   block scan, a decoupled look-back over tiles (Merrill & Garland 2016) taken
-//   last, and the kept tokens written straight into the final
-//   structure-of-arrays outputs with the length_t check of lexer.c:68-72.
+// Output, staged (lex_kernel): each tile writes the codes of its data bytes
+//   (16-byte stores from shared memory) and its (kept-token count, last
+//   boundary); lex_scan_kernel scans the tile totals and lex_emit_kernel turns
+//   each tile's codes into tokens at their final places, with the length_t
+//   check of lexer.c:68-72. No tile waits for another tile's count.
+// Output, direct (lex_direct_kernel, for the allocation-free entry point):
+//   boundary masks from the code words, a (token count, last boundary) block
+//   scan, a decoupled look-back over tiles (Merrill & Garland 2016) and the
+//   kept tokens written by the kernel itself.
 //
 // Reference equivalents: backends/cuda/lexer.cu:437-760 (``lexer`` kernel) and
 // backends/cuda/scan.cu:181-400 (look-back).
@@ -287,7 +292,7 @@ __device__ __forceinline__ void walk_lane(const LexArgs &a, const Tab &tb, LexSm
   sm->lend[l * kLexThreads + tc] = (uint8_t)state_of(tb, f);
 }
 
-template <int W>
+template <int W, bool kStaged>
 __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_smem, LexSmem *sm) {
   const int t = threadIdx.x;
   const int lane = t & 31;
@@ -579,6 +584,25 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
     int cnt_tot, pos_tot, cnt_ex, pos_ex;
     block_exclusive_scan2(sm->scan_a, sm->scan_b, (int)cnt, (int)lastb, &cnt_ex, &pos_ex, &cnt_tot, &pos_tot);
     LEX_PHASE(5);
+    if (kStaged) {
+      // the tile's totals and the codes of its data bytes, for the scan and
+      // emit kernels (the block scan above ended with a barrier: every row
+      // holds its final codes)
+      if (t == 0) {
+        a.tile_cnt[tile] = (uint32_t)cnt_tot;
+        a.tile_pos[tile] = (uint32_t)pos_tot;
+      }
+      if (final_kept) {  // one chunk of the document holds its last byte
+        st->final_term = sm->sterm[x_end];
+        st->final_kept = 1;
+      }
+      uint4 *dst = reinterpret_cast<uint4 *>(a.codes + tile * (unsigned long long)kLexData);
+      const uint4 *src = reinterpret_cast<const uint4 *>(reinterpret_cast<const uint8_t *>(sm->bytes) +
+                                                         kLexHalo * kLexChunk);
+      for (int v = t; v < kLexData / 16; v += kLexThreads) dst[v] = src[v];
+      LEX_PHASE(7);
+      continue;
+    }
     if (t < kWarp) {
       const Pair64 agg{cnt_tot, pos_tot};
       Pair64 prefix{0, 0};
@@ -640,13 +664,178 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
 __global__ void __launch_bounds__(kLexThreads, 5) lex_kernel(LexArgs args) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   __shared__ __align__(16) LexSmem sm;
-  lex_body<1>(args, dyn_smem, &sm);
+  lex_body<1, true>(args, dyn_smem, &sm);
 }
 
 __global__ void __launch_bounds__(kLexThreads, 5) lex_kernel_wide(LexArgs args) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   __shared__ __align__(16) LexSmem sm;
-  lex_body<4>(args, dyn_smem, &sm);
+  lex_body<4, true>(args, dyn_smem, &sm);
+}
+
+__global__ void __launch_bounds__(kLexThreads, 5) lex_direct_kernel(LexArgs args) {
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  __shared__ __align__(16) LexSmem sm;
+  lex_body<1, false>(args, dyn_smem, &sm);
+}
+
+__global__ void __launch_bounds__(kLexThreads, 5) lex_direct_kernel_wide(LexArgs args) {
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  __shared__ __align__(16) LexSmem sm;
+  lex_body<4, false>(args, dyn_smem, &sm);
+}
+
+// ---------------------------------------------------------------------------
+// Scan and token writes of the staged lexer
+// ---------------------------------------------------------------------------
+
+namespace {
+
+// (count, last boundary) with segment starts: the prefix restarts at a batch
+// document's first tile (flag kSeg in the position word).
+constexpr long long kSeg = 1ll << 62;
+
+struct SegCntPosOp {
+  __device__ Pair64 operator()(Pair64 l, Pair64 r) const {
+    if (r.b & kSeg) return r;
+    const long long lp = l.b & ~kSeg;
+    return Pair64{l.a + r.a, (lp > r.b ? lp : r.b) | (l.b & kSeg)};
+  }
+};
+
+}  // namespace
+
+// Exclusive (count, last boundary) prefix over the tiles, by one CTA: each
+// tile's first token index (in its document's token region) and the last
+// boundary before it; each document's token count and last boundary.
+__global__ void __launch_bounds__(kLexScanThreads) lex_scan_kernel(LexEmitArgs a) {
+  __shared__ Pair64 tmp[kLexScanThreads / 32];
+  const int t = threadIdx.x;
+  constexpr int kPer = 16;
+  const BatchDesc *bd = a.batch;
+  auto seg_doc = [&](unsigned long long i, bool *start) -> int {
+    if (!bd) {
+      *start = i == 0;
+      return 0;
+    }
+    const int d = batch_doc(bd->lex_tile0, bd->docs, i);
+    *start = bd->lex_tile0[d] == i;
+    return d;
+  };
+  Pair64 carry{0, 0};
+  for (unsigned long long base = 0; base < a.num_tiles; base += (unsigned long long)kLexScanThreads * kPer) {
+    const unsigned long long i0 = base + (unsigned long long)t * kPer;
+    Pair64 loc{0, 0};
+    for (int k = 0; k < kPer && i0 + k < a.num_tiles; ++k) {
+      bool start;
+      seg_doc(i0 + k, &start);
+      const Pair64 v{(long long)a.tile_cnt[i0 + k], (long long)a.tile_pos[i0 + k] | (start ? kSeg : 0)};
+      loc = SegCntPosOp()(loc, v);
+    }
+    Pair64 tot;
+    const Pair64 ex = block_exclusive_scan_pair(loc, SegCntPosOp(), Pair64{0, 0}, tmp, &tot);
+    Pair64 run = SegCntPosOp()(carry, ex);
+    for (int k = 0; k < kPer && i0 + k < a.num_tiles; ++k) {
+      bool start;
+      const int d = seg_doc(i0 + k, &start);
+      if (start) run = Pair64{0, 0};
+      const unsigned long long region = bd ? bd->tok_off[d] : 0;
+      a.tile_off[i0 + k] = region + (unsigned long long)run.a;
+      a.tile_prev[i0 + k] = (uint32_t)(run.b & ~kSeg);
+      const long long rp = run.b & ~kSeg, tp = (long long)a.tile_pos[i0 + k];
+      run = Pair64{run.a + (long long)a.tile_cnt[i0 + k], rp > tp ? rp : tp};
+      if (bd && i0 + k + 1 == bd->lex_tile0[d + 1]) {  // the document's last tile
+        bd->status[d].num_tokens = (unsigned long long)run.a;
+        bd->status[d].last_boundary = (unsigned long long)run.b;
+      }
+    }
+    carry = SegCntPosOp()(carry, tot);
+  }
+  if (t == 0 && !bd) {
+    a.status->num_tokens = (unsigned long long)carry.a;
+    a.status->last_boundary = (unsigned long long)(carry.b & ~kSeg);
+  }
+}
+
+// The tokens of each tile from its codes: per 60-byte chunk the boundary and
+// kept masks, a block scan of (count, last boundary) on top of the tile's
+// prefix, then each chunk's kept tokens written at their final places with
+// the length_t check (lexer.c:68-72); the input's last token (kept, ending at
+// byte n) after the last chunk's.
+__global__ void __launch_bounds__(256) lex_emit_kernel(LexEmitArgs a) {
+  __shared__ __align__(16) uint32_t rows[kLexThreads * kLexWords];
+  __shared__ int sa[8], sb[8];
+  const int t = threadIdx.x;
+  constexpr int kChunks = kLexThreads - kLexHalo;  // data chunks per tile
+  for (unsigned long long tile = blockIdx.x; tile < a.num_tiles; tile += gridDim.x) {
+    long long n = (long long)a.n;
+    unsigned long long lt = tile;
+    DeviceStatus *st = a.status;
+    if (a.batch) {
+      const int d = batch_doc(a.batch->lex_tile0, a.batch->docs, tile);
+      lt = tile - a.batch->lex_tile0[d];
+      n = (long long)a.batch->n[d];
+      st = a.batch->status + d;
+    }
+    __syncthreads();  // the previous tile's rows are consumed
+    const uint4 *src = reinterpret_cast<const uint4 *>(a.codes + tile * (unsigned long long)kLexData);
+    for (int v = t; v < kLexData / 16; v += kLexThreads) reinterpret_cast<uint4 *>(rows)[v] = src[v];
+    __syncthreads();
+    const long long g0 = (long long)lt * kLexData + (long long)t * kLexChunk;
+    int nb = 0;
+    if (t < kChunks && g0 < n) nb = (int)min((long long)kLexChunk, n - g0);
+    const uint32_t *row = rows + t * kLexWords;
+    const uint8_t *rb = reinterpret_cast<const uint8_t *>(row);
+    unsigned long long bmask = 0, kmask = 0;
+    if (nb > 0) {
+#pragma unroll
+      for (int w = 0; w < kLexWords; ++w) {
+        const uint32_t cw = row[w];
+        bmask |= (unsigned long long)movemask4(nonzero_bytes(~cw)) << (4 * w);
+        kmask |= (unsigned long long)movemask4(nonzero_bytes(~(cw | 0x01010101u))) << (4 * w);
+      }
+      if (nb < 64) {
+        bmask &= (1ull << nb) - 1;
+        kmask &= (1ull << nb) - 1;
+      }
+    }
+    const bool last = nb > 0 && g0 + nb == n;  // holds the input's last byte
+    const bool final_kept = last && !a.open_end && st->final_kept;
+    const int cnt = __popcll(kmask) + (final_kept ? 1 : 0);
+    const int lastb = bmask ? (int)(g0 + 63 - __clzll((long long)bmask)) : 0;
+    int cnt_ex, pos_ex, cnt_tot, pos_tot;
+    block_exclusive_scan2(sa, sb, cnt, lastb, &cnt_ex, &pos_ex, &cnt_tot, &pos_tot);
+    if (nb > 0) {
+      unsigned long long out = a.tile_off[tile] + (unsigned long long)cnt_ex;
+      const long long tp = (long long)a.tile_prev[tile];
+      long long prev = tp > pos_ex ? tp : pos_ex;  // 0: the token starts at byte 0
+      const unsigned long long len_max = a.len_max;
+      const unsigned long long base = a.index_base;
+      bool too_long = false;
+      for (unsigned long long m = bmask; m; m &= m - 1) {
+        const int j = __ffsll((long long)m) - 1;
+        const long long p = g0 + j;
+        const uint32_t code = rb[j];
+        if (code < kIgnored) {
+          const unsigned long long len = (unsigned long long)(p - prev);
+          too_long |= len > len_max;
+          store_uint(a.tok_ids, out, a.term_w, code);
+          store_uint(a.tok_starts, out, a.idx_w, base + (unsigned long long)prev);
+          store_uint(a.tok_lens, out, a.len_w, len);
+          ++out;
+        }
+        prev = p;
+      }
+      if (final_kept) {
+        const unsigned long long len = (unsigned long long)(n - prev);
+        too_long |= len > len_max;
+        store_uint(a.tok_ids, out, a.term_w, (unsigned long long)st->final_term);
+        store_uint(a.tok_starts, out, a.idx_w, base + (unsigned long long)prev);
+        store_uint(a.tok_lens, out, a.len_w, len);
+      }
+      if (too_long) record_reject(st, &st->lex_reject_reason, 3);
+    }
+  }
 }
 
 }  // namespace alpacc

@@ -144,7 +144,7 @@ int lex_noalloc_on_device(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n
   a.status = status;
   a.diag = 0;
   const unsigned grid = (unsigned)(tiles < (unsigned long long)g->lex_grid ? tiles : (unsigned long long)g->lex_grid);
-  if (launch_lex(g, a, grid, g->stream) != cudaSuccess) return ALPACC_E_CUDA;
+  if (launch_lex_direct(g, a, grid, g->stream) != cudaSuccess) return ALPACC_E_CUDA;
   DeviceStatus h;
   if (cudaMemcpyAsync(&h, status, sizeof h, cudaMemcpyDeviceToHost, g->stream) != cudaSuccess ||
       cudaStreamSynchronize(g->stream) != cudaSuccess) {

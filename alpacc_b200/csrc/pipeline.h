@@ -49,13 +49,54 @@ inline LexArgs lex_args(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, 
                         (unsigned long long *)g->st2_inc.p};
   a.status = g->d_status;
   a.diag = g->diag;
+  a.codes = (uint8_t *)g->codes.p;
+  a.tile_cnt = (uint32_t *)g->tile_cnt.p;
+  a.tile_pos = (uint32_t *)g->tile_pos.p;
   return a;
 }
 
-// The lexer kernel for this handle's machine.
+// The staged lexer kernel for this handle's machine (codes and tile totals).
 inline cudaError_t launch_lex(const alpacc_gpu_grammar *g, const LexArgs &a, unsigned grid, cudaStream_t s) {
   if (g->lex_w4) lex_kernel_wide<<<grid, kLexThreads, lex_dyn_smem(g), s>>>(a);
   else lex_kernel<<<grid, kLexThreads, lex_dyn_smem(g), s>>>(a);
+  return cudaGetLastError();
+}
+
+// The direct lexer kernel (tokens written by the kernel itself).
+inline cudaError_t launch_lex_direct(const alpacc_gpu_grammar *g, const LexArgs &a, unsigned grid, cudaStream_t s) {
+  if (g->lex_w4) lex_direct_kernel_wide<<<grid, kLexThreads, lex_dyn_smem(g), s>>>(a);
+  else lex_direct_kernel<<<grid, kLexThreads, lex_dyn_smem(g), s>>>(a);
+  return cudaGetLastError();
+}
+
+// Arguments of the scan and emit kernels of the staged lexer.
+inline LexEmitArgs lex_emit_args(const alpacc_gpu_grammar *g, const LexArgs &a) {
+  LexEmitArgs e{};
+  e.codes = a.codes;
+  e.n = a.n;
+  e.num_tiles = a.num_tiles;
+  e.tile_cnt = a.tile_cnt;
+  e.tile_pos = a.tile_pos;
+  e.tile_off = (unsigned long long *)g->tile_off.p;
+  e.tile_prev = (uint32_t *)g->tile_prev.p;
+  e.tok_ids = a.tok_ids;
+  e.tok_starts = a.tok_starts;
+  e.tok_lens = a.tok_lens;
+  e.term_w = a.term_w;
+  e.idx_w = a.idx_w;
+  e.len_w = a.len_w;
+  e.len_max = a.len_max;
+  e.index_base = a.index_base;
+  e.open_end = a.open_end;
+  e.status = a.status;
+  e.batch = a.batch;
+  return e;
+}
+
+// The scan and emit kernels after the staged lexer's launches.
+inline cudaError_t launch_lex_emit(const LexEmitArgs &e, cudaStream_t s) {
+  lex_scan_kernel<<<1, kLexScanThreads, 0, s>>>(e);
+  lex_emit_kernel<<<(unsigned)std::min<unsigned long long>(e.num_tiles, 148ull * 8), 256, 0, s>>>(e);
   return cudaGetLastError();
 }
 
