@@ -54,7 +54,20 @@ int upload_tables(alpacc_gpu_grammar *g) {
   g->cp_shift = lt.shift;
   g->swz = lt.swz;
   g->wide_cls = lt.wide_cls;
-  g->lex_w4 = lm.M > 64 ? 1 : 0;
+  // ALPACC_LEX_WINDOW=sets walks windows as explicit state sets even when the
+  // window machine exists (tests run that kernel on small machines too)
+  const char *wv = std::getenv("ALPACC_LEX_WINDOW");
+  const bool force_sets = wv && std::strcmp(wv, "sets") == 0;
+  if (!lt.ps_tab.empty() && !force_sets) {
+    g->lex_variant = lm.M > 64 ? 1 : 0;
+    g->ps_words = (int)lt.ps_tab.size();
+    g->ps_full = lt.ps_full;
+    TRY(upload(g->lex_ps, lt.ps_tab));
+    TRY(upload(g->lex_psmask, lt.ps_mask));
+  } else {
+    g->lex_variant = 2;
+    g->ps_words = 0;
+  }
   if (g->wide_cls) {
     TRY(upload(g->lex_cls4, lt.cls4));
   } else {
@@ -62,10 +75,8 @@ int upload_tables(alpacc_gpu_grammar *g) {
     TRY(upload(g->lex_cls4, c4));
   }
   TRY(upload(g->lex_tab, lt.tab));
-  TRY(upload(g->lane_of, lm.lane_of));
   TRY(upload(g->img, lm.img));
   TRY(upload(g->img_cnt, lm.img_cnt));
-  if (!lm.img2.empty()) TRY(upload(g->img2, lm.img2));
   TRY(upload(g->sterm, lm.term));
   TRY(upload(g->sflags, lm.flags));
   return g->hg.parts == ALPACC_PARTS_LEXER ? ALPACC_OK : upload_pairs(g);
@@ -120,14 +131,12 @@ int ensure_lex_smem(size_t bytes) {
   static size_t current = 0;
   std::lock_guard<std::mutex> lock(mu);
   if (bytes <= current) return ALPACC_OK;
-  if (cudaFuncSetAttribute(lex_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess ||
-      cudaFuncSetAttribute(lex_kernel_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess ||
-      cudaFuncSetAttribute(lex_direct_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess ||
-      cudaFuncSetAttribute(lex_direct_kernel_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
-          cudaSuccess) {
-    cudaGetLastError();
-    return ALPACC_E_CUDA;
-  }
+  for (auto k : {lex_kernel, lex_kernel_wide, lex_kernel_sets, lex_direct_kernel, lex_direct_kernel_wide,
+                 lex_direct_kernel_sets})
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return ALPACC_E_CUDA;
+    }
   current = bytes;
   return ALPACC_OK;
 }
@@ -215,7 +224,7 @@ struct LexWindow {
 // buffer, zeroed by one memset per call (byte offsets, 16-byte aligned).
 struct FlagLayout {
   size_t lex_ticket = 0, st1_flag = 0, st2_flags = 0, pair_ticket = 0, pst_flags = 0;
-  size_t pse_ticket[2] = {}, pse_flags[2] = {}, queue_len[2] = {}, super_key[2] = {};
+  size_t pse_ticket[2] = {}, pse_flags[2] = {}, super_key[2] = {};
   size_t total = 0;
   size_t take(size_t bytes) {
     const size_t off = total;
@@ -282,7 +291,6 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
   for (int w = 0; w < 2; ++w) {
     fl.pse_ticket[w] = fl.take(16);
     fl.pse_flags[w] = fl.take(parsing ? pse_tiles * 4 : 0);
-    fl.queue_len[w] = fl.take(16);
     fl.super_key[w] = fl.take(parsing ? super_n * 4 : 0);
   }
   TRY(grow(g->flags, fl.total));
@@ -311,11 +319,8 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
     TRY(grow(g->pr, pr_cap * 4));
     TRY(grow(g->pse_agg, pse_tiles * 16));
     TRY(grow(g->pse_inc, pse_tiles * 16));
-    TRY(grow(g->ch_h0, pse_tiles * kPseThreads * 4));
-    TRY(grow(g->ch_tc, pse_tiles * kPseThreads * 4));
-    TRY(grow(g->chunk_min, pse_tiles * kPseThreads * 4));
     TRY(grow(g->tile_min, pse_tiles * 4));
-    TRY(grow(g->queue, e_cap * 8));
+    TRY(grow(g->pse_regions, pse_region_bytes(pse_tiles)));
     TRY(grow(g->node_prods, std::max<uint64_t>(pr_cap, 1) * prod_w));
     TRY(grow(g->node_parents, std::max<uint64_t>(pr_cap, 1) * idx_w));
     TRY(grow(g->token_parents, std::max<uint64_t>(T_ub, 1) * idx_w));
@@ -389,11 +394,11 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
     // ------- depth walks (the parent walk also writes the compacted tree) -------
     const int walks = mode == kRunParse ? 1 : 2;  // the parser-mode result has no tree
     for (int walk = 0; walk < walks; ++walk) {
-      PseArgs pa = pse_args(g, walk, e_cap);
+      PseArgs pa = pse_args(g, walk, pse_tiles);
       pa.elem_cap = walk == kPseBrackets ? br_cap : pr_cap;
       pa.ticket = (unsigned *)(fb + fl.pse_ticket[walk]);
+      pa.resolve_ticket = pa.ticket + 1;
       pa.st.flags = (unsigned *)(fb + fl.pse_flags[walk]);
-      pa.queue_len = (unsigned long long *)(fb + fl.queue_len[walk]);
       pa.super_key = (uint32_t *)(fb + fl.super_key[walk]);
       const uint64_t tiles = (pa.elem_cap + kPseTile - 1) / kPseTile;
       stage_begin(g, 2 + 2 * walk);
@@ -562,13 +567,13 @@ void alpacc_gpu_free(alpacc_gpu_grammar *g) {
   if (!g) return;
   cudaSetDevice(g->device);
   if (g->stream) cudaStreamSynchronize(g->stream);
-  DevBuf *bufs[] = {&g->lex_tab, &g->lex_cls4, &g->lane_of, &g->img, &g->img_cnt, &g->img2, &g->sterm, &g->sflags,
+  DevBuf *bufs[] = {&g->lex_tab, &g->lex_cls4, &g->lex_ps, &g->lex_psmask, &g->img, &g->img_cnt, &g->sterm, &g->sflags,
                     &g->dense, &g->ht_key, &g->ht_rec, &g->rec, &g->stacks, &g->prods,
                     &g->arity, &g->is_term, &g->in, &g->lex_ticket, &g->st1_flag, &g->st1_state, &g->st1_vec,
                     &g->st2_flags, &g->st2_agg, &g->st2_inc, &g->tok_ids, &g->tok_starts, &g->tok_lens,
                     &g->pair_ticket, &g->pst_flags, &g->pst_agg, &g->pst_inc, &g->br, &g->pr, &g->pse_ticket,
-                    &g->pse_flags, &g->pse_agg, &g->pse_inc, &g->ch_h0, &g->ch_tc, &g->tile_min,
-                    &g->chunk_min, &g->super_key, &g->queue, &g->queue_len, &g->node_prods, &g->node_parents,
+                    &g->pse_flags, &g->pse_agg, &g->pse_inc, &g->tile_min, &g->super_key, &g->pse_regions,
+                    &g->node_prods, &g->node_parents,
                     &g->token_parents, &g->flags, &g->diag_cycles, &g->codes, &g->tile_cnt, &g->tile_pos,
                     &g->tile_off, &g->tile_prev, &g->b_arrays, &g->b_desc, &g->b_status,
                     &g->b_pack, &g->b_packed};

@@ -20,6 +20,7 @@
 #include "handle.h"
 #include "kernels.h"
 #include "pipeline.h"
+#include "scratch.h"
 
 using namespace alpacc;
 
@@ -49,11 +50,93 @@ __global__ void pack_ranges_kernel(const uint8_t *src, uint8_t *dst, const unsig
 }
 
 
+}  // namespace
+
+namespace alpacc {
+
+void BatchSizes::add(const alpacc_gpu_grammar *g, uint64_t n) {
+  const uint64_t max_br = (uint64_t)std::max(g->hg.pairs.max_br, 1), max_pr = (uint64_t)std::max(g->hg.pairs.max_pr, 1);
+  docs += 1;
+  bytes += n;
+  tokens += n + 1;
+  brackets += (n + 3) * max_br;
+  productions += (n + 3) * max_pr;
+  lex_tiles += (n + kLexData - 1) / kLexData;
+  pair_tiles += (n + 3 + kPairTile - 1) / kPairTile;
+  br_tiles += ((n + 3) * max_br + kPseTile - 1) / kPseTile;
+  pr_tiles += ((n + 3) * max_pr + kPseTile - 1) / kPseTile;
+}
+
+int batch_needs(alpacc_gpu_grammar *g, const BatchSizes &z, BufNeed *out) {
+  const alpacc_tables &tb = g->hg.t;
+  const uint64_t D = z.docs, lt = std::max<uint64_t>(z.lex_tiles, 1);
+  const uint64_t walk = std::max<uint64_t>(std::max(z.br_tiles, z.pr_tiles), 1);
+  const uint64_t words = 2 * D + 7 * (D + 1);
+  const uint64_t T = z.tokens, B = z.brackets, P = z.productions;
+  const uint64_t tw = tb.terminal_size, iw = tb.index_size, lw = tb.length_size, pw = tb.production_size;
+  const BufNeed v[] = {
+      {&g->b_arrays, words * 8}, {&g->b_desc, sizeof(BatchDesc)}, {&g->b_status, D * sizeof(DeviceStatus)},
+      {&g->in, z.bytes + 16}, {&g->lex_ticket, 16}, {&g->st1_flag, lt * 4}, {&g->st1_state, lt},
+      {&g->st1_vec, lt * (uint64_t)g->hg.lex.M}, {&g->st2_flags, lt * 4}, {&g->codes, lt * (uint64_t)kLexData},
+      {&g->tile_cnt, lt * 4}, {&g->tile_pos, lt * 4}, {&g->tile_off, lt * 8}, {&g->tile_prev, lt * 4},
+      {&g->st2_agg, lt * 16}, {&g->st2_inc, lt * 16}, {&g->tok_ids, T * tw}, {&g->tok_starts, T * iw},
+      {&g->tok_lens, T * lw}, {&g->pair_ticket, 16}, {&g->pst_flags, z.pair_tiles * 4},
+      {&g->pst_agg, z.pair_tiles * 16}, {&g->pst_inc, z.pair_tiles * 16}, {&g->br, B * 4}, {&g->pr, P * 4},
+      {&g->pse_ticket, 16}, {&g->pse_flags, walk * 4}, {&g->pse_agg, walk * 16}, {&g->pse_inc, walk * 16},
+      {&g->tile_min, walk * 4}, {&g->super_key, ((walk >> kPseSuperShift) + 1) * 4},
+      {&g->pse_regions, pse_region_bytes(walk)}, {&g->node_prods, P * pw}, {&g->node_parents, P * iw},
+      {&g->token_parents, T * iw},
+      // result packing: at most 6 ranges per document and every array packed
+      {&g->b_pack, std::max<uint64_t>(18 * D, 3) * 8},
+      {&g->b_packed, T * (tw + iw + lw + iw) + P * (pw + iw) + 6 * 16}};
+  constexpr int k = (int)(sizeof v / sizeof v[0]);
+  static_assert(k <= kBatchBufs, "batch buffer list");
+  for (int i = 0; i < k; i++) out[i] = BufNeed{v[i].buf, std::max<uint64_t>(v[i].bytes, 256)};
+  return k;
+}
+
+uint64_t batch_scratch_bytes(alpacc_gpu_grammar *g, const BatchSizes &z) {
+  BufNeed need[kBatchBufs];
+  const int k = batch_needs(g, z, need);
+  uint64_t sum = 0;
+  for (int i = 0; i < k; i++) sum += need[i].bytes;
+  return sum;
+}
+
+uint64_t fit_batch_scratch(alpacc_gpu_grammar *g, const BatchSizes &z, uint64_t budget) {
+  BufNeed need[kBatchBufs];
+  const int k = batch_needs(g, z, need);
+  uint64_t held = 0;
+  for (int i = 0; i < k; i++) held += std::max<uint64_t>(need[i].buf->cap, need[i].bytes);
+  if (held > budget) {
+    held = 0;
+    for (int i = 0; i < k; i++) {
+      if (need[i].buf->cap > need[i].bytes) {
+        if (g->stream) cudaStreamSynchronize(g->stream);
+        release(*need[i].buf);
+      }
+      held += need[i].bytes;
+    }
+  }
+  return held;
+}
+
+uint64_t batch_scratch_held(alpacc_gpu_grammar *g) {
+  BufNeed need[kBatchBufs];
+  const int k = batch_needs(g, BatchSizes{}, need);
+  uint64_t held = 0;
+  for (int i = 0; i < k; i++) held += need[i].buf->cap;
+  return held;
+}
+
+}  // namespace alpacc
+
+namespace {
+
 int run_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offsets, uint32_t count,
               alpacc_result *outs) {
   const HostGrammar &hg = g->hg;
   const alpacc_tables &tb = hg.t;
-  const LexerMachine &lm = hg.lex;
   const PairTable &pt = hg.pairs;
   const int D = (int)count;
   const uint64_t base = (uint64_t)offsets[0];
@@ -67,7 +150,7 @@ int run_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offset
   std::vector<unsigned long long> h(words, 0);
   unsigned long long *in_off = h.data(), *nd = in_off + D, *tok_off = nd + D, *br_off = tok_off + D + 1,
                      *pr_off = br_off + D + 1, *lex_tile0 = pr_off + D + 1;
-  uint64_t pair_ub = 0, br_ub = 0, pr_ub = 0;
+  BatchSizes z;
   for (int d = 0; d < D; d++) {
     const uint64_t n = (uint64_t)(offsets[d + 1] - offsets[d]);
     in_off[d] = (uint64_t)offsets[d] - base;
@@ -76,57 +159,21 @@ int run_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offset
     br_off[d + 1] = br_off[d] + (n + 3) * max_br;
     pr_off[d + 1] = pr_off[d] + (n + 3) * max_pr;
     lex_tile0[d + 1] = lex_tile0[d] + (n + kLexData - 1) / kLexData;
-    pair_ub += (n + 3 + kPairTile - 1) / kPairTile;
-    br_ub += ((n + 3) * max_br + kPseTile - 1) / kPseTile;
-    pr_ub += ((n + 3) * max_pr + kPseTile - 1) / kPseTile;
+    z.add(g, n);
   }
   const uint64_t lex_tiles = lex_tile0[D];
+  const uint64_t pair_ub = z.pair_tiles, br_ub = z.br_tiles, pr_ub = z.pr_tiles;
   const uint64_t walk_ub = std::max<uint64_t>(std::max(br_ub, pr_ub), 1);
-  const uint64_t T_cap = tok_off[D], B_cap = br_off[D], P_cap = pr_off[D];
   const int term_w = (int)tb.terminal_size, idx_w = (int)tb.index_size, len_w = (int)tb.length_size;
   const int prod_w = (int)tb.production_size;
 
-  // ---- device buffers ----
-  BTRY(grow(g->b_arrays, words * 8));
-  BTRY(grow(g->b_desc, sizeof(BatchDesc)));
-  BTRY(grow(g->b_status, (size_t)D * sizeof(DeviceStatus)));
-  BTRY(grow(g->in, total + 16));
-  BTRY(grow(g->lex_ticket, 16));
-  BTRY(grow(g->st1_flag, std::max<uint64_t>(lex_tiles, 1) * 4));
-  BTRY(grow(g->st1_state, std::max<uint64_t>(lex_tiles, 1)));
-  BTRY(grow(g->st1_vec, std::max<uint64_t>(lex_tiles, 1) * (uint64_t)lm.M));
-  BTRY(grow(g->st2_flags, std::max<uint64_t>(lex_tiles, 1) * 4));
-  BTRY(grow(g->codes, std::max<uint64_t>(lex_tiles, 1) * (uint64_t)kLexData));
-  BTRY(grow(g->tile_cnt, std::max<uint64_t>(lex_tiles, 1) * 4));
-  BTRY(grow(g->tile_pos, std::max<uint64_t>(lex_tiles, 1) * 4));
-  BTRY(grow(g->tile_off, std::max<uint64_t>(lex_tiles, 1) * 8));
-  BTRY(grow(g->tile_prev, std::max<uint64_t>(lex_tiles, 1) * 4));
-  BTRY(grow(g->st2_agg, std::max<uint64_t>(lex_tiles, 1) * 16));
-  BTRY(grow(g->st2_inc, std::max<uint64_t>(lex_tiles, 1) * 16));
-  BTRY(grow(g->tok_ids, T_cap * term_w));
-  BTRY(grow(g->tok_starts, T_cap * idx_w));
-  BTRY(grow(g->tok_lens, T_cap * len_w));
-  BTRY(grow(g->pair_ticket, 16));
-  BTRY(grow(g->pst_flags, pair_ub * 4));
-  BTRY(grow(g->pst_agg, pair_ub * 16));
-  BTRY(grow(g->pst_inc, pair_ub * 16));
-  BTRY(grow(g->br, B_cap * 4));
-  BTRY(grow(g->pr, P_cap * 4));
-  BTRY(grow(g->pse_ticket, 16));
-  BTRY(grow(g->pse_flags, walk_ub * 4));
-  BTRY(grow(g->pse_agg, walk_ub * 16));
-  BTRY(grow(g->pse_inc, walk_ub * 16));
-  BTRY(grow(g->ch_h0, walk_ub * kPseThreads * 4));
-  BTRY(grow(g->ch_tc, walk_ub * kPseThreads * 4));
-  BTRY(grow(g->tile_min, walk_ub * 4));
-  BTRY(grow(g->chunk_min, walk_ub * kPseThreads * 4));
-  BTRY(grow(g->super_key, ((walk_ub >> kPseSuperShift) + 1) * 4));
-  const uint64_t qcap = std::max(B_cap, P_cap);
-  BTRY(grow(g->queue, qcap * 8));
-  BTRY(grow(g->queue_len, 16));
-  BTRY(grow(g->node_prods, P_cap * prod_w));
-  BTRY(grow(g->node_parents, P_cap * idx_w));
-  BTRY(grow(g->token_parents, T_cap * idx_w));
+  // ---- device buffers (exactly batch_needs: the server admits by it) ----
+  {
+    BufNeed need[kBatchBufs];
+    const int k = batch_needs(g, z, need);
+    for (int i = 0; i < k; i++)
+      if (need[i].buf != &g->b_pack && need[i].buf != &g->b_packed) BTRY(grow(*need[i].buf, need[i].bytes));
+  }
 
   unsigned long long *da = (unsigned long long *)g->b_arrays.p;
   BatchDesc bd{};
@@ -181,9 +228,8 @@ int run_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offset
     if (!ub) continue;
     BCK(cudaMemsetAsync(g->pse_ticket.p, 0, 16, s));
     BCK(cudaMemsetAsync(g->pse_flags.p, 0, ub * 4, s));
-    BCK(cudaMemsetAsync(g->queue_len.p, 0, 16, s));
     BCK(cudaMemsetAsync(g->super_key.p, 0, ((ub >> kPseSuperShift) + 1) * 4, s));
-    PseArgs pa = pse_args(g, mode, qcap);
+    PseArgs pa = pse_args(g, mode, walk_ub);
     pa.batch = d_bd;
     pa.status = bd.status;
     pse_tile_kernel<<<(unsigned)std::min<uint64_t>(ub, (uint64_t)g->pse_grid), kPseThreads, 0, s>>>(pa);

@@ -2,6 +2,7 @@
 #include "device_tables.h"
 
 #include <algorithm>
+#include <array>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -233,6 +234,67 @@ int build_lexer_table(const LexerMachine &lm, LexerTable *out, std::string *why)
   out->shift = shift;
   out->swz = (int)swz;
   out->wide_cls = lm.C > 64 ? 1 : 0;
+
+  // ---- the window machine: sets of live states, breadth first from the
+  // set of all of them ----
+  using Set = std::array<unsigned long long, 4>;
+  std::map<Set, int> id;
+  std::vector<Set> sets;
+  Set full{};
+  for (int s = 0; s < lm.M; s++)
+    if (s != lm.dead) full[s >> 6] |= 1ull << (s & 63);
+  id[full] = 0;
+  sets.push_back(full);
+  std::vector<int> next;  // [P * C]
+  bool fits = true;
+  for (size_t i = 0; i < sets.size() && fits; i++) {
+    for (int c = 0; c < lm.C; c++) {
+      Set ns{};
+      for (int s = 0; s < lm.M; s++)
+        if (sets[i][s >> 6] >> (s & 63) & 1) {
+          const int x = lm.trans[(size_t)s * lm.C + c];
+          if (x != lm.dead) ns[x >> 6] |= 1ull << (x & 63);
+        }
+      auto it = id.find(ns);
+      int k;
+      if (it != id.end()) {
+        k = it->second;
+      } else {
+        k = (int)sets.size();
+        id[ns] = k;
+        sets.push_back(ns);
+      }
+      next.push_back(k);
+    }
+    if (sets.size() > (size_t)kMaxWindowSets || sets.size() * (size_t)cp * 4 > kWindowBytes) fits = false;
+  }
+  out->ps_tab.clear();
+  out->ps_mask.clear();
+  out->ps_sets = 0;
+  if (fits) {
+    const size_t P = sets.size();
+    out->ps_sets = (int)P;
+    out->ps_full = F(0);
+    out->ps_tab.assign(P * cp, 0);
+    out->ps_mask.assign(P * 4, 0);
+    for (size_t p = 0; p < P; p++) {
+      for (int w = 0; w < 4; w++) out->ps_mask[p * 4 + w] = sets[p][w];
+      for (int c = 0; c < cp; c++) {
+        uint32_t e = F((uint32_t)p) | (0xFFu << 24);  // columns >= C are never read
+        if (c < lm.C) {
+          const int k = next[p * lm.C + c];
+          int members = 0, one = -1;
+          for (int w = 0; w < 4; w++) {
+            members += __builtin_popcountll(sets[k][w]);
+            if (sets[k][w]) one = 64 * w + __builtin_ctzll(sets[k][w]);
+          }
+          const uint32_t info = members == 0 ? (uint32_t)lm.dead : members == 1 ? (uint32_t)one : 0xFFu;
+          e = F((uint32_t)k) | (info << 24);
+        }
+        out->ps_tab[p * cp + ((uint32_t)c ^ ((uint32_t)p & swz))] = e;
+      }
+    }
+  }
   return ALPACC_OK;
 }
 

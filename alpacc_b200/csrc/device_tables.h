@@ -44,12 +44,28 @@ struct LexerMachine {
 // byte offset of entry (s, c)), and code is what happens before the byte:
 // 0xFF no token boundary, 0xFE the token ending there is ignored, else its
 // terminal id.
+//
+// The window machine: the subset automaton of the machine's live states,
+// started from the set of all of them, in the same row format (rows of CP
+// entries, F and swizzle as above): entry(p, c) = F(next set) | info << 24,
+// info = the next set's one state when it has exactly one, the dead state
+// when it is empty, 0xFF when it has two or more. Walking it over the bytes
+// before a chunk gives the set of states the chunk can start in. Built when
+// it has at most kMaxWindowSets sets and its rows fit kWindowBytes; else
+// ps_tab is empty.
+constexpr int kMaxWindowSets = 1024;
+constexpr size_t kWindowBytes = 48 * 1024;
+
 struct LexerTable {
   std::vector<uint32_t> tab;   // [M * CP]
   std::vector<uint16_t> cls4;  // [256] class * 4
   int shift = 2;               // log2(CP) + 2
   int swz = 0;                 // min(CP, 32) - 1
   int wide_cls = 0;            // class * 4 does not fit a byte (C > 64)
+  std::vector<uint32_t> ps_tab;             // [P * CP] window machine, or empty
+  std::vector<unsigned long long> ps_mask;  // [P * 4] member states of each set (bit s of word s / 64)
+  uint32_t ps_full = 0;                     // F of the set of all live states
+  int ps_sets = 0;                          // P
 };
 
 int build_lexer_table(const LexerMachine &lm, LexerTable *out, std::string *why);

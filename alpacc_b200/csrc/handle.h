@@ -79,12 +79,16 @@ struct alpacc_gpu_grammar {
   bool stage_used[kStages] = {};
   double stage_ms[kStages] = {};
   // tables
-  DevBuf lex_tab, lex_cls4, lane_of, img, img_cnt, img2, sterm, sflags;
+  DevBuf lex_tab, lex_cls4, lex_ps, lex_psmask, img, img_cnt, sterm, sflags;
   DevBuf dense, ht_key, ht_rec, rec, stacks, prods, arity, is_term;
   // lexer table shape (build_lexer_table): entries, rows of 1 << (cp_shift - 2),
   // column swizzle mask, u16 class table when classes exceed 64
   int tab_words = 0, cp_shift = 2, swz = 0, wide_cls = 0;
-  int lex_w4 = 0;    // machine above 64 states: 256-bit state sets in pass 1
+  // lexer kernel variant: 0 window machine, at most 64 states; 1 window
+  // machine, more states; 2 windows walked as explicit state sets
+  int lex_variant = 0;
+  int ps_words = 0;        // window machine entries in shared memory (0: none)
+  uint32_t ps_full = 0;
   int lex_grid = 0;  // persistent grid of lex_kernel
   int pair_grid = 0, pse_grid = 0;  // resident CTAs of pair_kernel / pse_tile_kernel
   // parser-stage capacities: the largest exact needs seen (brackets, productions)
@@ -105,7 +109,8 @@ struct alpacc_gpu_grammar {
   DevBuf codes, tile_cnt, tile_pos, tile_off, tile_prev;  // staged lexer output
   DevBuf tok_ids, tok_starts, tok_lens;
   DevBuf pair_ticket, pst_flags, pst_agg, pst_inc, br, pr;
-  DevBuf pse_ticket, pse_flags, pse_agg, pse_inc, ch_h0, ch_tc, tile_min, chunk_min, super_key, queue, queue_len;
+  DevBuf pse_ticket, pse_flags, pse_agg, pse_inc, tile_min, super_key;
+  DevBuf pse_regions;  // per walk tile: staircase and queries (pse_region_bytes)
   DevBuf node_prods, node_parents, token_parents;
   // batches: descriptor arrays, per-document statuses, packing ranges, packed results
   DevBuf b_arrays, b_desc, b_status, b_pack, b_packed;
@@ -188,8 +193,8 @@ inline void release_block(alpacc_gpu_grammar *g, PinnedBlock *b, bool tree) {
   cudaFreeHost(b);
 }
 
-// Dynamic shared memory of lex_kernel for this handle's tables: the class
-// table, then the entries.
+// Dynamic shared memory of the lexer kernels for this handle's tables: the
+// class table, the entries, the window machine's entries.
 inline size_t lex_dyn_smem(const alpacc_gpu_grammar *g) {
-  return (g->wide_cls ? 512 : 256) + (size_t)g->tab_words * 4;
+  return (g->wide_cls ? 512 : 256) + (size_t)g->tab_words * 4 + (size_t)g->ps_words * 4;
 }

@@ -46,15 +46,15 @@ __device__ __forceinline__ int batch_doc(const unsigned long long *tile0, int do
 enum PlanKind : int { kPlanPairs = 0, kPlanBrackets = 1, kPlanParents = 2 };
 __global__ void batch_plan_kernel(BatchDesc b, int kind, unsigned long long *tile0, unsigned long long tile);
 
-// ---- lexer tiles: 256 chunks x 15 words (60 bytes); the first 8 chunks are
-// a halo repeating the end of the previous tile ----
+// ---- lexer tiles: 256 chunks x 15 words (60 bytes), loaded with the 16
+// bytes before the tile (the first chunk's window) ----
 constexpr int kLexThreads = 256;
 constexpr int kLexWords = 15;
 constexpr int kLexChunk = kLexWords * 4;
-constexpr int kLexHalo = 8;
-constexpr int kLexLoad = kLexThreads * kLexChunk;               // bytes loaded per tile
-constexpr int kLexData = (kLexThreads - kLexHalo) * kLexChunk;  // new bytes per tile
-constexpr int kLexLanes = kMaxLanes;                            // start lanes of an open chunk
+constexpr int kLexWin = 16;                                     // window bytes before each chunk
+constexpr int kLexData = kLexThreads * kLexChunk;               // bytes per tile
+constexpr int kLexLoad = kLexWin + kLexData;                    // bytes loaded per tile
+constexpr int kLexLanes = kMaxLanes;                            // candidate starts of an open chunk
 
 struct LexArgs {
   const uint8_t *in;
@@ -68,10 +68,14 @@ struct LexArgs {
   const uint8_t *cls4;              // byte -> class * 4: u8[256], or u16[256] when wide_cls
   int wide_cls;
   int cp_shift, swz;
-  const uint8_t *lane_of;           // [C*M] slot of a start state in img of a class, 0xff dead
-  const uint8_t *img;               // [C*kLexLanes]
+  // window machine (build_lexer_table): entries in the same row format,
+  // F of the set of all live states, member states of each set (4 words)
+  const uint32_t *ps_tab;           // [ps_words], null: windows walked as explicit state sets
+  int ps_words;
+  uint32_t ps_full;
+  const unsigned long long *ps_mask;
+  const uint8_t *img;               // [C*kLexLanes] live targets of each class (explicit set walks)
   const uint8_t *img_cnt;           // [C]
-  const unsigned long long *img2;   // [C*C] live states after two bytes (M <= 64), or null
   const uint8_t *sterm;             // [M]
   const uint8_t *sflags;            // [M] bit0 produce, bit1 accept, bit2 kept
   int M, C, dead, m0;
@@ -89,9 +93,9 @@ struct LexArgs {
   DeviceStatus *status;
   int diag;             // 1: accumulate diagnostic counters in status->scratch
   // diagnostics: SM cycles of each barrier-delimited phase summed over tiles
-  // (thread 0's clock): 0 load, 1 pass 1, 2 lane jobs, 3 constant-chunk scan,
-  // 4 start states, 5 pass 2 + masks + count scan, 6 count look-back,
-  // 7 token writes; null when off
+  // (thread 0's clock): 0 load, 1 window walk, 2 chunk walks + candidate
+  // jobs, 3 known-chunk scan, 4 start states, 5 open chunks' codes + masks +
+  // count scan, 6 count look-back, 7 token / code writes; null when off
   unsigned long long *phase_cycles;
   const BatchDesc *batch;  // null: one document (in, n, status); else tiles are virtual (lex_tile0)
   // One window of a longer input (chunked lexing): the input continues after
@@ -99,22 +103,26 @@ struct LexArgs {
   // window's last boundary is left in status->last_boundary.
   int open_end;
   unsigned long long index_base;  // added to every token start (a window's offset in chunked lexing)
-  // Staged output (lex_kernel, lex_kernel_wide): each tile writes the codes of
+  // Staged output (lex_kernel*): each tile writes the codes of
   // its data bytes to codes[tile * kLexData ...] and its (kept-token count,
   // last boundary) to tile_cnt / tile_pos; lex_scan_kernel and lex_emit_kernel
   // then write the tokens, so no tile waits for another's count. The direct
-  // kernels (lex_direct_kernel, lex_direct_kernel_wide) chain the counts by
+  // kernels (lex_direct_kernel*) chain the counts by
   // decoupled look-back (st2) and write the tokens themselves.
   uint8_t *codes;
   uint32_t *tile_cnt, *tile_pos;
 };
 
-// Machines of at most 64 states (one 64-bit state set in pass 1), and of up
-// to 255 states (four words); staged and direct output.
+// Staged and direct output, each for: machines of at most 64 states with a
+// window machine (one 64-bit candidate set), of up to 255 states with one
+// (four words), and any machine whose window machine was not built (windows
+// walked as explicit state sets).
 __global__ void lex_kernel(LexArgs args);
 __global__ void lex_kernel_wide(LexArgs args);
+__global__ void lex_kernel_sets(LexArgs args);
 __global__ void lex_direct_kernel(LexArgs args);
 __global__ void lex_direct_kernel_wide(LexArgs args);
+__global__ void lex_direct_kernel_sets(LexArgs args);
 
 struct LexEmitArgs {
   const uint8_t *codes;             // [tiles * kLexData] codes of every data byte (lex_kernel)
@@ -189,18 +197,21 @@ struct PseArgs {
   const int32_t *arity;             // parents: per production
   const uint8_t *is_term;           // parents: terminal production flags
   int num_prods;                    // entries of arity / is_term
-  int32_t *ch_h0;                   // [tiles * 256] depth before each chunk
-  int32_t *ch_min;                  // [tiles * 256] minimum depth in each chunk (INT_MAX if empty)
-  int32_t *ch_tc;                   // parents: [tiles * 256] terminal productions before each chunk
-  int32_t *tile_min;                // [tiles]
+  int32_t *tile_min;                // [tiles] minimum depth of each tile
   uint32_t *super_key;              // [ceil(tiles / 256)] INT_MAX - minimum over each run of 256 tiles (0: none)
-  unsigned long long *queue;        // elements whose answer lies in an earlier tile
-  unsigned long long queue_cap;
-  unsigned long long *queue_len;    // device counter
+  // per tile (regions of kPseTile entries): the staircase - the tile's
+  // right-to-left strict minima, in position order (their depths increase):
+  // offset in the tile, depth, (parents) inclusive terminal-production count -
+  // and the queries the tile could not answer, in position order (their query
+  // values decrease): offset, query value, (parents) inclusive terminal count
+  uint16_t *stair_off, *q_off;
+  int32_t *stair_val, *stair_tc, *q_val, *q_tc;
+  uint32_t *stair_cnt, *q_cnt;      // [tiles]
   // parents: the compacted tree (compact_tree), written as answers are found
   void *node_prods, *node_parents, *token_parents;
   int prod_w, idx_w;
-  unsigned *ticket;
+  unsigned *ticket;                 // tiles of the walk
+  unsigned *resolve_ticket;         // tiles with queries, taken by the resolve kernel's warps
   PairTileState st;                 // (sum of steps, terminal count)
   DeviceStatus *status;
   const BatchDesc *batch;           // null: one document; else virtual tiles (br_tile0 / pr_tile0)

@@ -1,5 +1,5 @@
 // Data-parallel lexer for sm_100a: the sequential semantics of lex_string
-// (backends/c/lexer.c:39-97) computed tile-parallel in one kernel.
+// (backends/c/lexer.c:39-97) computed tile-parallel.
 //
 // The lexer runs a Moore machine over byte classes that device_tables.cpp
 // derives from TO_STATE / COMPOSE / ACCEPT. Its transition table lives in
@@ -13,32 +13,32 @@
 // (entry & 0xFFFFFF) ^ class * 4) and one shared-memory load.
 //
 // A tile is 256 chunks of 60 bytes (15 words: an odd word stride, so per-thread
-// rows are bank-conflict free); the first 8 chunks are a halo repeating the
-// 480 bytes before the tile's 14880 data bytes, walked again so that the tile
-// can almost always derive its incoming state by itself.
+// rows are bank-conflict free), loaded with the 16 bytes before it.
 //
-// Pass 1 (each chunk, start state unknown): the set of live states after its
-//   first bytes is walked until it is one state (typically 1-4 bytes on JSON)
-//   and word aligned; from there a fully unrolled single-lane walk writes each
-//   byte's code over the consumed input word. Such a chunk maps every live
-//   start to one end state ("constant"). A chunk whose set is not one state
-//   after 16 bytes ("open") instead has each of its first byte's targets
-//   walked on its own - one job per lane, spread over the whole CTA so that no
-//   thread walks several lanes while the others wait - keeping the end state
-//   per start lane and, for the first 64 jobs, the lane's codes.
-// Resolution: each chunk's start state follows from the nearest constant chunk
-//   before it; only when no halo chunk is constant does the tile read its
-//   predecessor's published outgoing state (bounded look-back).
-// Pass 2: each data chunk re-walks the bytes before its walk converged from
-//   its true start, writing their codes; an open chunk copies its true lane's
-//   codes (or walks the chunk again when its lanes had no code slots), a
-//   partial chunk (the input's last) is walked whole.
-// Output, staged (lex_kernel): each tile writes the codes of its data bytes
+// Window: each chunk walks the 16 bytes before it in the window machine (the
+//   subset automaton of the live states, same row format, from the set of all
+//   of them), which yields the set of states the chunk can start in. On JSON
+//   that set is one state for ~95% of chunks, on s-expressions for all: the
+//   chunk's start is then known without looking at any other chunk
+//   ("known"). The window walk is the same fixed 16 steps in every thread.
+//   Machines whose subset automaton is too large walk the window as an
+//   explicit state set instead.
+// Walk: a known chunk walks its 60 bytes once from its start (fully unrolled),
+//   writing each byte's code over the consumed input word. A chunk whose
+//   window left two or more candidates ("open") has each candidate walked on
+//   its own - one job per candidate, spread over the whole CTA - keeping the
+//   end state per candidate and, for the first 64 jobs, the codes.
+// Resolution: an open chunk's start is the end of the nearest known chunk
+//   before it carried through the open chunks in between; only when the
+//   tile's first chunk is open does the tile read its predecessor's published
+//   outgoing state (bounded look-back). The open chunk then takes its true
+//   candidate's codes (or walks again when that candidate had no code slot).
+// Output, staged (lex_kernel*): each tile writes the codes of its bytes
 //   (16-byte stores from shared memory) and its (kept-token count, last
 //   boundary); lex_scan_kernel scans the tile totals and lex_emit_kernel turns
 //   each tile's codes into tokens at their final places, with the length_t
 //   check of lexer.c:68-72. No tile waits for another tile's count.
-// Output, direct (lex_direct_kernel, for the allocation-free entry point):
+// Output, direct (lex_direct_kernel*, for the allocation-free entry point):
 //   boundary masks from the code words, a (token count, last boundary) block
 //   scan, a decoupled look-back over tiles (Merrill & Garland 2016) and the
 //   kept tokens written by the kernel itself.
@@ -63,92 +63,20 @@ __device__ __forceinline__ void store_uint(void *base, unsigned long long i, int
   }
 }
 
-enum ChunkKind : uint8_t { kEmpty = 0, kConst = 1, kOpen = 2, kPartial = 3 };
+// kOpenTail: an open chunk holding the input's last byte (no candidate jobs:
+// walked once its start is known; nothing after it reads its end state)
+enum ChunkKind : uint8_t { kEmpty = 0, kKnown = 1, kOpen = 2, kOpenTail = 3 };
 
 constexpr uint32_t kAddrMask = 0xFFFFFFu;  // F(next) bits of an entry
 constexpr uint8_t kNoBoundary = 0xFF, kIgnored = 0xFE;
-// Bytes a chunk walks as a state set before it counts as open: bounds how long
-// one late-converging chunk can hold its warp in the set walk.
-constexpr int kSetWalk = 16;
-// Lane walks of open chunks run as jobs spread over the CTA (rounds of one
-// lane per thread); the first kCodeJobs keep their codes, so the chunk's
-// pass 2 copies the true lane's codes instead of walking again.
+constexpr uint32_t kOpenInfo = 0xFFu;        // window machine: two or more candidates
+constexpr int kWinWords = kLexWin / 4;
+// Candidate walks of open chunks run as jobs spread over the CTA (rounds of
+// one job per thread); the first kCodeJobs keep their codes, so the chunk's
+// second pass copies the true candidate's codes instead of walking again.
 constexpr int kCodeJobs = 64;
 
-struct LexSmem {
-  uint32_t bytes[kLexThreads * kLexWords];  // the tile; codes replace the consumed words
-  uint8_t lend[kLexLanes * kLexThreads];    // open chunks: end state per start lane (lane-major)
-  uint8_t kind[kLexThreads];
-  uint8_t endst[kLexThreads];  // constant chunks: end state
-  uint8_t c0[kLexThreads];     // class of the chunk's first byte
-  uint8_t start[kLexThreads];  // true start state of data chunks
-  uint16_t jfirst[kLexThreads];  // first lane job of each chunk (jobs of earlier chunks; none for closed ones)
-  uint32_t jcodes[kCodeJobs * kLexWords];  // codes of bytes 1..59 of the first lane jobs
-  uint8_t sterm[256];          // per machine state: terminal id
-  uint8_t sflags[256];         // bit1 accept, bit2 kept
-  int kconst[kLexThreads];
-  int scan_a[kLexThreads / 32], scan_b[kLexThreads / 32];
-  unsigned tile;
-  int s_in;
-  int need_lookback;
-  int out_published;
-  long long cnt_prefix, pos_prefix;
-};
-
-// The machine in shared memory: class table and entries, plus the shape
-// parameters that turn a state into its row offset and back.
-struct Tab {
-  const uint8_t *cls;  // [256] class * 4 (u8), or [512] bytes of u16 when wide
-  const uint8_t *ent;  // entries, addressed by byte offset
-  int wide;
-  int shift;           // F(x) >> shift == x
-  uint32_t swz;        // K - 1
-};
-
-__device__ __forceinline__ uint32_t cls4_of(const Tab &tb, uint32_t b) {
-  return tb.wide ? (uint32_t) reinterpret_cast<const uint16_t *>(tb.cls)[b] : (uint32_t)tb.cls[b];
-}
-
-__device__ __forceinline__ uint32_t row_of(const Tab &tb, uint32_t x) { return (x << tb.shift) | ((x & tb.swz) << 2); }
-
-__device__ __forceinline__ int state_of(const Tab &tb, uint32_t f) { return (int)((f & kAddrMask) >> tb.shift); }
-
-// One machine step: the entry for (state of f, class c4 / 4).
-__device__ __forceinline__ uint32_t step(const Tab &tb, uint32_t f, uint32_t c4) {
-  return *reinterpret_cast<const uint32_t *>(tb.ent + ((f & kAddrMask) ^ c4));
-}
-
-// f_t(x): the state after chunk t when it starts in state x. A constant chunk
-// maps every live start to its one end state (a start whose lane died instead
-// is caught when the chunk is re-walked from its true start, which then
-// rejects the input); an open chunk keeps the end state of each start lane.
-// A partial chunk (the input's last) is never followed by a non-empty chunk.
-__device__ __forceinline__ int eval_chunk(const LexArgs &a, const LexSmem *sm, int t, int x) {
-  const int kind = sm->kind[t];
-  if (kind == kEmpty) return x;
-  const int dead = a.dead;
-  if (x == dead || x < 0) return dead;
-  if (kind == kConst) return sm->endst[t];
-  if (kind == kPartial) return dead;
-  const int slot = __ldg(a.lane_of + (size_t)sm->c0[t] * a.M + x);
-  if (slot == 0xff) return dead;
-  return sm->lend[slot * kLexThreads + t];
-}
-
-struct CntPosOp {
-  __device__ Pair64 operator()(Pair64 e, Pair64 l) const { return Pair64{e.a + l.a, e.b > l.b ? e.b : l.b}; }
-};
-
-// Bytes of `w` that differ from 0: 0x80 in such a byte, 0 elsewhere (exact, no
-// borrow between bytes).
-__device__ __forceinline__ uint32_t nonzero_bytes(uint32_t w) {
-  return (((w & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | w) & 0x80808080u;
-}
-
-// The four 0x80 flags of nonzero_bytes as a 4-bit mask (byte i -> bit i).
-__device__ __forceinline__ uint32_t movemask4(uint32_t x) { return ((x >> 7) * 0x10204080u) >> 28; }
-
-// The set walk of pass 1 over W 64-bit words of states.
+// The set of states an open chunk can start in, W 64-bit words.
 template <int W>
 struct StateSet {
   unsigned long long w[W];
@@ -161,7 +89,6 @@ struct StateSet {
     for (int i = 0; i < W; i++)
       if ((s >> 6) == i) w[i] |= 1ull << (s & 63);
   }
-  // more than one state (no population count for a single word)
   __device__ __forceinline__ bool many() const {
     if (W == 1) return (w[0] & (w[0] - 1)) != 0;
     return count() > 1;
@@ -186,114 +113,197 @@ struct StateSet {
   }
 };
 
-// Pass 1 for a full chunk: returns the chunk kind; sets *jw_out (bytes walked
-// as a set, a multiple of 4: pass 2 re-walks them), the converged state at
-// that point (or -1), and the end state (constant) or the per-lane end states
-// in lend (open).
 template <int W>
-__device__ __forceinline__ int pass1_chunk(const LexArgs &a, const Tab &tb, LexSmem *sm, int t, int *jw_out,
-                                           int *end_out, int *conv_out) {
-  uint32_t *row = sm->bytes + t * kLexWords;
-  const uint8_t *rb = reinterpret_cast<const uint8_t *>(row);
-  const int dead = a.dead;
-  const int c0 = (int)(cls4_of(tb, rb[0]) >> 2);
-  sm->c0[t] = (uint8_t)c0;
-  StateSet<W> set;
-  set.clear();
-  int j;
-  if (W == 1 && a.img2) {  // the first two bytes at once
-    set.w[0] = __ldg(a.img2 + c0 * a.C + (int)(cls4_of(tb, rb[1]) >> 2));
-    j = 2;
-  } else {
-    const int cnt = __ldg(a.img_cnt + c0);
-    for (int l = 0; l < cnt; l++) set.add(__ldg(a.img + c0 * kLexLanes + l));
-    j = 1;
-  }
-  // walk the set until it is one state and the position is word aligned, at
-  // most kSetWalk bytes
-  bool many = set.many();
-  while (j < kSetWalk && (many || (j & 3))) {
-    const uint32_t c4 = cls4_of(tb, rb[j]);
-    StateSet<W> ns;
-    ns.clear();
-#pragma unroll
-    for (int i = 0; i < W; i++)
-      for (unsigned long long m = set.w[i]; m; m &= m - 1) {
-        const int s = 64 * i + __ffsll((long long)m) - 1;
-        const int nx = state_of(tb, step(tb, row_of(tb, (uint32_t)s), c4));
-        if (nx != dead) ns.add(nx);
-      }
-    set = ns;
-    many = set.many();
-    ++j;
-  }
-  *conv_out = -1;
-  if (set.empty()) {  // every live start dies in this chunk
-    *jw_out = j;
-    *end_out = dead;
-    return kConst;
-  }
-  if (many) {  // open: its start lanes are walked one by one as CTA-wide jobs
-    *jw_out = kLexChunk;
-    *end_out = -1;
-    return kOpen;
-  }
-  const int s_conv = set.first();
-  *conv_out = s_conv;
-  *jw_out = j;
-  if (j >= kLexChunk) {
-    *end_out = s_conv;
-    return kConst;
-  }
-  // the unrolled walk from the converged state: codes of words >= j / 4
-  const uint32_t fconv = row_of(tb, (uint32_t)s_conv);
-  const int jw4 = j >> 2;
-  uint32_t f = fconv;
+struct LexSmem {
+  uint32_t bytes[kLexLoad / 4];             // window + tile; codes replace the consumed words
+  uint8_t lend[kLexLanes * kLexThreads];    // open chunks: end state per candidate (candidate-major)
+  unsigned long long cand[W][kLexThreads];  // open chunks: their candidate start states
+  uint8_t kind[kLexThreads];
+  uint8_t endst[kLexThreads];  // known chunks: end state
+  uint8_t start[kLexThreads];  // every chunk's true start state
+  uint16_t jfirst[kLexThreads];  // first candidate job of each chunk (jobs of earlier chunks)
+  uint32_t jcodes[kCodeJobs * kLexWords];  // codes of the first candidate jobs
+  uint8_t sterm[256];          // per machine state: terminal id
+  uint8_t sflags[256];         // bit1 accept, bit2 kept
+  int kconst[kLexThreads];
+  int scan_a[kLexThreads / 32], scan_b[kLexThreads / 32];
+  unsigned tile;
+  int s_in;
+  int out_published;
+  long long cnt_prefix, pos_prefix;
+};
+
+// A machine in shared memory (the lexer's or the window machine): class
+// table and entries, plus the shape parameters that turn a state into its row
+// offset and back.
+struct Tab {
+  const uint8_t *cls;  // [256] class * 4 (u8), or [512] bytes of u16 when wide
+  const uint8_t *ent;  // entries, addressed by byte offset
+  int wide;
+  int shift;           // F(x) >> shift == x
+  uint32_t swz;        // K - 1
+};
+
+__device__ __forceinline__ uint32_t cls4_of(const Tab &tb, uint32_t b) {
+  return tb.wide ? (uint32_t) reinterpret_cast<const uint16_t *>(tb.cls)[b] : (uint32_t)tb.cls[b];
+}
+
+__device__ __forceinline__ uint32_t row_of(const Tab &tb, uint32_t x) { return (x << tb.shift) | ((x & tb.swz) << 2); }
+
+__device__ __forceinline__ int state_of(const Tab &tb, uint32_t f) { return (int)((f & kAddrMask) >> tb.shift); }
+
+// One machine step: the entry for (state of f, class c4 / 4).
+__device__ __forceinline__ uint32_t step(const Tab &tb, uint32_t f, uint32_t c4) {
+  return *reinterpret_cast<const uint32_t *>(tb.ent + ((f & kAddrMask) ^ c4));
+}
+
+// The four bytes' codes of a word walked from f (entries e0..e3 of its bytes)
+// packed into one word.
+__device__ __forceinline__ uint32_t pack_codes(uint32_t e0, uint32_t e1, uint32_t e2, uint32_t e3) {
+  return __byte_perm(__byte_perm(e0, e1, 0x0073), __byte_perm(e2, e3, 0x0073), 0x5410);
+}
+
+// A full chunk (15 words of src) walked from state x: the codes of its bytes
+// into dst (may be src), returns the end state.
+__device__ __forceinline__ int walk_chunk(const Tab &tb, const uint32_t *src, uint32_t *dst, int x) {
+  uint32_t f = row_of(tb, (uint32_t)x);
 #pragma unroll
   for (int w = 0; w < kLexWords; ++w) {
-    if (w == jw4) f = fconv;
-    const uint32_t word = row[w];
+    const uint32_t word = src[w];
     const uint32_t e0 = step(tb, f, cls4_of(tb, __byte_perm(word, 0, 0x4440)));
     const uint32_t e1 = step(tb, e0, cls4_of(tb, __byte_perm(word, 0, 0x4441)));
     const uint32_t e2 = step(tb, e1, cls4_of(tb, __byte_perm(word, 0, 0x4442)));
     const uint32_t e3 = step(tb, e2, cls4_of(tb, __byte_perm(word, 0, 0x4443)));
     f = e3;
-    if (w >= jw4) row[w] = __byte_perm(__byte_perm(e0, e1, 0x0073), __byte_perm(e2, e3, 0x0073), 0x5410);
+    dst[w] = pack_codes(e0, e1, e2, e3);
   }
-  *end_out = state_of(tb, f);
-  return kConst;
+  return state_of(tb, f);
 }
 
-// One lane of an open chunk: bytes 1..59 of chunk tc's row walked from lane
-// l's state (the state byte 0 leads to), end state into lend; with `codes`,
-// the codes of bytes 1..59 (byte 0 left 0xFF).
-__device__ __forceinline__ void walk_lane(const LexArgs &a, const Tab &tb, LexSmem *sm, int tc, int l,
-                                          uint32_t *codes) {
-  const uint32_t *row = sm->bytes + tc * kLexWords;
-  uint32_t f = row_of(tb, __ldg(a.img + sm->c0[tc] * kLexLanes + l));
-  {
-    const uint32_t word = row[0];
-    const uint32_t e1 = step(tb, f, cls4_of(tb, __byte_perm(word, 0, 0x4441)));
-    const uint32_t e2 = step(tb, e1, cls4_of(tb, __byte_perm(word, 0, 0x4442)));
-    const uint32_t e3 = step(tb, e2, cls4_of(tb, __byte_perm(word, 0, 0x4443)));
-    f = e3;
-    if (codes) codes[0] = __byte_perm(__byte_perm(0xFF000000u, e1, 0x0073), __byte_perm(e2, e3, 0x0073), 0x5410);
+// The first nb bytes of a row walked from state x, codes written over them;
+// returns the end state.
+__device__ __forceinline__ int walk_bytes(const Tab &tb, uint8_t *rb, int nb, int x) {
+  uint32_t f = row_of(tb, (uint32_t)x);
+  for (int j = 0; j < nb; ++j) {
+    const uint32_t e = step(tb, f, cls4_of(tb, rb[j]));
+    rb[j] = (uint8_t)(e >> 24);
+    f = e;
   }
-#pragma unroll 2
-  for (int w = 1; w < kLexWords; ++w) {
-    const uint32_t word = row[w];
-    const uint32_t e0 = step(tb, f, cls4_of(tb, __byte_perm(word, 0, 0x4440)));
-    const uint32_t e1 = step(tb, e0, cls4_of(tb, __byte_perm(word, 0, 0x4441)));
-    const uint32_t e2 = step(tb, e1, cls4_of(tb, __byte_perm(word, 0, 0x4442)));
-    const uint32_t e3 = step(tb, e2, cls4_of(tb, __byte_perm(word, 0, 0x4443)));
-    f = e3;
-    if (codes) codes[w] = __byte_perm(__byte_perm(e0, e1, 0x0073), __byte_perm(e2, e3, 0x0073), 0x5410);
-  }
-  sm->lend[l * kLexThreads + tc] = (uint8_t)state_of(tb, f);
+  return state_of(tb, f);
 }
 
-template <int W, bool kStaged>
-__device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_smem, LexSmem *sm) {
+// The window of chunk t (the kLexWin bytes before its row): the one state the
+// chunk can start in (the dead state when none), or -1 with the candidates in
+// *cand. kPs: walked in the window machine; else as an explicit state set
+// from the first window byte's image.
+template <int W, bool kPs>
+__device__ __forceinline__ int window_start(const LexArgs &a, const Tab &tb, const Tab &tw, const uint32_t *win,
+                                            StateSet<W> *cand) {
+  if (kPs) {
+    uint32_t f = a.ps_full, e = 0;
+#pragma unroll
+    for (int w = 0; w < kWinWords; ++w) {
+      const uint32_t word = win[w];
+      e = step(tw, f, cls4_of(tb, __byte_perm(word, 0, 0x4440)));
+      e = step(tw, e, cls4_of(tb, __byte_perm(word, 0, 0x4441)));
+      e = step(tw, e, cls4_of(tb, __byte_perm(word, 0, 0x4442)));
+      e = step(tw, e, cls4_of(tb, __byte_perm(word, 0, 0x4443)));
+      f = e;
+    }
+    const uint32_t info = e >> 24;
+    if (info != kOpenInfo) return (int)info;
+    const int p = state_of(tw, e);
+#pragma unroll
+    for (int i = 0; i < W; i++) cand->w[i] = __ldg(a.ps_mask + 4 * p + i);
+    return -1;
+  } else {
+    const uint8_t *wb = reinterpret_cast<const uint8_t *>(win);
+    StateSet<W> set;
+    set.clear();
+    const int c0 = (int)(cls4_of(tb, wb[0]) >> 2);
+    const int cnt = __ldg(a.img_cnt + c0);
+    for (int l = 0; l < cnt; l++) set.add(__ldg(a.img + c0 * kLexLanes + l));
+    for (int j = 1; j < kLexWin; ++j) {
+      const uint32_t c4 = cls4_of(tb, wb[j]);
+      StateSet<W> ns;
+      ns.clear();
+#pragma unroll
+      for (int i = 0; i < W; i++)
+        for (unsigned long long m = set.w[i]; m; m &= m - 1) {
+          const int s = 64 * i + __ffsll((long long)m) - 1;
+          const int nx = state_of(tb, step(tb, row_of(tb, (uint32_t)s), c4));
+          if (nx != a.dead) ns.add(nx);
+        }
+      set = ns;
+    }
+    if (set.empty()) return a.dead;  // (a machine without a dead state never empties a set)
+    if (!set.many()) return set.first();
+    *cand = set;
+    return -1;
+  }
+}
+
+// Candidate slot of state x among an open chunk's candidates (its rank in the
+// set), or -1 when x is not one of them.
+template <int W>
+__device__ __forceinline__ int cand_slot(const LexSmem<W> *sm, int t, int x) {
+  int r = 0;
+#pragma unroll
+  for (int i = 0; i < W; i++) {
+    const unsigned long long m = sm->cand[i][t];
+    if ((x >> 6) == i) return (m >> (x & 63) & 1) ? r + __popcll(m & ((1ull << (x & 63)) - 1)) : -1;
+    r += __popcll(m);
+  }
+  return -1;
+}
+
+// The l-th candidate (in state order) of open chunk t.
+template <int W>
+__device__ __forceinline__ int cand_state(const LexSmem<W> *sm, int t, int l) {
+#pragma unroll
+  for (int i = 0; i < W; i++) {
+    unsigned long long m = sm->cand[i][t];
+    const int c = __popcll(m);
+    if (l < c) {
+      for (int k = 0; k < l; k++) m &= m - 1;
+      return 64 * i + __ffsll((long long)m) - 1;
+    }
+    l -= c;
+  }
+  return 0;
+}
+
+// f_t(x): the state after chunk t when it starts in state x: a known chunk's
+// end state (its start is fixed), an open chunk's end for candidate x (dead
+// when x is not a candidate: the true state always is one while the input is
+// valid). A chunk holding the input's last byte is never followed by a
+// non-empty chunk.
+template <int W>
+__device__ __forceinline__ int eval_chunk(const LexArgs &a, const LexSmem<W> *sm, int t, int x) {
+  const int kind = sm->kind[t];
+  if (kind == kEmpty) return x;
+  const int dead = a.dead;
+  if (kind == kKnown) return sm->endst[t];
+  if (kind == kOpenTail || x == dead || x < 0) return dead;
+  const int slot = cand_slot(sm, t, x);
+  return slot < 0 ? dead : sm->lend[slot * kLexThreads + t];
+}
+
+struct CntPosOp {
+  __device__ Pair64 operator()(Pair64 e, Pair64 l) const { return Pair64{e.a + l.a, e.b > l.b ? e.b : l.b}; }
+};
+
+// Bytes of `w` that differ from 0: 0x80 in such a byte, 0 elsewhere (exact, no
+// borrow between bytes).
+__device__ __forceinline__ uint32_t nonzero_bytes(uint32_t w) {
+  return (((w & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | w) & 0x80808080u;
+}
+
+// The four 0x80 flags of nonzero_bytes as a 4-bit mask (byte i -> bit i).
+__device__ __forceinline__ uint32_t movemask4(uint32_t x) { return ((x >> 7) * 0x10204080u) >> 28; }
+
+template <int W, bool kPs, bool kStaged>
+__device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_smem, LexSmem<W> *sm) {
   const int t = threadIdx.x;
   const int lane = t & 31;
 
@@ -301,14 +311,18 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
   const int cls_bytes = a.wide_cls ? 512 : 256;
   uint8_t *s_cls = dyn_smem;
   uint8_t *s_ent = dyn_smem + cls_bytes;
+  uint8_t *s_win = s_ent + a.tab_words * 4;
   for (int i = t; i < cls_bytes / 4; i += kLexThreads)
     reinterpret_cast<uint32_t *>(s_cls)[i] = __ldg(reinterpret_cast<const uint32_t *>(a.cls4) + i);
   for (int i = t; i < a.tab_words; i += kLexThreads) reinterpret_cast<uint32_t *>(s_ent)[i] = __ldg(a.tab + i);
+  if (kPs)
+    for (int i = t; i < a.ps_words; i += kLexThreads) reinterpret_cast<uint32_t *>(s_win)[i] = __ldg(a.ps_tab + i);
   for (int i = t; i < 256; i += kLexThreads) {
     sm->sterm[i] = i < a.M ? __ldg(a.sterm + i) : 0;
     sm->sflags[i] = i < a.M ? __ldg(a.sflags + i) : 0;
   }
   const Tab tb{s_cls, s_ent, a.wide_cls, a.cp_shift, (uint32_t)a.swz};
+  const Tab tw{s_cls, s_win, a.wide_cls, a.cp_shift, (uint32_t)a.swz};
   const int dead = a.dead;
   const unsigned long long num_tiles = a.num_tiles;
   const unsigned long long tile_end = a.tile_end ? a.tile_end : num_tiles;
@@ -350,9 +364,9 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
       tok_base = b.tok_off[d];  // the document's token region
     }
     const long long data0 = (long long)lt * kLexData;
-    const long long load0 = data0 - (long long)kLexHalo * kLexChunk;
+    const long long load0 = data0 - (long long)kLexWin;
 
-    // ---- load halo + data ----
+    // ---- load window + tile ----
     {
       const uint8_t *in = in_base;
       uint8_t *dst = reinterpret_cast<uint8_t *>(sm->bytes);
@@ -377,58 +391,97 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
         }
       }
     }
-    const long long g0 = load0 + (long long)t * kLexChunk;
+    const long long g0 = data0 + (long long)t * kLexChunk;  // this chunk's first byte
     int nb = 0;
-    if (g0 >= 0 && g0 < n) nb = (int)min((long long)kLexChunk, n - g0);
+    if (g0 < n) nb = (int)min((long long)kLexChunk, n - g0);
+    uint32_t *row = sm->bytes + kWinWords + t * kLexWords;
+    uint8_t *rb = reinterpret_cast<uint8_t *>(row);
     __syncthreads();
     LEX_PHASE(0);
 
-    // ---- pass 1 ----
-    int jw = nb, end = -1, conv = -1, kind = kEmpty;
-    if (nb == kLexChunk) {
-      kind = pass1_chunk<W>(a, tb, sm, t, &jw, &end, &conv);
-    } else if (nb > 0) {
-      kind = kPartial;  // the input's last chunk: walked whole in pass 2
+    // ---- window: the states the chunk can start in ----
+    int x0 = -1;  // known start state
+    int kind = kEmpty;
+    if (nb > 0) {
+      if (g0 == 0) {
+        x0 = a.m0;  // the document's first chunk
+      } else {
+        StateSet<W> cand;
+        x0 = window_start<W, kPs>(a, tb, tw, row - kWinWords, &cand);
+        if (x0 < 0) {
+#pragma unroll
+          for (int i = 0; i < W; i++) sm->cand[i][t] = cand.w[i];
+        }
+      }
+      kind = x0 >= 0 ? kKnown : nb == kLexChunk ? kOpen : kOpenTail;
     }
     sm->kind[t] = (uint8_t)kind;
-    sm->endst[t] = (uint8_t)(end < 0 ? 0 : end);
-    if (a.diag) {
-      const unsigned w = __reduce_add_sync(0xffffffffu, (unsigned)(kind == kConst ? jw : nb));
-      if (lane == 0) atomicAdd(&st->scratch[3], (unsigned long long)w);
-    }
-    // ---- open chunks: one job per start lane, spread over the CTA ----
-    {
-      const int lanes = kind == kOpen ? (int)__ldg(a.img_cnt + sm->c0[t]) : 0;
-      int njobs;
-      const int jex = block_exclusive_scan<int>(lanes, AddI32(), 0, sm->scan_a, &njobs);
-      LEX_PHASE(1);
-      sm->jfirst[t] = (uint16_t)jex;  // non-decreasing over the chunks (at most 256 x 32 jobs)
-      __syncthreads();
-      for (int job = t; job < njobs; job += kLexThreads) {
-        // the job's chunk: the last chunk whose first job is <= job (a chunk
-        // without lanes shares its successor's first job, so it is skipped)
-        int lo = 0, hi = kLexThreads - 1;
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if ((int)sm->jfirst[mid] <= job) lo = mid;
-          else hi = mid - 1;
-        }
-        walk_lane(a, tb, sm, lo, job - (int)sm->jfirst[lo], job < kCodeJobs ? sm->jcodes + job * kLexWords : nullptr);
+    const int lanes = kind == kOpen ? [&] {
+      int c = 0;
+#pragma unroll
+      for (int i = 0; i < W; i++) c += __popcll(sm->cand[i][t]);
+      return c;
+    }() : 0;
+    int njobs;
+    // (the scan's barriers also end every window read before the walks
+    // below overwrite rows with codes)
+    const int jex = block_exclusive_scan<int>(lanes, AddI32(), 0, sm->scan_a, &njobs);
+    sm->jfirst[t] = (uint16_t)jex;  // non-decreasing over the chunks (at most 256 x 32 jobs)
+    LEX_PHASE(1);
+
+    // ---- walks: known chunks from their start; candidates of open chunks
+    // as jobs spread over the CTA ----
+    int x_end = dead;
+    if (kind == kKnown) {
+      if (x0 == dead) {
+        record_reject(st, &st->lex_reject_reason, 1);  // no state survives the window: invalid input
+      } else if (nb == kLexChunk) {
+        x_end = walk_chunk(tb, row, row, x0);
+      } else {
+        x_end = walk_bytes(tb, rb, nb, x0);
       }
+      if (g0 == 0) rb[0] = kNoBoundary;
+      sm->endst[t] = (uint8_t)(x_end < 0 ? 0 : x_end);
+      sm->start[t] = (uint8_t)(x0 < 0 ? 0 : x0);
+    }
+    __syncthreads();  // jfirst complete
+    if (a.diag && t == 0 && njobs) atomicAdd(&st->scratch[3], (unsigned long long)njobs);
+    for (int job = t; job < njobs; job += kLexThreads) {
+      // the job's chunk: the last chunk whose first job is <= job (a chunk
+      // without jobs shares its successor's first job, so it is skipped)
+      int lo = 0, hi = kLexThreads - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if ((int)sm->jfirst[mid] <= job) lo = mid;
+        else hi = mid - 1;
+      }
+      const int l = job - (int)sm->jfirst[lo];
+      const uint32_t *src = sm->bytes + kWinWords + lo * kLexWords;  // an open chunk's row: still its bytes
+      uint32_t *dst = job < kCodeJobs ? sm->jcodes + job * kLexWords : nullptr;
+      uint32_t f = row_of(tb, (uint32_t)cand_state(sm, lo, l));
+#pragma unroll 3
+      for (int w = 0; w < kLexWords; ++w) {
+        const uint32_t word = src[w];
+        const uint32_t e0 = step(tb, f, cls4_of(tb, __byte_perm(word, 0, 0x4440)));
+        const uint32_t e1 = step(tb, e0, cls4_of(tb, __byte_perm(word, 0, 0x4441)));
+        const uint32_t e2 = step(tb, e1, cls4_of(tb, __byte_perm(word, 0, 0x4442)));
+        const uint32_t e3 = step(tb, e2, cls4_of(tb, __byte_perm(word, 0, 0x4443)));
+        f = e3;
+        if (dst) dst[w] = pack_codes(e0, e1, e2, e3);
+      }
+      sm->lend[l * kLexThreads + lo] = (uint8_t)state_of(tb, f);
     }
     __syncthreads();
     LEX_PHASE(2);
 
-    // ---- resolution: nearest constant chunk before each chunk ----
-    const bool is_const = kind == kConst;
+    // ---- resolution: nearest known chunk before each chunk ----
     int ktot;
-    const int kex = block_exclusive_scan<int>(is_const ? t : -1, MaxI32(), -1, sm->scan_a, &ktot);
+    const int kex = block_exclusive_scan<int>(kind == kKnown ? t : -1, MaxI32(), -1, sm->scan_a, &ktot);
     sm->kconst[t] = kex;
-    if (t == kLexHalo) sm->need_lookback = kex < 0 ? 1 : 0;
     if (t == 0) sm->out_published = 0;
     if (a.diag) {
-      const int nconst = __syncthreads_count(is_const);
-      if (t == 0) atomicAdd(&st->scratch[1], (unsigned long long)nconst);
+      const int nknown = __syncthreads_count(kind == kKnown);
+      if (t == 0) atomicAdd(&st->scratch[1], (unsigned long long)nknown);
     }
     __syncthreads();
     LEX_PHASE(3);
@@ -443,10 +496,10 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
         sm->out_published = 1;
       }
     } else if (lt + 1 < tiles_t) {
-      // no constant chunk at all: publish the data region's transition vector
+      // no known chunk at all: publish the tile's transition vector
       for (int s = t; s < a.M; s += kLexThreads) {
         int x = s;
-        for (int jj = kLexHalo; jj < kLexThreads; ++jj) x = eval_chunk(a, sm, jj, x);
+        for (int jj = 0; jj < kLexThreads; ++jj) x = eval_chunk(a, sm, jj, x);
         a.st1_vec[tile * (unsigned long long)a.M + s] = (uint8_t)(x < 0 ? 0 : x);
       }
       __syncthreads();
@@ -456,7 +509,7 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
       }
     }
     __syncthreads();
-    if (sm->need_lookback) {
+    if (sm->kind[0] == kOpen || sm->kind[0] == kOpenTail) {  // the tile's incoming state: look back
       if (t == 0) {
         if (a.diag) atomicAdd(&st->scratch[0], 1ull);
         int s_in = a.m0;
@@ -487,9 +540,9 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
       }
       __syncthreads();
     }
-    // ---- each data chunk's start state ----
+    // ---- the start state of every chunk that is not known ----
     unsigned chain = 0;
-    if (t >= kLexHalo) {
+    if (kind != kKnown) {
       const int k = sm->kconst[t];
       int x, from;
       if (k >= 0) {
@@ -497,10 +550,11 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
         from = k + 1;
       } else {
         x = sm->s_in;
-        from = kLexHalo;
+        from = 0;
       }
       for (int jj = from; jj < t; ++jj) x = eval_chunk(a, sm, jj, x);
       sm->start[t] = (uint8_t)(x < 0 ? 0 : x);
+      x0 = x;
       chain = (unsigned)(t - from);
     }
     if (a.diag) {  // every lane of the warp takes part
@@ -516,48 +570,28 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
       st_release_u32(a.st1_flag + tile, 2u);
     }
 
-    // ---- pass 2: the bytes walked as a set (all of an open or partial
-    // chunk) again from the true start, writing their codes ----
+    // ---- open chunks: the true candidate's codes (or a walk from it) ----
     long long cnt = 0, lastb = 0;
     unsigned long long bmask = 0;
     bool final_kept = false;
-    int x_end = 0;
-    uint32_t *row = sm->bytes + t * kLexWords;
-    uint8_t *rb = reinterpret_cast<uint8_t *>(row);
-    if (t >= kLexHalo && nb > 0) {
-      const int x0 = sm->start[t];
-      bool died = x0 == dead;
-      uint32_t f = row_of(tb, (uint32_t)(x0 < 0 ? 0 : x0));
-      int slot = 0xff;
-      if (kind == kOpen && !died) {
-        slot = __ldg(a.lane_of + (size_t)sm->c0[t] * a.M + x0);
-        const int job = slot == 0xff ? kCodeJobs : (int)sm->jfirst[t] + slot;
-        if (job < kCodeJobs) {  // the true lane's codes, walked already: copy them
-          const uint32_t e0 = step(tb, f, cls4_of(tb, rb[0]));
+    if (kind == kOpenTail) {
+      x_end = x0 == dead || x0 < 0 ? dead : walk_bytes(tb, rb, nb, x0);
+    } else if (kind == kOpen) {
+      // (a start that is not a candidate: the true state died before the chunk)
+      const int slot = x0 == dead || x0 < 0 ? -1 : cand_slot(sm, t, x0);
+      if (slot >= 0) {
+        const int job = (int)sm->jfirst[t] + slot;
+        if (job < kCodeJobs) {
           const uint32_t *src = sm->jcodes + job * kLexWords;
 #pragma unroll
           for (int w = 0; w < kLexWords; ++w) row[w] = src[w];
-          rb[0] = g0 >= 1 ? (uint8_t)(e0 >> 24) : kNoBoundary;
-          jw = 0;  // nothing left to walk
+          x_end = sm->lend[slot * kLexThreads + t];
+        } else {
+          x_end = walk_chunk(tb, row, row, x0);
         }
       }
-      if (!died) {
-        for (int j = 0; j < jw; ++j) {
-          const uint32_t e = step(tb, f, cls4_of(tb, rb[j]));
-          rb[j] = (g0 + j >= 1) ? (uint8_t)(e >> 24) : kNoBoundary;
-          f = e;
-        }
-        died = state_of(tb, f) == dead;
-      }
-      if (kind == kConst) {
-        // the walk from the true start must meet the converged lane
-        if (!died && conv >= 0 && state_of(tb, f) != conv) atomicCAS(&st->error, 0, -1 /* internal error */);
-        x_end = died ? dead : end;
-      } else if (kind == kOpen && jw == 0) {
-        x_end = slot == 0xff ? dead : sm->lend[slot * kLexThreads + t];
-      } else {
-        x_end = died ? dead : state_of(tb, f);
-      }
+    }
+    if (nb > 0) {
       if (x_end == dead) record_reject(st, &st->lex_reject_reason, 1);
       // ---- boundaries (all) and kept boundaries (code < 0xFE, i.e.
       // (code | 1) != 0xFF) from the code words ----
@@ -598,7 +632,7 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
       }
       uint4 *dst = reinterpret_cast<uint4 *>(a.codes + tile * (unsigned long long)kLexData);
       const uint4 *src = reinterpret_cast<const uint4 *>(reinterpret_cast<const uint8_t *>(sm->bytes) +
-                                                         kLexHalo * kLexChunk);
+                                                         kLexWin);
       for (int v = t; v < kLexData / 16; v += kLexThreads) dst[v] = src[v];
       LEX_PHASE(7);
       continue;
@@ -625,7 +659,7 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
     LEX_PHASE(6);
 
     // ---- the kept tokens, straight into the outputs ----
-    if (t >= kLexHalo && nb > 0) {
+    if (nb > 0) {
       unsigned long long out = tok_base + (unsigned long long)(sm->cnt_prefix + cnt_ex);
       long long prev = sm->pos_prefix > pos_ex ? sm->pos_prefix : pos_ex;  // 0: the token starts at byte 0
       const unsigned long long len_max = a.len_max;
@@ -661,29 +695,21 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
 
 #undef LEX_PHASE
 
-__global__ void __launch_bounds__(kLexThreads, 5) lex_kernel(LexArgs args) {
-  extern __shared__ __align__(16) unsigned char dyn_smem[];
-  __shared__ __align__(16) LexSmem sm;
-  lex_body<1, true>(args, dyn_smem, &sm);
-}
+#define LEX_KERNEL(name, W, PS, STAGED)                          \
+  __global__ void __launch_bounds__(kLexThreads, 4) name(LexArgs args) { \
+    extern __shared__ __align__(16) unsigned char dyn_smem[];   \
+    __shared__ __align__(16) LexSmem<W> sm;                    \
+    lex_body<W, PS, STAGED>(args, dyn_smem, &sm);              \
+  }
 
-__global__ void __launch_bounds__(kLexThreads, 5) lex_kernel_wide(LexArgs args) {
-  extern __shared__ __align__(16) unsigned char dyn_smem[];
-  __shared__ __align__(16) LexSmem sm;
-  lex_body<4, true>(args, dyn_smem, &sm);
-}
+LEX_KERNEL(lex_kernel, 1, true, true)
+LEX_KERNEL(lex_kernel_wide, 4, true, true)
+LEX_KERNEL(lex_kernel_sets, 4, false, true)
+LEX_KERNEL(lex_direct_kernel, 1, true, false)
+LEX_KERNEL(lex_direct_kernel_wide, 4, true, false)
+LEX_KERNEL(lex_direct_kernel_sets, 4, false, false)
 
-__global__ void __launch_bounds__(kLexThreads, 5) lex_direct_kernel(LexArgs args) {
-  extern __shared__ __align__(16) unsigned char dyn_smem[];
-  __shared__ __align__(16) LexSmem sm;
-  lex_body<1, false>(args, dyn_smem, &sm);
-}
-
-__global__ void __launch_bounds__(kLexThreads, 5) lex_direct_kernel_wide(LexArgs args) {
-  extern __shared__ __align__(16) unsigned char dyn_smem[];
-  __shared__ __align__(16) LexSmem sm;
-  lex_body<4, false>(args, dyn_smem, &sm);
-}
+#undef LEX_KERNEL
 
 // ---------------------------------------------------------------------------
 // Scan and token writes of the staged lexer
@@ -766,7 +792,6 @@ __global__ void __launch_bounds__(256) lex_emit_kernel(LexEmitArgs a) {
   __shared__ __align__(16) uint32_t rows[kLexThreads * kLexWords];
   __shared__ int sa[8], sb[8];
   const int t = threadIdx.x;
-  constexpr int kChunks = kLexThreads - kLexHalo;  // data chunks per tile
   for (unsigned long long tile = blockIdx.x; tile < a.num_tiles; tile += gridDim.x) {
     long long n = (long long)a.n;
     unsigned long long lt = tile;
@@ -783,7 +808,7 @@ __global__ void __launch_bounds__(256) lex_emit_kernel(LexEmitArgs a) {
     __syncthreads();
     const long long g0 = (long long)lt * kLexData + (long long)t * kLexChunk;
     int nb = 0;
-    if (t < kChunks && g0 < n) nb = (int)min((long long)kLexChunk, n - g0);
+    if (g0 < n) nb = (int)min((long long)kLexChunk, n - g0);
     const uint32_t *row = rows + t * kLexWords;
     const uint8_t *rb = reinterpret_cast<const uint8_t *>(row);
     unsigned long long bmask = 0, kmask = 0;

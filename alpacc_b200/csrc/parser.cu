@@ -9,11 +9,14 @@
 //                 (+arity-1), with the match of each right bracket / the parent
 //                 of each production found as the previous element whose depth
 //                 is <= a query value, inside the tile; parents found are
-//                 written straight into the compacted tree (compact_tree); the
-//                 rest is queued (parser.c:74-87,103-118,126-153).
-// pse_resolve     queued queries walk back over tile minima, then chunk
-//                 minima, then the elements of one chunk, and emit the same
-//                 outputs.
+//                 written straight into the compacted tree (compact_tree). Each
+//                 tile stores its staircase (the elements a later query can
+//                 find) and the queries it could not answer
+//                 (parser.c:74-87,103-118,126-153).
+// pse_resolve     one warp per tile with queries: 32 queries at a time walk
+//                 back over tile minima (super-tile minima skip long runs) and
+//                 binary-search the answering tile's staircase, then emit the
+//                 same outputs.
 #include <climits>
 #include <cstdint>
 
@@ -262,11 +265,6 @@ struct PseSmem {
   long long tmp[kPseWarps];
   long long prefix_a, prefix_b;
 };
-
-__device__ __forceinline__ int pse_step(const PseArgs &a, uint32_t v) {
-  if (a.mode == kPseBrackets) return (v >> 31) ? 1 : -1;
-  return __ldg(a.arity + v) - 1;
-}
 
 constexpr int kPseSmemProds = 1024;  // production tables copied to shared memory up to this size
 
@@ -540,27 +538,6 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
       need &= need - 1u;
     }
   }
-  // ---- queue what the tile could not answer (warp-aggregated) ----
-  {
-    int pending = 0;
-#pragma unroll
-    for (int j = 0; j < kPseItems; ++j) pending += ans[j] == -1 ? 1 : 0;
-    if (__any_sync(0xffffffffu, pending != 0)) {
-      const int incl = warp_inclusive_scan(pending, [](int x, int y) { return x + y; });
-      unsigned long long base = 0;
-      if (lane == kWarp - 1) base = atomicAdd(a.queue_len, (unsigned long long)incl);
-      base = __shfl_sync(0xffffffffu, base, kWarp - 1);
-      unsigned long long qi = base + (unsigned long long)(incl - pending);
-#pragma unroll
-      for (int j = 0; j < kPseItems; ++j)
-        if (ans[j] == -1) {
-          if (qi < a.queue_cap) a.queue[qi] = ((unsigned long long)doc << 40) | (unsigned long long)(c0 + j);
-          else record_overflow(st);
-          ++qi;
-        }
-    }
-  }
-
   // ---- the tile's prefix: look-back by warp 0, now that predecessors had time ----
   if (t < kWarp) {
     Pair64 prefix{0, 0};
@@ -582,32 +559,80 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   }
   __syncthreads();
 
-  // ---- chunk state, tile minimum, tree nodes ----
+  // ---- staircase, unanswered queries, tile minimum ----
+  // An element is on the staircase when every later element of the tile is
+  // deeper: only those can answer a later tile's query. In position order the
+  // stairs' depths increase and the unanswered queries' values decrease.
   const int32_t off = (int32_t)((parents ? 1 : 0) + sm.prefix_a);
   const long long pb = sm.prefix_b;
-  const unsigned long long ci = tile * kPseThreads + t;
-  a.ch_h0[ci] = off + ex_s;
-  a.ch_min[ci] = cmin == INT_MAX ? INT_MAX : cmin + off;
-  if (parents) a.ch_tc[ci] = (int32_t)(pb + ex_t);
-  if (t == 0) {
-    int32_t r = sm.wmin[0];
+  {
+    int suf = cmin;  // minimum over this warp's chunks from this one on
 #pragma unroll
-    for (int w = 1; w < kPseWarps; ++w) r = sm.wmin[w] < r ? sm.wmin[w] : r;
-    const int32_t tm = r + off;  // the tile holds at least one element
-    a.tile_min[tile] = tm;
-    atomicMax(a.super_key + (tile >> kPseSuperShift), (uint32_t)((long long)INT_MAX - (long long)tm));
+    for (int d = 1; d < kWarp; d <<= 1) {
+      const int o = __shfl_down_sync(0xffffffffu, suf, d);
+      if (lane + d < kWarp && o < suf) suf = o;
+    }
+    int later = __shfl_down_sync(0xffffffffu, suf, 1);  // minimum over the later chunks of the tile
+    if (lane == kWarp - 1) later = INT_MAX;
+    for (int w = warp + 1; w < kPseWarps; ++w) later = sm.wmin[w] < later ? sm.wmin[w] : later;
+    // (depths, values and terminal counts are read back from shared memory:
+    // fewer registers live across the look-back)
+    const int row = t * kPseStride;
+    unsigned smask = 0, qmask = 0;
+#pragma unroll
+    for (int j = kPseItems - 1; j >= 0; --j) {
+      const int h = sm.h[row + j];
+      if (c0 + j < E && h < later) {
+        smask |= 1u << j;
+        later = h;
+      }
+      if (ans[j] == -1) qmask |= 1u << j;
+    }
+    long long ctot;
+    const long long cex = block_exclusive_scan<long long>((long long)__popc(smask) * kPack + __popc(qmask), AddI64(),
+                                                          0ll, sm.tmp, &ctot);
+    const unsigned long long base = tile * (unsigned long long)kPseTile;
+    unsigned long long si = base + (unsigned long long)(cex >> 32);
+    unsigned long long qi = base + (unsigned long long)(cex & 0xffffffffll);
+#pragma unroll
+    for (int j = 0; j < kPseItems; ++j) {
+      if (smask >> j & 1u) {
+        a.stair_off[si] = (uint16_t)(t * kPseItems + j);
+        a.stair_val[si] = sm.h[row + j] + off;
+        if (parents) a.stair_tc[si] = (int32_t)(pb + sm.tc[row + j]);
+        ++si;
+      }
+      if (qmask >> j & 1u) {
+        a.q_off[qi] = (uint16_t)(t * kPseItems + j);
+        a.q_val[qi] = sm.h[row + j] + off - (parents ? 0 : 1);
+        if (parents) a.q_tc[qi] = (int32_t)(pb + sm.tc[row + j]);
+        ++qi;
+      }
+    }
+    if (t == 0) {
+      int32_t r = sm.wmin[0];
+#pragma unroll
+      for (int w = 1; w < kPseWarps; ++w) r = sm.wmin[w] < r ? sm.wmin[w] : r;
+      const int32_t tm = r + off;  // the tile holds at least one element
+      a.tile_min[tile] = tm;
+      atomicMax(a.super_key + (tile >> kPseSuperShift), (uint32_t)((long long)INT_MAX - (long long)tm));
+      a.stair_cnt[tile] = (uint32_t)(ctot >> 32);
+      a.q_cnt[tile] = (uint32_t)(ctot & 0xffffffffll);
+    }
   }
   if (parents) {
+    const int row = t * kPseStride;
 #pragma unroll
     for (int j = 0; j < kPseItems; ++j) {
       const int an = ans[j];
-      const bool term = tcr[j] != (j > 0 ? tcr[j - 1] : 0);
+      const int tc = sm.tc[row + j];
+      const bool term = tc != (j > 0 ? sm.tc[row + j - 1] : ex_t);
       if (an == -3) {  // the root: compute_parents gives it parent 0
-        emit_node(a, dv, v[j], term, c0 + j, pb + ex_t + tcr[j], 0 - (pb + sm.tc[0]));
+        emit_node(a, dv, sm.v[row + j], term, c0 + j, pb + tc, 0 - (pb + sm.tc[0]));
       } else if (an >= 0) {
         const long long p = tile0 + an;
         const long long tinc_p = pb + sm.tc[(an / kPseItems) * kPseStride + an % kPseItems];
-        emit_node(a, dv, v[j], term, c0 + j, pb + ex_t + tcr[j], p - tinc_p);
+        emit_node(a, dv, sm.v[row + j], term, c0 + j, pb + tc, p - tinc_p);
       }
     }
   }
@@ -641,98 +666,104 @@ __device__ __forceinline__ long long warp_latest_le_key(const uint32_t *keys, lo
   return -1;
 }
 
-// Depth before each element of a chunk, for lanes 0..7 (lane l: element
-// eb + l of the document, the chunk's state at virtual chunk index cc); other
-// lanes and elements past the end get INT_MAX.
-__device__ __forceinline__ int32_t chunk_depth(const PseArgs &a, const PseDoc &dv, long long cc, long long eb,
-                                               int lane) {
-  const long long e = eb + lane;
-  const bool ok = lane < kPseItems && e < dv.E;
-  int stp = ok ? pse_step(a, dv.elems[e]) : 0;
-  const int32_t h0 = a.ch_h0[cc];
-#pragma unroll
-  for (int d = 1; d < kPseItems; d <<= 1) {
-    const int o = __shfl_up_sync(0xffffffffu, stp, d);
-    if (lane >= d) stp += o;
+// Latest tile in [first, hi] whose minimum is <= qv, or -1: the tiles of
+// hi's super-tile first, then the super-tile minima before it, then the tiles
+// of the super-tile found (never before the document's first tile).
+__device__ __forceinline__ long long latest_tile_le(const PseArgs &a, long long hi, long long first, int32_t qv,
+                                                    int lane) {
+  const long long sup0 = (hi >> kPseSuperShift) << kPseSuperShift;
+  long long tt = warp_latest_le(a.tile_min, hi, sup0 > first ? sup0 : first, qv, lane);
+  if (tt < 0 && sup0 > first) {
+    const long long sp =
+        warp_latest_le_key(a.super_key, (sup0 >> kPseSuperShift) - 1, first >> kPseSuperShift, qv, lane);
+    if (sp >= 0) {
+      const long long lo = sp << kPseSuperShift;
+      tt = warp_latest_le(a.tile_min, ((sp + 1) << kPseSuperShift) - 1, lo > first ? lo : first, qv, lane);
+    }
   }
-  const int excl = __shfl_up_sync(0xffffffffu, stp, 1);
-  return ok ? h0 + (lane > 0 ? excl : 0) : INT_MAX;
-}
-
-// Inclusive terminal-production count up to element x of the document (warp-wide call).
-__device__ __forceinline__ long long terminal_count(const PseArgs &a, const PseDoc &dv, long long x, int lane) {
-  const long long c = x / kPseItems;
-  const long long e = c * kPseItems + lane;
-  const bool t = lane <= (int)(x - c * kPseItems) && __ldg(a.is_term + dv.elems[e < x ? e : x]);
-  return (long long)a.ch_tc[(long long)dv.tile_first * kPseThreads + c] + __popc(__ballot_sync(0xffffffffu, t));
+  return tt;
 }
 
 }  // namespace
 
-// One warp per queued query: latest tile of the query's document whose
-// minimum is <= the query (within the query's super-tile of 256 tiles, else
-// via super-tile minima, never before the document's first tile), then the
-// latest chunk of that tile, then the latest element of that chunk (depths
-// recomputed from the chunk's start depth).
-__global__ void pse_resolve_kernel(PseArgs a) {
-  // the walk did not complete (no kernel sets these words while this one runs)
-  if (!a.batch && (*reinterpret_cast<volatile int *>(&a.status->error) ||
-                   *reinterpret_cast<volatile int *>(&a.status->overflow)))
-    return;
-  const unsigned long long qn = *a.queue_len;
+// One warp per tile with unanswered queries. The queries (values decreasing
+// in position order) are taken 32 at a time: the latest earlier tile whose
+// minimum is <= the first query's value answers that query and every later
+// one whose value is still >= that minimum (the tiles in between are deeper
+// than all of them); each such lane binary-searches the tile's staircase for
+// its last stair of depth <= its value. The walk back goes on from that tile
+// for the rest. Queries no tile answers: an unmatched right bracket, or
+// compute_parents' parent 0 of an empty stack.
+__global__ void __launch_bounds__(256) pse_resolve_kernel(PseArgs a) {
   const bool parents = a.mode == kPseParents;
+  unsigned long long total;
+  if (a.batch) {
+    total = (parents ? a.batch->pr_tile0 : a.batch->br_tile0)[a.batch->docs];
+  } else {
+    // the walk stopped early or not at all (no kernel sets these words while
+    // this one runs; the tile kernel checks the same words before it starts)
+    if (*reinterpret_cast<volatile int *>(&a.status->error) || *reinterpret_cast<volatile int *>(&a.status->reject) ||
+        *reinterpret_cast<volatile int *>(&a.status->overflow))
+      return;
+    const unsigned long long E = *a.count;
+    if (E > a.elem_cap) return;
+    total = (E + kPseTile - 1) / kPseTile;
+  }
   const int lane = threadIdx.x & 31;
-  const unsigned long long warp = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) >> 5;
-  const unsigned long long warps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
-  for (unsigned long long qi = warp; qi < qn && qi < a.queue_cap; qi += warps) {
-    const unsigned long long qe = a.queue[qi];
-    const int doc = (int)(qe >> 40);
-    const long long e = (long long)(qe & ((1ull << 40) - 1));
-    PseDoc dv;
-    if (a.batch) {
-      const unsigned long long *tile0 = parents ? a.batch->pr_tile0 : a.batch->br_tile0;
-      int dd;
-      dv = pse_doc(a, tile0[doc], &dd);  // the document's first tile
-    } else {
-      int dd;
-      dv = pse_doc(a, 0, &dd);
-    }
+  for (;;) {
+    unsigned long long tile = 0;
+    if (lane == 0) tile = atomicAdd(a.resolve_ticket, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if (tile >= total) break;
+    int doc;
+    const PseDoc dv = pse_doc(a, tile, &doc);
+    const long long first = (long long)dv.tile_first;
+    if ((long long)(tile - first) * kPseTile >= dv.E) continue;
+    const unsigned nq = a.q_cnt[tile];
+    if (nq == 0) continue;
     DeviceStatus *st = dv.st;
-    const long long first = (long long)dv.tile_first;  // virtual tiles of the document start here
-    const uint32_t v = dv.elems[e];
-    const long long ce = e / kPseItems;
-    const int32_t he = __shfl_sync(0xffffffffu, chunk_depth(a, dv, first * kPseThreads + ce, ce * kPseItems, lane),
-                                   (int)(e - ce * kPseItems));
-    const int32_t qv = parents ? he : he - 1;
-    const long long tile = first + e / kPseTile;
-    const long long sup0 = (tile >> kPseSuperShift) << kPseSuperShift;
-    long long tt = warp_latest_le(a.tile_min, tile - 1, sup0 > first ? sup0 : first, qv, lane);
-    if (tt < 0 && sup0 > first) {
-      const long long sp =
-          warp_latest_le_key(a.super_key, (sup0 >> kPseSuperShift) - 1, first >> kPseSuperShift, qv, lane);
-      if (sp >= 0) {
-        const long long lo = sp << kPseSuperShift;
-        tt = warp_latest_le(a.tile_min, ((sp + 1) << kPseSuperShift) - 1, lo > first ? lo : first, qv, lane);
+    const unsigned long long qb = tile * (unsigned long long)kPseTile;
+    const long long ebase = (long long)(tile - first) * kPseTile;
+    long long j = (long long)tile - 1;  // answering tiles are at most this one
+    unsigned q = 0;
+    while (q < nq) {
+      const unsigned qi = q + lane;
+      const bool have = qi < nq;
+      const int32_t qv = have ? a.q_val[qb + qi] : INT_MIN;
+      j = j >= first ? latest_tile_le(a, j, first, __shfl_sync(0xffffffffu, qv, 0), lane) : -1;
+      if (j < 0) break;
+      const int32_t tm = a.tile_min[j];
+      const bool ok = have && qv >= tm;
+      if (ok) {
+        const unsigned long long sb = (unsigned long long)j * kPseTile;
+        int lo = 0, hi = (int)a.stair_cnt[j] - 1;  // stair_val[sb] == tm <= qv
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (a.stair_val[sb + mid] <= qv) lo = mid;
+          else hi = mid - 1;
+        }
+        const long long e = ebase + a.q_off[qb + qi];
+        const long long p = (j - first) * kPseTile + a.stair_off[sb + lo];
+        const uint32_t v = dv.elems[e];
+        if (parents) {
+          emit_node(a, dv, v, __ldg(a.is_term + v) != 0, e, a.q_tc[qb + qi], p - a.stair_tc[sb + lo]);
+        } else if ((dv.elems[p] ^ v) & 0x7fffffffu) {
+          record_reject(st, &st->parse_reject_reason, 2);
+        }
       }
+      q += __popc(__ballot_sync(0xffffffffu, ok));  // lane 0 is answered: progress
     }
-    long long found = -1;
-    if (tt >= 0) {
-      const long long c = warp_latest_le(a.ch_min + tt * kPseThreads, kPseThreads - 1, 0, qv, lane);
-      if (c >= 0) {
-        const long long eb = (tt - first) * kPseTile + c * kPseItems;  // element index in the document
-        const unsigned b = __ballot_sync(0xffffffffu, chunk_depth(a, dv, tt * kPseThreads + c, eb, lane) <= qv);
-        if (b) found = eb + (31 - __clz(b));
+    if (q < nq) {  // no earlier tile answers the rest
+      if (!parents) {
+        if (lane == 0) record_reject(st, &st->parse_reject_reason, 3);
+        continue;
       }
-    }
-    if (parents) {
-      // compute_parents takes 0 when its stack is empty
-      const long long p = found >= 0 ? found : 0;
-      const long long tinc_p = terminal_count(a, dv, p, lane);
-      const long long tinc_e = terminal_count(a, dv, e, lane);
-      if (lane == 0) emit_node(a, dv, v, __ldg(a.is_term + v) != 0, e, tinc_e, p - tinc_p);
-    } else if (lane == 0) {
-      if (found < 0) record_reject(st, &st->parse_reject_reason, 3);
-      else if ((dv.elems[found] & 0x7fffffffu) != (v & 0x7fffffffu)) record_reject(st, &st->parse_reject_reason, 2);
+      const long long tinc0 = __ldg(a.is_term + dv.elems[0]) ? 1 : 0;  // inclusive terminal count at element 0
+      for (unsigned qi = q + lane; qi < nq; qi += kWarp) {
+        const long long e = ebase + a.q_off[qb + qi];
+        const uint32_t v = dv.elems[e];
+        emit_node(a, dv, v, __ldg(a.is_term + v) != 0, e, a.q_tc[qb + qi], 0 - tinc0);
+      }
     }
   }
 }

@@ -24,10 +24,12 @@ inline LexArgs lex_args(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, 
   a.wide_cls = g->wide_cls;
   a.cp_shift = g->cp_shift;
   a.swz = g->swz;
-  a.lane_of = (const uint8_t *)g->lane_of.p;
+  a.ps_tab = g->ps_words ? (const uint32_t *)g->lex_ps.p : nullptr;
+  a.ps_words = g->ps_words;
+  a.ps_full = g->ps_full;
+  a.ps_mask = (const unsigned long long *)g->lex_psmask.p;
   a.img = (const uint8_t *)g->img.p;
   a.img_cnt = (const uint8_t *)g->img_cnt.p;
-  a.img2 = lm.img2.empty() ? nullptr : (const unsigned long long *)g->img2.p;
   a.sterm = (const uint8_t *)g->sterm.p;
   a.sflags = (const uint8_t *)g->sflags.p;
   a.M = lm.M;
@@ -55,17 +57,26 @@ inline LexArgs lex_args(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, 
   return a;
 }
 
+// The lexer kernels by variant (alpacc_gpu_grammar::lex_variant).
+using LexKernel = void (*)(LexArgs);
+inline LexKernel lex_staged_kernel(const alpacc_gpu_grammar *g) {
+  static const LexKernel k[3] = {lex_kernel, lex_kernel_wide, lex_kernel_sets};
+  return k[g->lex_variant];
+}
+inline LexKernel lex_direct_kernel_of(const alpacc_gpu_grammar *g) {
+  static const LexKernel k[3] = {lex_direct_kernel, lex_direct_kernel_wide, lex_direct_kernel_sets};
+  return k[g->lex_variant];
+}
+
 // The staged lexer kernel for this handle's machine (codes and tile totals).
 inline cudaError_t launch_lex(const alpacc_gpu_grammar *g, const LexArgs &a, unsigned grid, cudaStream_t s) {
-  if (g->lex_w4) lex_kernel_wide<<<grid, kLexThreads, lex_dyn_smem(g), s>>>(a);
-  else lex_kernel<<<grid, kLexThreads, lex_dyn_smem(g), s>>>(a);
+  lex_staged_kernel(g)<<<grid, kLexThreads, lex_dyn_smem(g), s>>>(a);
   return cudaGetLastError();
 }
 
 // The direct lexer kernel (tokens written by the kernel itself).
 inline cudaError_t launch_lex_direct(const alpacc_gpu_grammar *g, const LexArgs &a, unsigned grid, cudaStream_t s) {
-  if (g->lex_w4) lex_direct_kernel_wide<<<grid, kLexThreads, lex_dyn_smem(g), s>>>(a);
-  else lex_direct_kernel<<<grid, kLexThreads, lex_dyn_smem(g), s>>>(a);
+  lex_direct_kernel_of(g)<<<grid, kLexThreads, lex_dyn_smem(g), s>>>(a);
   return cudaGetLastError();
 }
 
@@ -100,11 +111,9 @@ inline cudaError_t launch_lex_emit(const LexEmitArgs &e, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-// Resident CTAs of that kernel per SM.
+// Resident CTAs of the staged lexer kernel per SM.
 inline cudaError_t lex_occupancy(const alpacc_gpu_grammar *g, int *per_sm) {
-  return g->lex_w4 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, lex_kernel_wide, kLexThreads,
-                                                                   lex_dyn_smem(g))
-                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, lex_kernel, kLexThreads, lex_dyn_smem(g));
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, lex_staged_kernel(g), kLexThreads, lex_dyn_smem(g));
 }
 
 inline PairArgs pair_args(alpacc_gpu_grammar *g) {
@@ -137,7 +146,14 @@ inline PairArgs pair_args(alpacc_gpu_grammar *g) {
   return a;
 }
 
-inline PseArgs pse_args(alpacc_gpu_grammar *g, int mode, unsigned long long queue_cap) {
+// Bytes of the walk's per-tile regions for `tiles` tiles: staircase depths,
+// query values, their terminal counts (4 bytes each per entry), staircase and
+// query offsets (2 bytes each), then the two per-tile counts.
+inline uint64_t pse_region_bytes(uint64_t tiles) {
+  return std::max<uint64_t>(tiles, 1) * ((uint64_t)kPseTile * 20 + 8);
+}
+
+inline PseArgs pse_args(alpacc_gpu_grammar *g, int mode, uint64_t tiles) {
   const alpacc_tables &tb = g->hg.t;
   PseArgs a{};
   a.mode = mode;
@@ -147,20 +163,25 @@ inline PseArgs pse_args(alpacc_gpu_grammar *g, int mode, unsigned long long queu
   a.arity = (const int32_t *)g->arity.p;
   a.is_term = (const uint8_t *)g->is_term.p;
   a.num_prods = (int)g->hg.pairs.arity.size();
-  a.ch_h0 = (int32_t *)g->ch_h0.p;
-  a.ch_min = (int32_t *)g->chunk_min.p;
-  a.ch_tc = (int32_t *)g->ch_tc.p;
   a.tile_min = (int32_t *)g->tile_min.p;
   a.super_key = (uint32_t *)g->super_key.p;
-  a.queue = (unsigned long long *)g->queue.p;
-  a.queue_cap = queue_cap;
-  a.queue_len = (unsigned long long *)g->queue_len.p;
+  const uint64_t entries = std::max<uint64_t>(tiles, 1) * kPseTile;
+  uint8_t *r = (uint8_t *)g->pse_regions.p;
+  a.stair_val = (int32_t *)r;
+  a.q_val = a.stair_val + entries;
+  a.stair_tc = a.q_val + entries;
+  a.q_tc = a.stair_tc + entries;
+  a.stair_off = (uint16_t *)(a.q_tc + entries);
+  a.q_off = a.stair_off + entries;
+  a.stair_cnt = (uint32_t *)(a.q_off + entries);
+  a.q_cnt = a.stair_cnt + std::max<uint64_t>(tiles, 1);
   a.node_prods = g->node_prods.p;
   a.node_parents = g->node_parents.p;
   a.token_parents = g->token_parents.p;
   a.prod_w = (int)tb.production_size;
   a.idx_w = (int)tb.index_size;
   a.ticket = (unsigned *)g->pse_ticket.p;
+  a.resolve_ticket = a.ticket + 1;
   a.st = PairTileState{(unsigned *)g->pse_flags.p, (unsigned long long *)g->pse_agg.p,
                        (unsigned long long *)g->pse_inc.p};
   a.status = g->d_status;

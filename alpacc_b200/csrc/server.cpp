@@ -3,12 +3,15 @@
 // The reference's `--server` mode (backends/c/cli.c:153-161,
 // backends/cuda/cli.cu:846-875) answers counted batches one input at a time.
 // Here requests are submitted individually and whenever a worker is free it
-// takes every queued request that fits its share of the device scratch budget
-// and runs them as one batch (alpacc_gpu_parse_batch) on its own grammar
+// takes every queued request whose batch still fits its share of the device
+// scratch budget - the exact bytes the batch path grows the worker's handle
+// to, so the handle never holds more than that share unless a single request
+// needs more on its own - and runs them as one batch (alpacc_gpu_parse_batch) on its own grammar
 // handle and stream. With several workers, requests that arrive while one
 // batch is on the GPU are admitted into the next worker's batch, so batches
 // overlap on the device. Each result is identical to parsing its input alone.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -21,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/alpacc_b200.h"
+#include "scratch.h"
 
 namespace {
 
@@ -36,10 +40,6 @@ struct Request {
   alpacc_result res{};
 };
 
-// Device scratch one input of n bytes may need at most (tokens, staging,
-// brackets, productions, walk state, outputs), with a fixed part per input.
-uint64_t scratch_estimate(uint64_t n) { return 96 * n + 16384; }
-
 }  // namespace
 
 struct alpacc_server {
@@ -54,6 +54,7 @@ struct alpacc_server {
   uint32_t max_batch = 8192;
   bool stopping = false;
   int64_t batches = 0, served = 0, largest_batch = 0;
+  uint64_t max_held = 0;  // most batch scratch any worker's handle held
 };
 
 namespace {
@@ -65,21 +66,24 @@ void worker_loop(alpacc_server *s, int w) {
   std::vector<Request *> batch;
   std::vector<int64_t> offs;
   std::vector<alpacc_result> outs;
+  alpacc::BatchSizes sizes;
   for (;;) {
     batch.clear();
     {
       std::unique_lock<std::mutex> lock(s->mu);
       s->cv_work.wait(lock, [&] { return s->stopping || !s->queue.empty(); });
       if (s->queue.empty()) break;  // stopping
-      uint64_t used = 0;
+      alpacc::BatchSizes z;
       while (!s->queue.empty() && batch.size() < s->max_batch) {
         Request *r = s->queue.front();
-        const uint64_t need = scratch_estimate(r->data.size());
-        if (!batch.empty() && used + need > s->budget_per_worker) break;  // admitted by memory budget
-        used += need;
+        alpacc::BatchSizes z2 = z;
+        z2.add(g, r->data.size());
+        if (!batch.empty() && alpacc::batch_scratch_bytes(g, z2) > s->budget_per_worker) break;
+        z = z2;
         batch.push_back(r);
         s->queue.pop_front();
       }
+      sizes = z;
       s->batches++;
       if ((int64_t)batch.size() > s->largest_batch) s->largest_batch = (int64_t)batch.size();
     }
@@ -102,7 +106,9 @@ void worker_loop(alpacc_server *s, int w) {
     for (size_t i = 0; i < batch.size(); i++)
       if (!batch[i]->data.empty()) std::memcpy(buf + offs[i], batch[i]->data.data(), batch[i]->data.size());
     outs.assign(batch.size(), alpacc_result{});
+    alpacc::fit_batch_scratch(g, sizes, s->budget_per_worker);
     const int rc = alpacc_gpu_parse_batch(g, buf, offs.data(), (uint32_t)batch.size(), outs.data());
+    const uint64_t held = alpacc::batch_scratch_held(g);
     const Clock::time_point now = Clock::now();
     {
       std::lock_guard<std::mutex> lock(s->mu);
@@ -116,6 +122,7 @@ void worker_loop(alpacc_server *s, int w) {
         r->data.shrink_to_fit();
       }
       s->served += (int64_t)batch.size();
+      if (held > s->max_held) s->max_held = held;
     }
     s->cv_done.notify_all();
   }
@@ -135,7 +142,7 @@ alpacc_server *alpacc_server_start(const alpacc_tables *tables, int device, int 
     return nullptr;
   }
   alpacc_server *s = new alpacc_server();
-  s->budget_per_worker = std::max<uint64_t>(scratch_budget / (uint64_t)workers, scratch_estimate(1));
+  s->budget_per_worker = scratch_budget / (uint64_t)workers;
   for (int i = 0; i < workers; i++) {
     alpacc_gpu_grammar *g = alpacc_gpu_load(tables, device, 0, err);
     if (!g) {
@@ -192,9 +199,10 @@ int alpacc_server_wait(alpacc_server *s, uint64_t id, alpacc_result *out, double
 int alpacc_server_stats(alpacc_server *s, int64_t *vals, int n) {
   if (!s || !vals) return ALPACC_E_INVALID;
   std::lock_guard<std::mutex> lock(s->mu);
-  const int64_t v[4] = {s->batches, s->served, s->largest_batch, (int64_t)s->queue.size()};
-  for (int i = 0; i < n && i < 4; i++) vals[i] = v[i];
-  return 4;
+  const int64_t v[6] = {s->batches,        s->served,           s->largest_batch, (int64_t)s->queue.size(),
+                        (int64_t)s->max_held, (int64_t)s->budget_per_worker};
+  for (int i = 0; i < n && i < 6; i++) vals[i] = v[i];
+  return 6;
 }
 
 void alpacc_server_stop(alpacc_server *s) {
@@ -211,6 +219,95 @@ void alpacc_server_stop(alpacc_server *s) {
   }
   for (alpacc_gpu_grammar *g : s->handles) alpacc_gpu_free(g);
   delete s;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Trace replay (load generation for measurement)
+// ---------------------------------------------------------------------------
+
+namespace {
+
+// Sleeps until t, spinning for the last 100 microseconds (sleep_until alone
+// wakes tens of microseconds late, more than the gap between arrivals at high
+// rates).
+void wait_until(Clock::time_point t) {
+  for (;;) {
+    const Clock::time_point now = Clock::now();
+    if (now >= t) return;
+    if (t - now > std::chrono::microseconds(200)) std::this_thread::sleep_for(t - now - std::chrono::microseconds(100));
+  }
+}
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+}  // namespace
+
+extern "C" {
+
+int alpacc_server_replay(alpacc_server *s, const uint8_t *bytes, const int64_t *offsets, const uint32_t *doc,
+                         uint64_t count, const double *arrival_s, double *latency_ms, int *status,
+                         double *elapsed_s) {
+  if (!s || !offsets || !doc || !arrival_s || !latency_ms || !status) return ALPACC_E_INVALID;
+  std::vector<uint64_t> ids(count, 0);
+  std::vector<Clock::time_point> sub_at(count);
+  std::atomic<uint64_t> submitted{0};
+  const Clock::time_point t0 = Clock::now() + std::chrono::milliseconds(2);
+  auto at = [&](uint64_t i) { return t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(arrival_s[i])); };
+  std::thread sub([&] {
+    for (uint64_t i = 0; i < count; i++) {
+      wait_until(at(i));
+      const uint32_t d = doc[i];
+      const uint64_t n = (uint64_t)(offsets[d + 1] - offsets[d]);
+      sub_at[i] = Clock::now();
+      if (alpacc_server_submit(s, n ? bytes + offsets[d] : nullptr, n, &ids[i]) != ALPACC_OK) ids[i] = 0;
+      submitted.store(i + 1, std::memory_order_release);
+    }
+  });
+  Clock::time_point last = t0;
+  for (uint64_t i = 0; i < count; i++) {
+    while (submitted.load(std::memory_order_acquire) <= i) std::this_thread::yield();
+    if (!ids[i]) {
+      status[i] = ALPACC_E_INVALID;
+      latency_ms[i] = -1.0;
+      continue;
+    }
+    alpacc_result r{};
+    double ms = 0;
+    status[i] = alpacc_server_wait(s, ids[i], &r, &ms);
+    alpacc_result_free(&r);
+    // from the scheduled arrival: the time the submitter lagged counts
+    const Clock::time_point done = sub_at[i] + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double, std::milli>(ms));
+    latency_ms[i] = ms_between(at(i), done);
+    if (done > last) last = done;
+  }
+  sub.join();
+  if (elapsed_s) *elapsed_s = std::chrono::duration<double>(last - t0).count();
+  return ALPACC_OK;
+}
+
+int alpacc_gpu_replay(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offsets, const uint32_t *doc,
+                      uint64_t count, const double *arrival_s, double *latency_ms, int *status, double *elapsed_s) {
+  if (!g || !offsets || !doc || !arrival_s || !latency_ms || !status) return ALPACC_E_INVALID;
+  const Clock::time_point t0 = Clock::now() + std::chrono::milliseconds(2);
+  Clock::time_point last = t0;
+  for (uint64_t i = 0; i < count; i++) {
+    const Clock::time_point at =
+        t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(arrival_s[i]));
+    wait_until(at);
+    const uint32_t d = doc[i];
+    const uint64_t n = (uint64_t)(offsets[d + 1] - offsets[d]);
+    alpacc_result r{};
+    status[i] = alpacc_gpu_parse(g, n ? bytes + offsets[d] : nullptr, n, &r);
+    alpacc_result_free(&r);
+    last = Clock::now();
+    latency_ms[i] = ms_between(at, last);
+  }
+  if (elapsed_s) *elapsed_s = std::chrono::duration<double>(last - t0).count();
+  return ALPACC_OK;
 }
 
 }  // extern "C"

@@ -104,6 +104,10 @@ def lib():
         L.alpacc_server_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
         L.alpacc_server_stop.restype = None
         L.alpacc_server_stop.argtypes = [ctypes.c_void_p]
+        for f in (L.alpacc_server_replay, L.alpacc_gpu_replay):
+            f.restype = ctypes.c_int
+            f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
         L.alpacc_gpu_autotune.restype = ctypes.c_int
         L.alpacc_gpu_autotune.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                           ctypes.POINTER(ctypes.c_int)]
@@ -213,6 +217,24 @@ def _np_from(ptr, count, nbytes, signed=False):
     dt = np.dtype(("i" if signed else "u") + str(nbytes))
     buf = (ctypes.c_char * (count * nbytes)).from_address(ptr)
     return np.frombuffer(buf, dtype=dt, count=count).copy()
+
+
+
+def _replay(fn, handle, pool: bytes, offsets, doc, arrival_s):
+    """Shared body of the trace replays: (latency ms, status, elapsed s)."""
+    buf = np.frombuffer(pool, dtype=np.uint8)
+    offs = np.ascontiguousarray(offsets, dtype=np.int64)
+    doc = np.ascontiguousarray(doc, dtype=np.uint32)
+    arr = np.ascontiguousarray(arrival_s, dtype=np.float64)
+    n = len(doc)
+    lat = np.zeros(n, dtype=np.float64)
+    st = np.zeros(n, dtype=np.int32)
+    el = ctypes.c_double(0)
+    rc = fn(handle, buf.ctypes.data if buf.size else None, offs.ctypes.data, doc.ctypes.data, n, arr.ctypes.data,
+            lat.ctypes.data, st.ctypes.data, ctypes.byref(el))
+    if rc < 0:
+        raise AlpaccError(rc, lib().alpacc_strerror(rc).decode())
+    return lat, st, el.value
 
 
 class Parser:
@@ -408,10 +430,10 @@ class Parser:
         vals = (ctypes.c_int64 * 17)()
         lib().alpacc_gpu_counts(self._h, vals, 17)
         return {"T": vals[0], "B": vals[1], "P": vals[2], "N": vals[3], "lookback_tiles": vals[4],
-                "const_chunks": vals[5], "chain_evals": vals[6], "set_walk_bytes": vals[7], "launches": vals[8],
+                "known_chunks": vals[5], "chain_evals": vals[6], "candidate_jobs": vals[7], "launches": vals[8],
                 "lexer_phase_cycles": {k: vals[9 + i] for i, k in enumerate(
-                    ("load", "pass1", "lane_jobs", "const_scan", "start_states", "pass2_masks_scan",
-                     "count_lookback", "token_writes"))}}
+                    ("load", "window", "walks", "known_scan", "start_states", "open_codes_masks_scan",
+                     "count_lookback", "writes"))}}
 
     def set_diagnostics(self, on: bool):
         lib().alpacc_gpu_set_diagnostics(self._h, 1 if on else 0)
@@ -430,6 +452,12 @@ class Parser:
     @staticmethod
     def free_result(r: Result):
         lib().alpacc_result_free(ctypes.byref(r))
+
+    def replay(self, pool: bytes, offsets, doc, arrival_s):
+        """One plain parse per request of a timed trace (alpacc_gpu_replay):
+        request i is input doc[i] of the pool, arriving arrival_s[i] seconds
+        after the start. Returns (latency ms, status, elapsed s)."""
+        return _replay(self._lib.alpacc_gpu_replay, self._h, pool, offsets, doc, arrival_s)
 
     def record_digest_raw(self, host_ptr: int, n: int):
         """(status, SHA-256 hex, byte count) of the combined-mode response
@@ -530,10 +558,16 @@ class Server:
         finally:
             self._lib.alpacc_result_free(ctypes.byref(r))
 
+    def replay(self, pool: bytes, offsets, doc, arrival_s):
+        """The trace submitted from a native thread at its arrival times
+        (alpacc_server_replay). Returns (latency ms, status, elapsed s)."""
+        return _replay(self._lib.alpacc_server_replay, self._s, pool, offsets, doc, arrival_s)
+
     def stats(self) -> dict:
-        v = (ctypes.c_int64 * 4)()
-        self._lib.alpacc_server_stats(self._s, v, 4)
-        return {"batches": v[0], "served": v[1], "largest_batch": v[2], "queued": v[3]}
+        v = (ctypes.c_int64 * 6)()
+        self._lib.alpacc_server_stats(self._s, v, 6)
+        return {"batches": v[0], "served": v[1], "largest_batch": v[2], "queued": v[3], "max_scratch_held": v[4],
+                "scratch_share": v[5]}
 
     def close(self):
         if getattr(self, "_s", None):

@@ -53,7 +53,7 @@ WORKLOADS = {
                        "64 B to 16 MiB; %d MiB)"),
 }
 
-SERVE_RATES = (2000, 5000, 10000, 20000, 50000)
+SERVE_RATES = (2000, 5000, 10000, 20000, 50000, 100000)
 
 
 def _pct(x, q):
@@ -62,12 +62,12 @@ def _pct(x, q):
 
 
 def ours_serve(a, rank, world, local_rank, dist):
-    """The served form: a seeded Poisson trace of JSON requests replayed in
-    real time against alpacc_server (continuous batching, 8 GiB scratch
-    budget) and against one plain alpacc_gpu_parse per request in arrival
-    order; p50/p99 latency (arrival to result) and GB/s per arrival rate."""
-    import threading
-
+    """The served form: per arrival rate, a seeded Poisson trace of at least
+    --serve-seconds of JSON requests (drawn from a pool of seeded documents
+    with log-normal sizes) replayed in real time from a native client thread
+    against alpacc_server (continuous batching, 8 GiB scratch budget), and the
+    same trace as one plain alpacc_gpu_parse per request in arrival order;
+    p50/p99 latency (scheduled arrival to result) and GB/s per rate."""
     import numpy as np
     import torch
 
@@ -78,69 +78,49 @@ def ours_serve(a, rank, world, local_rank, dist):
     torch.cuda.set_device(local_rank)
     wl = WORKLOADS["serve"]
     tables = load_tables(os.path.join(REPO, "grammars", wl["grammar"]), index32=True)
-    count = a.serve_requests
-    docs, _ = W.json_trace(count, 1.0, seed=5 + rank)
-    sizes = np.array([len(d) for d in docs], dtype=np.int64)
+    pool, offs = W.json_batch(a.serve_pool, 16384, 64, 16 << 20, 5 + rank)
+    offs = np.asarray(offs, dtype=np.int64)
+    sizes = np.diff(offs)
     srv = Server(tables, device=local_rank, workers=2, budget=8 << 30)
     plain = Parser(tables, device=local_rank, max_input=int(sizes.max()))
-    pins = [np.frombuffer(d, dtype=np.uint8) for d in docs]
-    for d in docs[:32]:  # warm-up of both paths
-        srv.wait(srv.submit(d))
-        plain.parse(d)
+    warm = np.arange(min(64, len(sizes)), dtype=np.uint32)
+    srv.replay(pool, offs, warm, np.zeros(len(warm)))
+    plain.replay(pool, offs, warm, np.zeros(len(warm)))
+    rates = [int(r) for r in a.serve_rates.split(",")]
     sweep = []
-    for rate in SERVE_RATES:
-        gaps = np.random.default_rng(1000 + rate).exponential(1.0 / rate, count)
+    total_req = 0
+    for rate in rates:
+        rng = np.random.default_rng(1000 + rate)
+        count = max(int(rate * a.serve_seconds), 1000)
+        gaps = rng.exponential(1.0 / rate, count)
         arr = np.cumsum(gaps) - gaps[0]
-        # continuous batching
-        ids = [None] * count
-        t0 = time.perf_counter() + 0.01
-
-        def submitter():
-            for i in range(count):
-                dt = t0 + arr[i] - time.perf_counter()
-                if dt > 0:
-                    time.sleep(dt)
-                ids[i] = srv.submit(docs[i])
-
-        th = threading.Thread(target=submitter)
-        th.start()
-        lat = []
-        last = t0
-        for i in range(count):
-            while ids[i] is None:
-                time.sleep(0.0001)
-            r, ms = srv.wait(ids[i])
-            lat.append(ms)
-            last = max(last, time.perf_counter())
-        th.join()
-        served_gbs = float(sizes.sum()) / (last - t0) / 1e9
-        # one plain call per request, in arrival order
-        plat = []
-        t1 = time.perf_counter() + 0.01
-        for i in range(count):
-            dt = t1 + arr[i] - time.perf_counter()
-            if dt > 0:
-                time.sleep(dt)
-            rc, res = plain.parse_raw(pins[i].ctypes.data, len(pins[i]))
-            Parser.free_result(res)
-            plat.append((time.perf_counter() - (t1 + arr[i])) * 1e3)
-        plain_gbs = float(sizes.sum()) / (time.perf_counter() - t1) / 1e9
-        sweep.append({"rate_per_s": rate, "p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99), "gbs": served_gbs,
-                      "plain_p50_ms": _pct(plat, 50), "plain_p99_ms": _pct(plat, 99), "plain_gbs": plain_gbs})
-    st = srv.stats()
+        doc = rng.integers(0, len(sizes), count).astype(np.uint32)
+        nbytes = float(sizes[doc].sum())
+        lat, st, el = srv.replay(pool, offs, doc, arr)
+        plat, pst, pel = plain.replay(pool, offs, doc, arr)
+        if (st != 0).any() or (pst != 0).any():
+            raise SystemExit("serve: %d served and %d plain requests did not parse" % ((st != 0).sum(), (pst != 0).sum()))
+        total_req += count
+        sweep.append({"rate_per_s": rate, "requests": count, "arrival_s": float(arr[-1]), "bytes": int(nbytes),
+                      "p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99), "gbs": nbytes / el / 1e9,
+                      "plain_p50_ms": _pct(plat, 50), "plain_p99_ms": _pct(plat, 99), "plain_gbs": nbytes / pel / 1e9})
+    stt = srv.stats()
     srv.close()
     if rank != 0:
         return
     top = sweep[-1]
     line = {
-        "metric": METRIC, "value": top["gbs"], "unit": "GB/s", "n_gpus": world, "steps": len(SERVE_RATES),
-        "warmup": 32, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "u8", "data": "synthetic (seeded JSON requests, seeded Poisson arrivals)",
-        "config": dict(workload_config(int(sizes.sum()), world, "serve"), requests=count, workers=2,
-                       scratch_budget_gib=8, batches=st["batches"], largest_batch=st["largest_batch"]),
+        "metric": METRIC, "value": top["gbs"], "unit": "GB/s", "n_gpus": world, "steps": len(rates),
+        "warmup": len(warm), "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8", "data": "synthetic (seeded JSON request pool, seeded Poisson arrivals)",
+        "config": dict(workload_config(int(sizes.sum()), world, "serve"), pool=len(sizes), requests=total_req,
+                       seconds_per_rate=a.serve_seconds, workers=2, scratch_budget_gib=8,
+                       batches=stt["batches"], largest_batch=stt["largest_batch"],
+                       max_scratch_held=stt["max_scratch_held"], scratch_share=stt["scratch_share"]),
         "serve": sweep,
         "p99_ms_at_max_rate": top["p99_ms"], "plain_p99_ms_at_max_rate": top["plain_p99_ms"],
-        "e2e": {"value": top["gbs"], "unit": "GB/s", "h2d_bytes_per_step": int(sizes.sum()), "d2h_bytes_per_step": None,
+        "served_over_plain_at_max_rate": top["gbs"] / top["plain_gbs"],
+        "e2e": {"value": top["gbs"], "unit": "GB/s", "h2d_bytes_per_step": top["bytes"], "d2h_bytes_per_step": None,
                 "note": "requests arrive as host buffers and results return to host memory"},
     }
     print(json.dumps(line))
@@ -588,7 +568,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=0, help="input bytes (default: the workload's size)")
     ap.add_argument("--workload", default="json", choices=sorted(WORKLOADS))
-    ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--serve-pool", type=int, default=2048, help="documents in the serve request pool")
+    ap.add_argument("--serve-seconds", type=float, default=2.0, help="seconds of arrivals per rate")
+    ap.add_argument("--serve-rates", default=",".join(str(r) for r in SERVE_RATES))
     ap.add_argument("--cpu-sample", type=int, default=256 << 20)
     ap.add_argument("--ref-sample", type=int, default=16 << 20)
     ap.add_argument("--no-cpu-baseline", action="store_true")

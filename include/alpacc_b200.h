@@ -210,18 +210,22 @@ void alpacc_result_free(alpacc_result *r);
  * Request server with continuous batching (replaces the reference's
  * sequential `--server` loop, backends/c/cli.c:153-161 and
  * backends/cuda/cli.cu:846-875, for in-process callers). `workers` threads each
- * own a handle and a stream; a free worker takes every queued request that
- * fits its share (scratch_budget / workers) of the device scratch budget and
+ * own a handle and a stream; a free worker takes queued requests, in order,
+ * while the exact device scratch of their batch (the sizes the batch path
+ * grows its buffers to) stays within its share (scratch_budget / workers), and
  * parses them as one batch, so requests arriving while a batch runs join the
- * next one and batches overlap on the device. Each result equals parsing its
- * input alone.
+ * next one and batches overlap on the device. A worker's handle never holds
+ * more batch scratch than its share, except while a single request that needs
+ * more on its own runs. Each result equals parsing its input alone.
  *   submit: copies the input, returns its id;
  *   wait:   blocks until that request is done; its status (OK / REJECT /
  *           error), its result (release with alpacc_result_free before
  *           stopping the server) and the latency from submit to completion.
  *           One caller may wait for an id; a second wait on the same id
  *           (concurrent or later) returns ALPACC_E_INVALID;
- *   stats:  batches run, requests served, largest batch, requests queued;
+ *   stats:  batches run, requests served, largest batch, requests queued,
+ *           most batch scratch bytes a worker's handle held, the per-worker
+ *           share (returns the number of values, 6; fills at most n);
  *   stop:   drains the queue, joins the workers, frees the handles.
  */
 typedef struct alpacc_server alpacc_server;
@@ -231,6 +235,23 @@ int alpacc_server_submit(alpacc_server *s, const uint8_t *in, uint64_t n, uint64
 int alpacc_server_wait(alpacc_server *s, uint64_t id, alpacc_result *out, double *latency_ms);
 int alpacc_server_stats(alpacc_server *s, int64_t *vals, int n);
 void alpacc_server_stop(alpacc_server *s);
+
+/*
+ * Trace replay, for measuring the served form against plain calls (no
+ * counterpart in the reference). Request i is input doc[i] of a pool
+ * (bytes[offsets[k]..offsets[k+1]) is input k) arriving arrival_s[i] seconds
+ * after the call starts (non-decreasing). alpacc_server_replay submits each
+ * at its arrival from a native thread and waits for all in order;
+ * alpacc_gpu_replay makes one alpacc_gpu_parse per request on g, in order,
+ * none before its arrival. Both release every result and fill, per request,
+ * status[i] (OK, REJECT or an error) and latency_ms[i] (scheduled arrival to
+ * result), and *elapsed_s (start to the last result).
+ */
+int alpacc_server_replay(alpacc_server *s, const uint8_t *bytes, const int64_t *offsets, const uint32_t *doc,
+                         uint64_t count, const double *arrival_s, double *latency_ms, int *status,
+                         double *elapsed_s);
+int alpacc_gpu_replay(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offsets, const uint32_t *doc,
+                      uint64_t count, const double *arrival_s, double *latency_ms, int *status, double *elapsed_s);
 
 /*
  * Lexer-only mode: the lexemes of lex_string (backends/c/lexer.c:39-97) for
@@ -333,12 +354,14 @@ const char *alpacc_gpu_last_error(const alpacc_gpu_grammar *g);
 int alpacc_gpu_stage_ms(const alpacc_gpu_grammar *g, double *out, int n);
 /* Tokens, brackets, productions and tree nodes of the last call, then four
    lexer diagnostic counters (collected when diagnostics are on): tiles that
-   read their incoming state from the previous tile, constant chunks, chunk
-   evaluations chained to find start states, bytes walked as state sets; then
-   the number of kernels the call launched; then (diagnostics on) the SM
-   cycles thread 0 of the lexer's CTAs spent in each phase, summed over tiles:
-   load, pass 1, lane jobs, constant-chunk scan, start states, pass 2 with the
-   masks and the count scan, the count look-back, the token writes. */
+   read their incoming state from the previous tile, chunks whose start state
+   their window settled, chunk evaluations chained to find the other chunks'
+   start states, candidate walks of those chunks; then the number of kernels
+   the call launched; then (diagnostics on) the SM cycles thread 0 of the
+   lexer's CTAs spent in each phase, summed over tiles: load, window walk,
+   chunk and candidate walks, known-chunk scan, start states, open chunks'
+   codes with the masks and the count scan, the count look-back, the token or
+   code writes. */
 int alpacc_gpu_counts(const alpacc_gpu_grammar *g, int64_t *vals, int n);
 void alpacc_gpu_set_diagnostics(alpacc_gpu_grammar *g, int on);
 /* Number of device allocations (cudaMalloc) this library has made in the

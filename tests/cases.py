@@ -141,9 +141,9 @@ def simple_json(n: int, seed: int) -> bytes:
     return doc + b" " * (n - len(doc))
 
 
-# sizes around the lexer's tile geometry: tiles of 14880 new bytes after a
-# 480-byte halo, chunks of 60 bytes
-TILE_SIZES = (1, 7, 60, 61, 64, 1000, 14879, 14880, 14881, 15359, 15360, 15361, 29760, 29761, 40000)
+# sizes around the lexer's tile geometry: tiles of 15360 bytes (256 chunks of
+# 60 bytes, each also reading the 16 bytes before it)
+TILE_SIZES = (1, 7, 16, 17, 60, 61, 64, 76, 1000, 15359, 15360, 15361, 15376, 30720, 30721, 40000)
 
 
 def case_inputs(config: str, sizes=TILE_SIZES, seeds=(0, 1)):

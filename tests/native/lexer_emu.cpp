@@ -1,17 +1,17 @@
 // Test harness (tests only): a sequential CPU emulation of the tile algorithm
-// of alpacc_b200/csrc/lexer.cu - the same shared-memory table
-// (build_lexer_table), tile and chunk geometry, pass 1 (state-set walk to a
-// word-aligned convergence point, unrolled single-lane walk writing codes over
-// the consumed words, per-lane end states of chunks whose set is not one
-// state after 16 bytes ("open"), with the true lane's codes), resolution from the
-// nearest constant chunk or the previous tile's published outgoing state /
-// transition vector, pass 2 (re-walk of the bytes walked as a set from the
-// true start), the boundary and kept masks computed with the kernel's byte
-// tricks, the (count, last boundary) carry and the token emission with the
-// length check. Its lexemes are compared with machine_lex's (the machine
-// walked byte by byte, itself compared with the oracle), so the algorithm's
-// logic is checked without a GPU; the parallel mechanics (barriers, look-back
-// waits) are not.
+// of alpacc_b200/csrc/lexer.cu - the same shared-memory tables
+// (build_lexer_table: the machine and its window machine), tile and chunk
+// geometry, the window walk over the 16 bytes before each chunk (in the
+// window machine, or as an explicit state set from the first window byte's
+// image), the single walk of each chunk whose window left one candidate
+// ("known"), per-candidate end states and codes of the other ("open")
+// chunks, resolution from the nearest known chunk or the previous tile's
+// published outgoing state / transition vector, the boundary and kept masks
+// computed with the kernel's byte tricks, the (count, last boundary) carry and
+// the token emission with the length check. Its lexemes are compared with
+// machine_lex's (the machine walked byte by byte, itself compared with the
+// oracle), so the algorithm's logic is checked without a GPU; the parallel
+// mechanics (barriers, look-back waits) are not.
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
@@ -22,10 +22,9 @@
 
 namespace {
 
-constexpr int kThreads = 256, kWords = 15, kChunk = 60, kHalo = 8;
-constexpr int kSetWalk = 16;  // bytes a chunk walks as a state set before it counts as open
-constexpr int kLoad = kThreads * kChunk, kData = (kThreads - kHalo) * kChunk;
-enum { kEmpty = 0, kConst = 1, kOpen = 2, kPartial = 3 };
+constexpr int kThreads = 256, kWords = 15, kChunk = 60, kWin = 16;
+constexpr int kData = kThreads * kChunk, kLoad = kWin + kData;
+enum { kEmpty = 0, kKnown = 1, kOpen = 2, kOpenTail = 3 };
 
 struct Emu {
   const alpacc::LexerMachine &lm;
@@ -33,6 +32,7 @@ struct Emu {
   uint32_t row_of(uint32_t x) const { return (x << lt.shift) | ((x & (uint32_t)lt.swz) << 2); }
   int state_of(uint32_t f) const { return (int)((f & 0xFFFFFFu) >> lt.shift); }
   uint32_t step(uint32_t f, uint32_t c4) const { return lt.tab[((f & 0xFFFFFFu) ^ c4) >> 2]; }
+  uint32_t wstep(uint32_t f, uint32_t c4) const { return lt.ps_tab[((f & 0xFFFFFFu) ^ c4) >> 2]; }
   uint32_t c4(uint8_t b) const { return lt.cls4[b]; }
 };
 
@@ -44,9 +44,11 @@ uint32_t pack_codes(uint32_t e0, uint32_t e1, uint32_t e2, uint32_t e3) {
 
 }  // namespace
 
-// stats: [0] open chunks, [1] constant chunks, [2] tiles that took the look-back, [3] bytes walked as sets
-extern "C" int lexer_emu(const alpacc_tables *t, const uint8_t *in, uint64_t n, int open_end, uint64_t *out,
-                         uint64_t cap, uint64_t *count, int64_t *stats, uint64_t *last_boundary) {
+// sets: walk windows as explicit state sets (the kernel's variant for
+// machines without a window machine). stats: [0] open chunks, [1] known
+// chunks, [2] tiles that took the look-back, [3] candidate walks.
+extern "C" int lexer_emu(const alpacc_tables *t, const uint8_t *in, uint64_t n, int open_end, int sets,
+                         uint64_t *out, uint64_t cap, uint64_t *count, int64_t *stats, uint64_t *last_boundary) {
   alpacc::HostGrammar hg;
   std::string why;
   int rc = alpacc::build_host_grammar(t, &hg, &why);
@@ -55,6 +57,7 @@ extern "C" int lexer_emu(const alpacc_tables *t, const uint8_t *in, uint64_t n, 
   alpacc::LexerTable ltab;
   rc = alpacc::build_lexer_table(lm, &ltab, &why);
   if (rc != ALPACC_OK) return rc;
+  if (ltab.ps_tab.empty()) sets = 1;
   const Emu E{lm, ltab};
   const int dead = lm.dead;
   *count = 0;
@@ -70,108 +73,128 @@ extern "C" int lexer_emu(const alpacc_tables *t, const uint8_t *in, uint64_t n, 
   long long carry_cnt = 0, carry_pos = 0;
   uint64_t k = 0;
   for (uint64_t tile = 0; tile < tiles; tile++) {
-    const long long data0 = (long long)tile * kData, load0 = data0 - (long long)kHalo * kChunk;
+    const long long data0 = (long long)tile * kData, load0 = data0 - kWin;
     std::vector<uint8_t> bytes(kLoad, 0);
     for (int i = 0; i < kLoad; i++) {
       const long long p = load0 + i;
       if (p >= 0 && p < (long long)n) bytes[i] = in[p];
     }
-    std::vector<int> kind(kThreads), endst(kThreads, 0), c0(kThreads, 0), nbv(kThreads), jwv(kThreads),
-        conv(kThreads, -1), start(kThreads, 0);
-    std::vector<std::vector<int>> lend(kThreads);
-    // ---- pass 1 ----
+    std::vector<int> kind(kThreads, kEmpty), endst(kThreads, 0), nbv(kThreads, 0), start(kThreads, 0);
+    std::vector<std::vector<int>> cand(kThreads), lend(kThreads);
+    std::vector<std::vector<uint8_t>> lcodes(kThreads);  // open chunks: codes per candidate
+    // ---- windows (every chunk's, before any walk writes codes over the
+    // bytes: the kernel's barrier), then walks ----
+    std::vector<int> x0v(kThreads, -1);
     for (int c = 0; c < kThreads; c++) {
-      uint8_t *rb = bytes.data() + c * kChunk;
-      const long long g0 = load0 + (long long)c * kChunk;
+      uint8_t *rb = bytes.data() + kWin + c * kChunk;
+      const uint8_t *wb = rb - kWin;
+      const long long g0 = data0 + (long long)c * kChunk;
       int nb = 0;
-      if (g0 >= 0 && g0 < (long long)n) nb = (int)std::min<long long>(kChunk, (long long)n - g0);
+      if (g0 < (long long)n) nb = (int)std::min<long long>(kChunk, (long long)n - g0);
       nbv[c] = nb;
-      jwv[c] = nb;
-      kind[c] = nb == kChunk ? kConst : nb > 0 ? kPartial : kEmpty;
-      if (nb != kChunk) continue;
-      c0[c] = lm.cls[rb[0]];
-      std::vector<char> set(lm.M, 0);
-      int j;
-      if (!lm.img2.empty()) {
-        const unsigned long long m = lm.img2[(size_t)c0[c] * lm.C + lm.cls[rb[1]]];
-        for (int s = 0; s < 64 && s < lm.M; s++) set[s] = (m >> s) & 1;
-        j = 2;
+      if (nb == 0) continue;
+      int x0 = -1;
+      if (g0 == 0) {
+        x0 = lm.m0;
+      } else if (!sets) {
+        uint32_t f = ltab.ps_full, e = 0;
+        for (int j = 0; j < kWin; j++) {
+          e = E.wstep(f, E.c4(wb[j]));
+          f = e;
+        }
+        const uint32_t info = e >> 24;
+        if (info != 0xFF) {
+          x0 = (int)info;
+        } else {
+          const int p = E.state_of(e);
+          for (int s = 0; s < lm.M; s++)
+            if (ltab.ps_mask[(size_t)p * 4 + (s >> 6)] >> (s & 63) & 1) cand[c].push_back(s);
+        }
       } else {
-        for (int l = 0; l < lm.img_cnt[c0[c]]; l++) set[lm.img[(size_t)c0[c] * alpacc::kMaxLanes + l]] = 1;
-        j = 1;
-      }
-      auto live_count = [&] { return (int)std::count(set.begin(), set.end(), 1); };
-      int live = live_count();
-      while (j < kSetWalk && (live > 1 || (j & 3))) {
-        std::vector<char> ns(lm.M, 0);
-        for (int s = 0; s < lm.M; s++)
-          if (set[s]) {
-            const int nx = E.state_of(E.step(E.row_of((uint32_t)s), E.c4(rb[j])));
-            if (nx != dead) ns[nx] = 1;
-          }
-        set.swap(ns);
-        live = live_count();
-        ++j;
-      }
-      stats[3] += j;
-      if (live == 0) {
-        jwv[c] = j;
-        endst[c] = dead;
-        continue;
-      }
-      if (live > 1) {
-        kind[c] = kOpen;
-        jwv[c] = kChunk;
-        stats[0]++;
-        const int cnt = lm.img_cnt[c0[c]];
-        lend[c].assign(cnt, 0);
-        for (int l = 0; l < cnt; l++) {
-          uint32_t f = E.row_of(lm.img[(size_t)c0[c] * alpacc::kMaxLanes + l]);
-          for (int q = 1; q < kChunk; q++) f = E.step(f, E.c4(rb[q]));
-          lend[c][l] = E.state_of(f);
+        std::vector<char> set(lm.M, 0);
+        const int c0 = lm.cls[wb[0]];
+        for (int l = 0; l < lm.img_cnt[c0]; l++) set[lm.img[(size_t)c0 * alpacc::kMaxLanes + l]] = 1;
+        for (int j = 1; j < kWin; j++) {
+          std::vector<char> ns(lm.M, 0);
+          for (int s = 0; s < lm.M; s++)
+            if (set[s]) {
+              const int nx = E.state_of(E.step(E.row_of((uint32_t)s), E.c4(wb[j])));
+              if (nx != dead) ns[nx] = 1;
+            }
+          set.swap(ns);
         }
-        continue;
+        const int live = (int)std::count(set.begin(), set.end(), 1);
+        if (live == 0) x0 = dead;
+        else if (live == 1) x0 = (int)(std::find(set.begin(), set.end(), 1) - set.begin());
+        else
+          for (int s = 0; s < lm.M; s++)
+            if (set[s]) cand[c].push_back(s);
       }
-      const int s_conv = (int)(std::find(set.begin(), set.end(), 1) - set.begin());
-      conv[c] = s_conv;
-      jwv[c] = j;
-      if (j >= kChunk) {
-        endst[c] = s_conv;
-        continue;
-      }
-      const uint32_t fconv = E.row_of((uint32_t)s_conv);
-      const int jw4 = j >> 2;
-      uint32_t f = fconv;
-      for (int w = 0; w < kWords; w++) {
-        if (w == jw4) f = fconv;
-        uint32_t e[4];
-        for (int q = 0; q < 4; q++) {
-          e[q] = E.step(f, E.c4(rb[4 * w + q]));
-          f = e[q];
-        }
-        if (w >= jw4) {
-          const uint32_t cw = pack_codes(e[0], e[1], e[2], e[3]);
-          std::memcpy(rb + 4 * w, &cw, 4);
-        }
-      }
-      endst[c] = E.state_of(f);
+      x0v[c] = x0;
     }
-    for (int c = 0; c < kThreads; c++) stats[1] += kind[c] == kConst;
+    for (int c = 0; c < kThreads; c++) {
+      uint8_t *rb = bytes.data() + kWin + c * kChunk;
+      const long long g0 = data0 + (long long)c * kChunk;
+      const int nb = nbv[c];
+      if (nb == 0) continue;
+      const int x0 = x0v[c];
+      if (x0 >= 0) {
+        kind[c] = kKnown;
+        start[c] = x0;
+        if (x0 == dead) {
+          reject = true;
+          endst[c] = dead;
+        } else {
+          uint32_t f = E.row_of((uint32_t)x0);
+          for (int j = 0; j < nb; j++) {
+            const uint32_t e = E.step(f, E.c4(rb[j]));
+            rb[j] = (uint8_t)(e >> 24);
+            f = e;
+          }
+          endst[c] = E.state_of(f);
+        }
+        if (g0 == 0) rb[0] = 0xFF;
+        continue;
+      }
+      if ((int)cand[c].size() > alpacc::kMaxLanes) error = 3;  // more candidates than slots
+      kind[c] = nb == kChunk ? kOpen : kOpenTail;
+      stats[0]++;
+      if (kind[c] == kOpenTail) continue;
+      stats[3] += (int64_t)cand[c].size();
+      lend[c].resize(cand[c].size());
+      lcodes[c].resize(cand[c].size() * kChunk);
+      for (size_t l = 0; l < cand[c].size(); l++) {
+        uint32_t f = E.row_of((uint32_t)cand[c][l]);
+        for (int w = 0; w < kWords; w++) {
+          uint32_t e[4];
+          for (int q = 0; q < 4; q++) {
+            e[q] = E.step(f, E.c4(rb[4 * w + q]));
+            f = e[q];
+          }
+          const uint32_t cw = pack_codes(e[0], e[1], e[2], e[3]);
+          std::memcpy(lcodes[c].data() + l * kChunk + 4 * w, &cw, 4);
+        }
+        lend[c][l] = E.state_of(f);
+      }
+    }
+    for (int c = 0; c < kThreads; c++) stats[1] += kind[c] == kKnown;
+    auto slot_of = [&](int c, int x) -> int {
+      auto it = std::find(cand[c].begin(), cand[c].end(), x);
+      return it == cand[c].end() ? -1 : (int)(it - cand[c].begin());
+    };
     auto eval = [&](int c, int x) -> int {
       if (kind[c] == kEmpty) return x;
-      if (x == dead || x < 0) return dead;
-      if (kind[c] == kConst) return endst[c];
-      if (kind[c] == kPartial) return dead;
-      const int slot = lm.lane_of[(size_t)c0[c] * lm.M + x];
-      if (slot == 0xff) return dead;
-      return lend[c][slot];
+      if (kind[c] == kKnown) return endst[c];
+      if (kind[c] == kOpenTail || x == dead || x < 0) return dead;
+      const int slot = slot_of(c, x);
+      return slot < 0 ? dead : lend[c][slot];
     };
     // ---- resolution ----
     int ktot = -1;
     std::vector<int> kconst(kThreads);
     for (int c = 0; c < kThreads; c++) {
       kconst[c] = ktot;
-      if (kind[c] == kConst) ktot = c;
+      if (kind[c] == kKnown) ktot = c;
     }
     if (ktot >= 0) {
       int x = endst[ktot];
@@ -182,13 +205,13 @@ extern "C" int lexer_emu(const alpacc_tables *t, const uint8_t *in, uint64_t n, 
       vec[tile].resize(lm.M);
       for (int s = 0; s < lm.M; s++) {
         int x = s;
-        for (int jj = kHalo; jj < kThreads; jj++) x = eval(jj, x);
+        for (int jj = 0; jj < kThreads; jj++) x = eval(jj, x);
         vec[tile][s] = x < 0 ? 0 : x;
       }
       flag[tile] = 1;
     }
     int s_in = lm.m0;
-    if (kconst[kHalo] < 0) {
+    if (kind[0] == kOpen || kind[0] == kOpenTail) {
       stats[2]++;
       if (tile > 0) {
         long long j = (long long)tile - 1;
@@ -212,14 +235,15 @@ extern "C" int lexer_emu(const alpacc_tables *t, const uint8_t *in, uint64_t n, 
         s_in = x;
       }
     }
-    for (int c = kHalo; c < kThreads; c++) {
+    for (int c = 0; c < kThreads; c++) {
+      if (kind[c] == kKnown) continue;
       int x, from;
       if (kconst[c] >= 0) {
         x = endst[kconst[c]];
         from = kconst[c] + 1;
       } else {
         x = s_in;
-        from = kHalo;
+        from = 0;
       }
       for (int jj = from; jj < c; jj++) x = eval(jj, x);
       start[c] = x < 0 ? 0 : x;
@@ -229,32 +253,37 @@ extern "C" int lexer_emu(const alpacc_tables *t, const uint8_t *in, uint64_t n, 
       const int x = eval(kThreads - 1, start[kThreads - 1]);
       outst[tile] = x < 0 ? 0 : x;
     }
-    // ---- pass 2, masks, counts ----
+    // ---- open chunks' codes, masks, counts ----
     std::vector<unsigned long long> bmask(kThreads, 0);
     std::vector<long long> cnt(kThreads, 0), lastb(kThreads, 0);
     std::vector<int> final_kept(kThreads, 0), x_endv(kThreads, 0);
-    for (int c = kHalo; c < kThreads; c++) {
+    for (int c = 0; c < kThreads; c++) {
       const int nb = nbv[c];
       if (nb == 0) continue;
-      uint8_t *rb = bytes.data() + c * kChunk;
-      const long long g0 = load0 + (long long)c * kChunk;
-      const int x0 = start[c];
-      bool died = x0 == dead;
-      uint32_t f = E.row_of((uint32_t)(x0 < 0 ? 0 : x0));
-      if (!died) {
-        for (int j = 0; j < jwv[c]; j++) {
-          const uint32_t e = E.step(f, E.c4(rb[j]));
-          rb[j] = (g0 + j >= 1) ? (uint8_t)(e >> 24) : 0xFF;
-          f = e;
-        }
-        died = E.state_of(f) == dead;
-      }
-      int x_end;
-      if (kind[c] == kConst) {
-        if (!died && conv[c] >= 0 && E.state_of(f) != conv[c]) error = 1;
-        x_end = died ? dead : endst[c];
+      uint8_t *rb = bytes.data() + kWin + c * kChunk;
+      const long long g0 = data0 + (long long)c * kChunk;
+      int x_end = dead;
+      if (kind[c] == kKnown) {
+        x_end = endst[c];
       } else {
-        x_end = died ? dead : E.state_of(f);
+        const int x0 = start[c];
+        if (kind[c] == kOpenTail) {
+          if (x0 != dead) {
+            uint32_t f = E.row_of((uint32_t)x0);
+            for (int j = 0; j < nb; j++) {
+              const uint32_t e = E.step(f, E.c4(rb[j]));
+              rb[j] = (uint8_t)(e >> 24);
+              f = e;
+            }
+            x_end = E.state_of(f);
+          }
+        } else {
+          const int slot = x0 == dead ? -1 : slot_of(c, x0);
+          if (slot >= 0) {
+            std::memcpy(rb, lcodes[c].data() + slot * kChunk, kChunk);
+            x_end = lend[c][slot];
+          }
+        }
       }
       x_endv[c] = x_end;
       if (x_end == dead) reject = true;
@@ -276,10 +305,10 @@ extern "C" int lexer_emu(const alpacc_tables *t, const uint8_t *in, uint64_t n, 
     }
     // ---- carry and emission ----
     long long ce = carry_cnt, pe = carry_pos;
-    for (int c = kHalo; c < kThreads; c++) {
+    for (int c = 0; c < kThreads; c++) {
       const int nb = nbv[c];
-      const long long g0 = load0 + (long long)c * kChunk;
-      const uint8_t *rb = bytes.data() + c * kChunk;
+      const long long g0 = data0 + (long long)c * kChunk;
+      const uint8_t *rb = bytes.data() + kWin + c * kChunk;
       if (nb > 0) {
         long long prev = pe;
         uint64_t o = (uint64_t)ce;

@@ -106,3 +106,44 @@ extern "C" int pair_lookup(const alpacc_tables *t, const uint64_t *keys, uint64_
   }
   return ALPACC_OK;
 }
+
+// The window machine of build_lexer_table, checked against the subset
+// construction it encodes: info = {sets, entries naming one state, entries
+// naming two or more, entries whose info byte disagrees with the member
+// masks}; returns 0, or 1 when no window machine was built.
+extern "C" int window_info(const alpacc_tables *t, int64_t *info) {
+  alpacc::HostGrammar hg;
+  std::string why;
+  if (alpacc::build_host_grammar(t, &hg, &why) != ALPACC_OK) return -1;
+  const alpacc::LexerMachine &lm = hg.lex;
+  alpacc::LexerTable lt;
+  if (alpacc::build_lexer_table(lm, &lt, &why) != ALPACC_OK) return -1;
+  for (int i = 0; i < 4; i++) info[i] = 0;
+  if (lt.ps_tab.empty()) return 1;
+  const int P = lt.ps_sets, cp = 1 << (lt.shift - 2);
+  info[0] = P;
+  for (int p = 0; p < P; p++)
+    for (int c = 0; c < lm.C; c++) {
+      const uint32_t e = lt.ps_tab[(size_t)p * cp + ((uint32_t)c ^ ((uint32_t)p & (uint32_t)lt.swz))];
+      const int k = (int)((e & 0xFFFFFFu) >> lt.shift);
+      // the next set from the members of p
+      unsigned long long want[4] = {0, 0, 0, 0};
+      for (int s = 0; s < lm.M; s++)
+        if (lt.ps_mask[(size_t)p * 4 + (s >> 6)] >> (s & 63) & 1) {
+          const int x = lm.trans[(size_t)s * lm.C + c];
+          if (x != lm.dead) want[x >> 6] |= 1ull << (x & 63);
+        }
+      int members = 0, one = -1;
+      bool same = true;
+      for (int w = 0; w < 4; w++) {
+        same = same && want[w] == lt.ps_mask[(size_t)k * 4 + w];
+        members += __builtin_popcountll(want[w]);
+        if (want[w]) one = 64 * w + __builtin_ctzll(want[w]);
+      }
+      const uint32_t expect = members == 0 ? (uint32_t)lm.dead : members == 1 ? (uint32_t)one : 0xFFu;
+      if (!same || (e >> 24) != (expect & 0xFF)) info[3]++;
+      if (members == 1) info[1]++;
+      if (members > 1) info[2]++;
+    }
+  return 0;
+}

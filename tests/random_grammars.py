@@ -220,7 +220,7 @@ class RandomGrammar:
             for _ in range(3):
                 out.append(self.sentence(rng, budget))
         # strings of the grammar's characters across lexer tile boundaries
-        # (14880 new bytes per tile): mostly rejected by the parser, they
+        # (15360 bytes per tile): mostly rejected by the parser, they
         # exercise the lexer's state resolution between tiles
         for n in noise:
             out.append("".join(self.chars[int(i)] for i in rng.integers(0, len(self.chars), n)))

@@ -52,3 +52,26 @@ def test_server_results_equal_alone(gpu, config):
             assert wire.encode_record(r, srv.layout) == alone.run_case(d)
     finally:
         srv.close()
+
+
+def test_server_scratch_within_share(gpu):
+    """Admission by the batch path's exact scratch: with a share far below
+    what all requests together need, batches split and no worker's handle
+    ever holds more batch scratch than its share."""
+    config = "json_ext_i32"
+    tables = cases.tables(config)
+    alone = native.Parser(tables, device=0)
+    srv = native.Server(tables, device=0, workers=2, budget=96 << 20)
+    try:
+        rng = np.random.default_rng(11)
+        docs = [cases.generated(config, int(n), 500 + i) for i, n in enumerate(rng.integers(20000, 60000, 48))]
+        ids = [srv.submit(d) for d in docs]
+        got = [srv.wait(i) for i in ids]
+        for d, (r, _) in zip(docs, got):
+            assert wire.encode_record(r, srv.layout) == alone.run_case(d)
+        st = srv.stats()
+        assert st["scratch_share"] == 48 << 20
+        assert 0 < st["max_scratch_held"] <= st["scratch_share"], st
+        assert st["batches"] > 2, st
+    finally:
+        srv.close()

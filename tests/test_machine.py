@@ -33,6 +33,8 @@ def harness(tmp_path_factory):
                            os.path.join(HERE, "native", "machine_lex.cpp"),
                            os.path.join(REPO, "alpacc_b200", "csrc", "device_tables.cpp"), "-o", so])
     L = ctypes.CDLL(so)
+    L.window_info.restype = ctypes.c_int
+    L.window_info.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     L.machine_lex.restype = ctypes.c_int
     L.machine_lex.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64,
                               ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int)]
@@ -171,15 +173,16 @@ def emu(tmp_path_factory):
                            os.path.join(REPO, "alpacc_b200", "csrc", "device_tables.cpp"), "-o", so])
     L = ctypes.CDLL(so)
     L.lexer_emu.restype = ctypes.c_int
-    L.lexer_emu.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p,
-                            ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64), ctypes.c_void_p,
+    L.lexer_emu.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int,
+                            ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64), ctypes.c_void_p,
                             ctypes.POINTER(ctypes.c_uint64)]
     return L
 
 
-def _emu_vs_machine(L, M, t, inputs):
+def _emu_vs_machine(L, M, t, inputs, sets=False):
     """The tile algorithm of the lexer kernel (emulated) against the machine
-    walked byte by byte: status and every lexeme."""
+    walked byte by byte: status and every lexeme. ``sets``: windows walked as
+    explicit state sets instead of in the window machine."""
     s, keep = native.make_tables(t)
     states = ctypes.c_int(0)
     stats = np.zeros(4, dtype=np.int64)
@@ -190,8 +193,8 @@ def _emu_vs_machine(L, M, t, inputs):
         got = np.zeros(3 * cap, dtype=np.uint64)
         cw, cg, lb = ctypes.c_uint64(0), ctypes.c_uint64(0), ctypes.c_uint64(0)
         rw = M.machine_lex(ctypes.byref(s), d, len(d), want.ctypes.data, cap, ctypes.byref(cw), ctypes.byref(states))
-        rg = L.lexer_emu(ctypes.byref(s), d, len(d), 0, got.ctypes.data, cap, ctypes.byref(cg), stats.ctypes.data,
-                         ctypes.byref(lb))
+        rg = L.lexer_emu(ctypes.byref(s), d, len(d), 0, 1 if sets else 0, got.ctypes.data, cap, ctypes.byref(cg),
+                         stats.ctypes.data, ctypes.byref(lb))
         total += stats
         assert rg == rw, (t.name, len(d), d[:40], rg, rw)
         if rw == native.OK:
@@ -200,27 +203,43 @@ def _emu_vs_machine(L, M, t, inputs):
     return total
 
 
-TILE = 14880
+TILE = 15360
 
 
+@pytest.mark.parametrize("sets", [False, True], ids=["window_machine", "state_sets"])
 @pytest.mark.parametrize("config", sorted(cases.CONFIGS))
-def test_lexer_tile_algorithm(harness, emu, config):
+def test_lexer_tile_algorithm(harness, emu, config, sets):
     ins = cases.case_inputs(config, sizes=(1, 59, 60, 61, 3000, TILE - 1, TILE, TILE + 1, 3 * TILE + 7),
                             seeds=(0,))
-    _emu_vs_machine(emu, harness, cases.tables(config, "both"), ins)
+    _emu_vs_machine(emu, harness, cases.tables(config, "both"), ins, sets)
 
 
-def test_lexer_tile_algorithm_open_chunks(harness, emu):
-    """Inputs whose chunks never converge (a numeric array on one line is
-    valid both inside and outside a JSON string): per-lane chunk functions and
-    tiles without a constant chunk (transition vectors, look-back)."""
+@pytest.mark.parametrize("sets", [False, True], ids=["window_machine", "state_sets"])
+def test_lexer_tile_algorithm_open_chunks(harness, emu, sets):
+    """Inputs whose windows never settle on one state (a numeric array on one
+    line is valid both inside and outside a JSON string): per-candidate chunk
+    functions and tiles without a known chunk (transition vectors,
+    look-back)."""
     t = cases.tables("json_ext_i32")
     rng = np.random.default_rng(7)
     nums = b"[" + b", ".join(str(int(x)).encode() for x in rng.integers(0, 1000, 30000)) + b"]"
     mixed = b'{"a": ' + nums + b', "b": "x y z"}'
     bad = nums[:50000] + b"\x01" + nums[50000:]
-    stats = _emu_vs_machine(emu, harness, t, [nums, mixed, bad, nums[:TILE * 2 + 5] + b"]"])
+    stats = _emu_vs_machine(emu, harness, t, [nums, mixed, bad, nums[:TILE * 2 + 5] + b"]"], sets)
     assert stats[0] > 1000 and stats[2] > 0  # open chunks and look-back tiles were exercised
+
+
+def test_window_machine_tables(harness):
+    """The window machine of every shipped grammar is built (its sets fit the
+    budget) and each entry's info byte names the next set's one state, the
+    dead state for an empty set, or 0xFF for two or more."""
+    for config in sorted(cases.CONFIGS):
+        t = cases.tables(config, "both")
+        s, keep = native.make_tables(t)
+        info = np.zeros(4, dtype=np.int64)
+        assert harness.window_info(ctypes.byref(s), info.ctypes.data) == 0, config
+        sets, singles, opens, bad = info
+        assert 0 < sets <= 1024 and singles > 0 and bad == 0, (config, info)
 
 
 def test_lexer_tile_algorithm_rejects_and_lengths(harness, emu):
@@ -233,7 +252,9 @@ def test_lexer_tile_algorithm_rejects_and_lengths(harness, emu):
 
 @pytest.mark.parametrize("nkw", [8, 24, 32])
 def test_lexer_tile_algorithm_keyword_lexers(harness, emu, nkw):
-    """Machines above 64 states (256-bit state sets) and many start lanes."""
+    """Machines above 64 states (256-bit candidate sets) and many candidates;
+    the 32-keyword machine's window machine exceeds its budget, so it walks
+    windows as state sets."""
     t = generate_parts(keyword_grammar(nkw), "kw%d" % nkw, False, "both")
     _emu_vs_machine(emu, harness, t, keyword_inputs(nkw, seed=nkw, sizes=(0, 1, 20, 300, 15000, 40000)))
 
