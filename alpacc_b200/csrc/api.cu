@@ -62,6 +62,7 @@ int upload_tables(alpacc_gpu_grammar *g) {
     g->lex_variant = lm.M > 64 ? 1 : 0;
     g->ps_words = (int)lt.ps_tab.size();
     g->ps_full = lt.ps_full;
+    g->ps_sets = lt.ps_sets;
     TRY(upload(g->lex_ps, lt.ps_tab));
     TRY(upload(g->lex_psmask, lt.ps_mask));
   } else {
@@ -921,7 +922,8 @@ int alpacc_gpu_info(const alpacc_gpu_grammar *g, int64_t *vals, int nvals) {
                        g->hg.pairs.nt, (int64_t)g->hg.pairs.rec_ss.size(), g->lex_grid,
                        g->h_status ? g->h_status->lex_reject_reason : 0,
                        g->h_status ? g->h_status->parse_reject_reason : 0,
-                       g->h_status ? g->h_status->timeout_site : 0, g->hg.pairs.hashed ? 1 : 0};
+                       g->h_status ? g->h_status->timeout_site : 0, g->hg.pairs.hashed ? 1 : 0, g->lex_variant,
+                       g->ps_sets};
   const int nv = (int)(sizeof(v) / sizeof(v[0]));
   for (int i = 0; i < nvals && i < nv; i++) vals[i] = v[i];
   return nv;

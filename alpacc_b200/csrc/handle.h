@@ -89,6 +89,7 @@ struct alpacc_gpu_grammar {
   int lex_variant = 0;
   int ps_words = 0;        // window machine entries in shared memory (0: none)
   uint32_t ps_full = 0;
+  int ps_sets = 0;
   int lex_grid = 0;  // persistent grid of lex_kernel
   int pair_grid = 0, pse_grid = 0;  // resident CTAs of pair_kernel / pse_tile_kernel
   // parser-stage capacities: the largest exact needs seen (brackets, productions)

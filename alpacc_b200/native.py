@@ -263,7 +263,7 @@ class Parser:
         vals = (ctypes.c_int64 * 16)()
         n = lib().alpacc_gpu_info(self._h, vals, 16)
         keys = ["M", "C", "max_lanes", "reachable", "dead", "nt", "records", "lex_grid", "lex_reject_reason",
-                "parse_reject_reason", "timeout_site", "pair_hashed"]
+                "parse_reject_reason", "timeout_site", "pair_hashed", "lex_variant", "window_sets"]
         return dict(zip(keys, [vals[i] for i in range(min(n, len(keys)))]))
 
     def _check(self, rc: int) -> int:

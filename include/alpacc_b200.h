@@ -339,13 +339,17 @@ void *alpacc_gpu_stream(alpacc_gpu_grammar *g);
  * Diagnostics (no counterpart in the reference): sizes of the derived device
  * tables (states and byte classes of the minimised lexer automaton, lanes,
  * reachable endomorphisms, pair records), the lexer's grid, the reject reason /
- * wait site of the last call and whether the pair table is in its hashed form;
- * and the text of the last internal error.
+ * wait site of the last call, whether the pair table is in its hashed form,
+ * the lexer kernel variant (0 / 1: window machine for machines of at most /
+ * more than 64 states, 2: windows walked as explicit state sets) and the
+ * window machine's sets (0: not built); and the text of the last internal
+ * error.
  *
  * The pair table is a dense array for key spaces up to 2^26 keys and the
  * reference's own hash table, probed on the device as lookup_key probes it,
  * beyond; ALPACC_PAIR_LOOKUP=hashed in the environment at load time selects
- * the hashed form for any grammar (for checking it).
+ * the hashed form for any grammar (for checking it). Likewise
+ * ALPACC_LEX_WINDOW=sets selects the explicit state-set window walk.
  */
 int alpacc_gpu_info(const alpacc_gpu_grammar *g, int64_t *vals, int nvals);
 const char *alpacc_gpu_last_error(const alpacc_gpu_grammar *g);
