@@ -260,8 +260,10 @@ struct PseSmem {
   uint32_t v[kPseThreads * kPseStride];
   int32_t h[kPseThreads * kPseStride];   // depth before each element, relative to the tile start
   int32_t tc[kPseThreads * kPseStride];  // parents: inclusive terminal count, relative to the tile start
-  int32_t lv[5][kPseThreads];            // lv[k][i]: minimum of chunk minima over (i - 2^k, i] within i's warp
+  int32_t lv[6][kPseThreads];            // lv[k][i]: minimum of chunk minima over (i - 2^k, i] within i's warp
   int32_t wmin[kPseWarps];               // minimum of each warp's chunk minima
+  uint16_t wq[kPseTile];                 // per warp: its pending queries (element index in the tile)
+  int16_t wans[kPseTile];                // answer of a pending query (element index), or -1
   long long tmp[kPseWarps];
   long long prefix_a, prefix_b;
 };
@@ -437,7 +439,7 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
     L[k] = (lane >= (1 << (k - 1)) && o < L[k - 1]) ? o : L[k - 1];
   }
 #pragma unroll
-  for (int k = 0; k < 5; ++k) sm.lv[k][t] = L[k];
+  for (int k = 0; k < 6; ++k) sm.lv[k][t] = L[k];
   if (lane == kWarp - 1) sm.wmin[warp] = L[5];
   __syncthreads();
 
@@ -489,55 +491,59 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
       need |= 1u << j;
     }
   }
-  // ---- earlier chunks of the tile: one query per lane per round ----
-  for (int guard = 0; __any_sync(0xffffffffu, need != 0u); ++guard) {
-    if (guard > kPseItems) {  // one item per round: cannot happen
-      if (lane == 0) record_timeout(st, kSitePseQuery);
-      break;
-    }
-    const bool act = need != 0u;
-    const int j = act ? __ffs(need) - 1 : 0;
-    const int qv = act ? sm.h[t * kPseStride + j] - (parents ? 0 : 1) : INT_MIN;
-    int pos = lane > 0 ? lane - 1 : 0;
-    const int pm = __shfl_sync(0xffffffffu, L[5], pos);  // prefix minimum of the warp up to pos
-    const bool inwarp = act && lane > 0 && pm <= qv;
+  // ---- earlier chunks of the tile: the warp's pending queries, 32 at a
+  // time (one per lane, whichever thread they came from) ----
+  {
+    const int pend = __popc(need);
+    const int incl = warp_inclusive_scan(pend, [](int x, int y) { return x + y; });
+    const int total_w = __shfl_sync(0xffffffffu, incl, kWarp - 1);
+    if (total_w) {  // warp-uniform
+      uint16_t *q = sm.wq + warp * (kWarp * kPseItems);
+      int slot = incl - pend;
+      for (unsigned m = need; m; m &= m - 1) q[slot++] = (uint16_t)(t * kPseItems + __ffs(m) - 1);
+      __syncwarp();
+      for (int i = lane; i < total_w; i += kWarp) {
+        const int e = q[i];
+        const int ct = e / kPseItems;  // its chunk (thread)
+        const int qv = sm.h[ct * kPseStride + e % kPseItems] - (parents ? 0 : 1);
+        int found = -1;
+        // chunks of this warp before the previous one (checked already): the
+        // latest whose minimum is <= qv, by binary descent over the windows
+        int pos = ct - warp * kWarp - 2;
+        if (pos >= 0 && sm.lv[5][warp * kWarp + pos] <= qv) {
 #pragma unroll
-    for (int k = 4; k >= 0; --k) {
-      const int w = __shfl_sync(0xffffffffu, L[k], pos);
-      if (inwarp && w > qv && pos >= (1 << k)) pos -= 1 << k;
-    }
-    int found = -1;
-    if (inwarp) {
-      const int pl = warp * kWarp + pos;
+          for (int k = 4; k >= 0; --k)
+            if (pos >= (1 << k) && sm.lv[k][warp * kWarp + pos] > qv) pos -= 1 << k;
+          const int pl = warp * kWarp + pos;
 #pragma unroll
-      for (int jj = kPseItems - 1; jj >= 0; --jj)
-        if (found < 0 && sm.h[pl * kPseStride + jj] <= qv) found = pl * kPseItems + jj;
-    } else if (act) {
-      for (int w = warp - 1; w >= 0 && found < 0; --w) {
-        if (sm.wmin[w] > qv) continue;
-        int p = w * kWarp + kWarp - 1;
+          for (int jj = kPseItems - 1; jj >= 0; --jj)
+            if (found < 0 && sm.h[pl * kPseStride + jj] <= qv) found = pl * kPseItems + jj;
+        }
+        // then earlier warps of the tile
+        for (int w = warp - 1; w >= 0 && found < 0; --w) {
+          if (sm.wmin[w] > qv) continue;
+          int p = w * kWarp + kWarp - 1;
 #pragma unroll
-        for (int k = 4; k >= 0; --k)
-          if (sm.lv[k][p] > qv && p - (1 << k) >= w * kWarp) p -= 1 << k;
+          for (int k = 4; k >= 0; --k)
+            if (sm.lv[k][p] > qv && p - (1 << k) >= w * kWarp) p -= 1 << k;
 #pragma unroll
-        for (int jj = kPseItems - 1; jj >= 0; --jj)
-          if (found < 0 && sm.h[p * kPseStride + jj] <= qv) found = p * kPseItems + jj;
-      }
-    }
-    if (act) {
-      if (found >= 0) {
-        if (!parents) {
+          for (int jj = kPseItems - 1; jj >= 0; --jj)
+            if (found < 0 && sm.h[p * kPseStride + jj] <= qv) found = p * kPseItems + jj;
+        }
+        if (found >= 0 && !parents) {
           const uint32_t pv = sm.v[(found / kPseItems) * kPseStride + found % kPseItems];
-          if ((pv & 0x7fffffffu) != (sm.v[t * kPseStride + j] & 0x7fffffffu))
+          if ((pv ^ sm.v[ct * kPseStride + e % kPseItems]) & 0x7fffffffu)
             record_reject(st, &st->parse_reject_reason, 2);
         }
-#pragma unroll
-        for (int jj = 0; jj < kPseItems; ++jj)
-          if (jj == j) ans[jj] = found;
+        sm.wans[e] = (int16_t)found;
       }
-      need &= need - 1u;
+      __syncwarp();
+#pragma unroll
+      for (int j = 0; j < kPseItems; ++j)
+        if (need >> j & 1u) ans[j] = sm.wans[t * kPseItems + j];
     }
   }
+
   // ---- the tile's prefix: look-back by warp 0, now that predecessors had time ----
   if (t < kWarp) {
     Pair64 prefix{0, 0};
