@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <new>
 #include <string>
@@ -43,6 +44,30 @@ namespace {
   } while (0)
 
 int upload_pairs(alpacc_gpu_grammar *g);
+
+// FNV-1a over a byte range, continuing from h (the grammar digest that keys
+// the autotuner's cache).
+uint64_t fnv_bytes(uint64_t h, const void *p, size_t n) {
+  const uint8_t *b = static_cast<const uint8_t *>(p);
+  for (size_t i = 0; i < n; i++) h = (h ^ b[i]) * 1099511628211ull;
+  return h;
+}
+
+// Launch geometry chosen by alpacc_gpu_autotune, cached per (grammar digest,
+// device) for the process: handles loaded later for the same grammar and
+// device start with it.
+struct Geometry {
+  int win_words, lex_per_sm, pair_per_sm, pse_per_sm;
+};
+std::mutex g_geo_mu;
+std::map<std::pair<uint64_t, int>, Geometry> g_geo_cache;
+
+void apply_geometry(alpacc_gpu_grammar *g, const Geometry &geo, int sms) {
+  g->lex_win_words = geo.win_words;
+  g->lex_grid = geo.lex_per_sm * sms;
+  g->pair_grid = geo.pair_per_sm * sms;
+  g->pse_grid = geo.pse_per_sm * sms;
+}
 
 int upload_tables(alpacc_gpu_grammar *g) {
   const LexerMachine &lm = g->hg.lex;
@@ -78,6 +103,10 @@ int upload_tables(alpacc_gpu_grammar *g) {
   TRY(upload(g->lex_tab, lt.tab));
   TRY(upload(g->img, lm.img));
   TRY(upload(g->img_cnt, lm.img_cnt));
+  g->digest = fnv_bytes(g->digest, lt.tab.data(), lt.tab.size() * 4);
+  g->digest = fnv_bytes(g->digest, lt.cls4.data(), lt.cls4.size() * 2);
+  g->digest = fnv_bytes(g->digest, lm.term.data(), lm.term.size());
+  g->digest = fnv_bytes(g->digest, lm.flags.data(), lm.flags.size());
   TRY(upload(g->sterm, lm.term));
   TRY(upload(g->sflags, lm.flags));
   return g->hg.parts == ALPACC_PARTS_LEXER ? ALPACC_OK : upload_pairs(g);
@@ -85,6 +114,11 @@ int upload_tables(alpacc_gpu_grammar *g) {
 
 int upload_pairs(alpacc_gpu_grammar *g) {
   const PairTable &pt = g->hg.pairs;
+  g->digest = fnv_bytes(g->digest, pt.dense.data(), pt.dense.size() * 4);
+  g->digest = fnv_bytes(g->digest, pt.ht_key.data(), pt.ht_key.size() * 8);
+  g->digest = fnv_bytes(g->digest, pt.stacks.data(), pt.stacks.size() * 4);
+  g->digest = fnv_bytes(g->digest, pt.prods.data(), pt.prods.size() * 4);
+  g->digest = fnv_bytes(g->digest, pt.arity.data(), pt.arity.size() * 4);
   if (pt.hashed) {
     TRY(upload(g->ht_key, pt.ht_key));
     TRY(upload(g->ht_rec, pt.ht_rec));
@@ -552,6 +586,13 @@ alpacc_gpu_grammar *alpacc_gpu_load(const alpacc_tables *tables, int device, uin
       g->lex_grid = per_sm * sms;
       g->pair_grid = pair_sm * sms;
       g->pse_grid = pse_sm * sms;
+      g->sms = sms;
+      std::lock_guard<std::mutex> lock(g_geo_mu);
+      auto it = g_geo_cache.find({g->digest, device});
+      if (it != g_geo_cache.end()) {
+        apply_geometry(g, it->second, sms);
+        g->geo_cached = 1;
+      }
     }
   }
   if (rc == ALPACC_OK && max_input > 0) rc = grow(g->in, max_input + 16);
@@ -881,36 +922,89 @@ double alpacc_gpu_last_ms(alpacc_gpu_grammar *g) { return g ? g->last_ms : -1.0;
 
 int alpacc_gpu_autotune(alpacc_gpu_grammar *g, const uint8_t *d_sample, uint64_t n, int *choice) {
   if (!g || (n > 0 && !d_sample) || g->hg.parts == ALPACC_PARTS_PARSER) return ALPACC_E_INVALID;
-  const int run_mode = g->hg.parts == ALPACC_PARTS_LEXER ? kRunLex : kRunBoth;
+  const bool both = g->hg.parts == ALPACC_PARTS_BOTH;
   if (cudaSetDevice(g->device) != cudaSuccess) return ALPACC_E_CUDA;
-  int max_per_sm = 0, sms = 0;
-  if (lex_occupancy(g, &max_per_sm) != cudaSuccess ||
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device) != cudaSuccess || max_per_sm < 1) {
+  int lex_max = 0, pair_max = 0, pse_max = 0;
+  const int sms = g->sms;
+  if (lex_occupancy(g, &lex_max) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pair_max, pair_kernel, kPairThreads, 0) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pse_max, pse_tile_kernel, kPseThreads, 0) != cudaSuccess ||
+      lex_max < 1 || pair_max < 1 || pse_max < 1 || sms < 1) {
     cudaGetLastError();
     return ALPACC_E_CUDA;
   }
-  // the lexer's persistent grid: resident CTAs per SM from the occupancy
-  // limit down (fewer CTAs: less contention for shared-memory banks and the
-  // look-back; more: more latency hidden)
-  int best = max_per_sm;
-  double best_ms = -1.0;
-  for (int c = max_per_sm; c >= 1 && c >= max_per_sm - 4; --c) {
-    g->lex_grid = c * sms;
+  // mean time of stages [k0, k1) over two runs after one warm-up, or < 0
+  auto timed = [&](int mode, int k0, int k1) -> double {
     double ms = 0;
-    int ok = 1;
-    for (int rep = 0; rep < 3 && ok; ++rep) {  // first run warms up
-      const int rc = run_device(g, d_sample, n, run_mode);
-      if (rc < 0) ok = 0;
-      else if (rep > 0) ms += g->stage_ms[0];
+    for (int rep = 0; rep < 3; ++rep) {
+      if (run_device(g, d_sample, n, mode) < 0) return -1.0;
+      if (rep > 0)
+        for (int k = k0; k < k1; ++k) ms += g->stage_ms[k];
     }
-    if (ok && (best_ms < 0 || ms < best_ms)) {
-      best_ms = ms;
-      best = c;
+    return ms / 2;
+  };
+  Geometry geo{g->lex_win_words, g->lex_grid / sms, g->pair_grid / sms, g->pse_grid / sms};
+  double best = -1.0;
+  // lexer: window length x resident CTAs per SM (fewer CTAs: less contention
+  // for shared-memory banks and the look-back; more: more latency hidden)
+  const int wins[3] = {4, 6, 8};
+  for (int wi = 0; wi < 3; ++wi)
+    for (int c = lex_max; c >= 1 && c >= lex_max - 2; --c) {
+      Geometry t = geo;
+      t.win_words = wins[wi];
+      t.lex_per_sm = c;
+      apply_geometry(g, t, sms);
+      const double ms = timed(kRunLex, 0, 1);
+      if (ms >= 0 && (best < 0 || ms < best)) {
+        best = ms;
+        geo.win_words = t.win_words;
+        geo.lex_per_sm = c;
+      }
+    }
+  if (best < 0) {
+    apply_geometry(g, geo, sms);
+    return ALPACC_E_CUDA;
+  }
+  if (both) {  // the pair kernel's and the walks' resident CTAs per SM
+    best = -1.0;
+    for (int c = pair_max; c >= 1 && c >= pair_max - 2; --c) {
+      Geometry t = geo;
+      t.pair_per_sm = c;
+      apply_geometry(g, t, sms);
+      const double ms = timed(kRunBoth, 1, 2);
+      if (ms >= 0 && (best < 0 || ms < best)) {
+        best = ms;
+        geo.pair_per_sm = c;
+      }
+    }
+    best = -1.0;
+    for (int c = pse_max; c >= 1 && c >= pse_max - 2; --c) {
+      Geometry t = geo;
+      t.pse_per_sm = c;
+      apply_geometry(g, t, sms);
+      const double ms = timed(kRunBoth, 2, 6);
+      if (ms >= 0 && (best < 0 || ms < best)) {
+        best = ms;
+        geo.pse_per_sm = c;
+      }
     }
   }
-  g->lex_grid = best * sms;
-  if (choice) *choice = best;
-  return best_ms < 0 ? ALPACC_E_CUDA : ALPACC_OK;
+  apply_geometry(g, geo, sms);
+  {
+    std::lock_guard<std::mutex> lock(g_geo_mu);
+    g_geo_cache[{g->digest, g->device}] = geo;
+  }
+  g->geo_cached = 0;
+  if (choice) *choice = geo.lex_per_sm;
+  return ALPACC_OK;
+}
+
+int alpacc_gpu_geometry(const alpacc_gpu_grammar *g, int64_t *vals, int n) {
+  if (!g || !vals || g->sms < 1) return ALPACC_E_INVALID;
+  const int64_t v[6] = {4 * g->lex_win_words, g->lex_grid / g->sms, g->pair_grid / g->sms, g->pse_grid / g->sms,
+                        g->geo_cached, (int64_t)g->digest};
+  for (int i = 0; i < n && i < 6; i++) vals[i] = v[i];
+  return 6;
 }
 
 void *alpacc_gpu_stream(alpacc_gpu_grammar *g) { return g ? (void *)g->stream : nullptr; }

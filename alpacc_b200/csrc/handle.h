@@ -90,6 +90,10 @@ struct alpacc_gpu_grammar {
   int ps_words = 0;        // window machine entries in shared memory (0: none)
   uint32_t ps_full = 0;
   int ps_sets = 0;
+  int lex_win_words = 4;   // window before each chunk (words; 4..8)
+  int sms = 0;             // SMs of the device
+  uint64_t digest = 14695981039346656037ull;  // FNV-1a of the device tables (autotuner cache key)
+  int geo_cached = 0;      // the launch geometry came from the autotuner's cache
   int lex_grid = 0;  // persistent grid of lex_kernel
   int pair_grid = 0, pse_grid = 0;  // resident CTAs of pair_kernel / pse_tile_kernel
   // parser-stage capacities: the largest exact needs seen (brackets, productions)

@@ -13,14 +13,16 @@
 // (entry & 0xFFFFFF) ^ class * 4) and one shared-memory load.
 //
 // A tile is 256 chunks of 60 bytes (15 words: an odd word stride, so per-thread
-// rows are bank-conflict free), loaded with the 16 bytes before it.
+// rows are bank-conflict free), loaded with the 32 bytes before it.
 //
-// Window: each chunk walks the 16 bytes before it in the window machine (the
+// Window: each chunk walks the 16 (up to 32: a per-grammar choice of the
+// autotuner) bytes before it in the window machine (the
 //   subset automaton of the live states, same row format, from the set of all
 //   of them), which yields the set of states the chunk can start in. On JSON
 //   that set is one state for ~95% of chunks, on s-expressions for all: the
 //   chunk's start is then known without looking at any other chunk
-//   ("known"). The window walk is the same fixed 16 steps in every thread.
+//   ("known"). The window walk is the same fixed number of steps in every
+//   thread.
 //   Machines whose subset automaton is too large walk the window as an
 //   explicit state set instead.
 // Walk: a known chunk walks its 60 bytes once from its start (fully unrolled),
@@ -70,7 +72,7 @@ enum ChunkKind : uint8_t { kEmpty = 0, kKnown = 1, kOpen = 2, kOpenTail = 3 };
 constexpr uint32_t kAddrMask = 0xFFFFFFu;  // F(next) bits of an entry
 constexpr uint8_t kNoBoundary = 0xFF, kIgnored = 0xFE;
 constexpr uint32_t kOpenInfo = 0xFFu;        // window machine: two or more candidates
-constexpr int kWinWords = kLexWin / 4;
+constexpr int kWinWords = kLexWin / 4;  // words loaded before the tile
 // Candidate walks of open chunks run as jobs spread over the CTA (rounds of
 // one job per thread); the first kCodeJobs keep their codes, so the chunk's
 // second pass copies the true candidate's codes instead of walking again.
@@ -192,17 +194,17 @@ __device__ __forceinline__ int walk_bytes(const Tab &tb, uint8_t *rb, int nb, in
   return state_of(tb, f);
 }
 
-// The window of chunk t (the kLexWin bytes before its row): the one state the
-// chunk can start in (the dead state when none), or -1 with the candidates in
-// *cand. kPs: walked in the window machine; else as an explicit state set
-// from the first window byte's image.
+// The window of chunk t (the nw words before its row, `win` pointing at the
+// first): the one state the chunk can start in (the dead state when none), or
+// -1 with the candidates in *cand. kPs: walked in the window machine; else as
+// an explicit state set from the first window byte's image.
 template <int W, bool kPs>
 __device__ __forceinline__ int window_start(const LexArgs &a, const Tab &tb, const Tab &tw, const uint32_t *win,
-                                            StateSet<W> *cand) {
+                                            int nw, StateSet<W> *cand) {
   if (kPs) {
     uint32_t f = a.ps_full, e = 0;
-#pragma unroll
-    for (int w = 0; w < kWinWords; ++w) {
+#pragma unroll 4
+    for (int w = 0; w < nw; ++w) {
       const uint32_t word = win[w];
       e = step(tw, f, cls4_of(tb, __byte_perm(word, 0, 0x4440)));
       e = step(tw, e, cls4_of(tb, __byte_perm(word, 0, 0x4441)));
@@ -223,7 +225,7 @@ __device__ __forceinline__ int window_start(const LexArgs &a, const Tab &tb, con
     const int c0 = (int)(cls4_of(tb, wb[0]) >> 2);
     const int cnt = __ldg(a.img_cnt + c0);
     for (int l = 0; l < cnt; l++) set.add(__ldg(a.img + c0 * kLexLanes + l));
-    for (int j = 1; j < kLexWin; ++j) {
+    for (int j = 1; j < 4 * nw; ++j) {
       const uint32_t c4 = cls4_of(tb, wb[j]);
       StateSet<W> ns;
       ns.clear();
@@ -407,7 +409,7 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
         x0 = a.m0;  // the document's first chunk
       } else {
         StateSet<W> cand;
-        x0 = window_start<W, kPs>(a, tb, tw, row - kWinWords, &cand);
+        x0 = window_start<W, kPs>(a, tb, tw, row - a.win_words, a.win_words, &cand);
         if (x0 < 0) {
 #pragma unroll
           for (int i = 0; i < W; i++) sm->cand[i][t] = cand.w[i];

@@ -28,6 +28,7 @@ inline LexArgs lex_args(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, 
   a.ps_words = g->ps_words;
   a.ps_full = g->ps_full;
   a.ps_mask = (const unsigned long long *)g->lex_psmask.p;
+  a.win_words = g->lex_win_words;
   a.img = (const uint8_t *)g->img.p;
   a.img_cnt = (const uint8_t *)g->img_cnt.p;
   a.sterm = (const uint8_t *)g->sterm.p;

@@ -108,6 +108,8 @@ def lib():
             f.restype = ctypes.c_int
             f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        L.alpacc_gpu_geometry.restype = ctypes.c_int
+        L.alpacc_gpu_geometry.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
         L.alpacc_gpu_autotune.restype = ctypes.c_int
         L.alpacc_gpu_autotune.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                           ctypes.POINTER(ctypes.c_int)]
@@ -360,11 +362,19 @@ class Parser:
             lib().alpacc_result_free(ctypes.byref(r))
 
     def autotune(self, dev_ptr: int, n: int) -> int:
-        """Pick the lexer's table copies on a device-resident sample; returns the choice."""
+        """Tune the launch geometry on a device-resident sample
+        (alpacc_gpu_autotune); returns the lexer's CTAs per SM."""
         c = ctypes.c_int(0)
         self._check(lib().alpacc_gpu_autotune(self._h, dev_ptr, n, ctypes.byref(c)))
         return c.value
 
+
+    def geometry(self) -> dict:
+        """The launch geometry (alpacc_gpu_geometry)."""
+        v = (ctypes.c_int64 * 6)()
+        lib().alpacc_gpu_geometry(self._h, v, 6)
+        return {"lex_window_bytes": v[0], "lex_ctas_per_sm": v[1], "pair_ctas_per_sm": v[2],
+                "walk_ctas_per_sm": v[3], "from_cache": bool(v[4]), "grammar_digest": "%016x" % (v[5] & (2**64 - 1))}
     def parse_batch(self, docs) -> list:
         """Many independent inputs in one batched call; one ParseResult each."""
         parts = [bytes(d) for d in docs]

@@ -148,7 +148,7 @@ def ours_batch(a, rank, world, local_rank, dist):
     pin.numpy()[:] = np.frombuffer(buf, dtype=np.uint8)
     offs = np.ascontiguousarray(offs, dtype=np.int64)
     d_all = pin.to(dev)
-    choice = parser.autotune(d_all.data_ptr(), total)  # the lexer's resident CTAs per SM for this grammar
+    parser.autotune(d_all.data_ptr(), total)  # launch geometry for this grammar
     ext = torch.cuda.ExternalStream(parser.stream_handle(), device=dev)
     count = len(offs) - 1
 
@@ -197,7 +197,7 @@ def ours_batch(a, rank, world, local_rank, dist):
         "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u8", "data": "synthetic (seeded JSON generator, log-normal lengths)",
         "config": dict(workload_config(total, world, "batch"), documents=count, accepted=int(accepted),
-                       autotune_lexer_ctas_per_sm=choice),
+                       geometry=parser.geometry()),
         "per_input": {"value": job_throughput(world, total, 1, per_ms), "unit": "GB/s", "ms": per_ms,
                       "what": "one alpacc_gpu_parse per document, same host buffers"},
         "speedup_vs_per_input": (job_throughput(world, total, a.steps, ms) / job_throughput(world, total, 1, per_ms)),
@@ -443,6 +443,8 @@ def ours(a, rank, world, local_rank, dist):
         rc, r = parser.parse_device(d_in.data_ptr(), n)
         return rc, r
 
+    if not a.no_autotune:  # launch geometry for this grammar, tuned on the document (outside the timed region)
+        parser.autotune(d_in.data_ptr(), n)
     for _ in range(a.warmup):
         rc, r = step()
     if rc != (1 if wl["reject"] else 0):
@@ -508,7 +510,8 @@ def ours(a, rank, world, local_rank, dist):
         "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic (seeded JSON generator, one document per rank)",
-        "config": dict(workload_config(n, world, a.workload), tokens=T, nodes=N, brackets=B, productions=P),
+        "config": dict(workload_config(n, world, a.workload), tokens=T, nodes=N, brackets=B, productions=P,
+                       geometry=parser.geometry()),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                      "algorithmic_bytes": kb, "ms": mean[dom]},
@@ -569,6 +572,7 @@ def main():
     ap.add_argument("--size", type=int, default=0, help="input bytes (default: the workload's size)")
     ap.add_argument("--workload", default="json", choices=sorted(WORKLOADS))
     ap.add_argument("--serve-pool", type=int, default=2048, help="documents in the serve request pool")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch geometry")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="seconds of arrivals per rate")
     ap.add_argument("--serve-rates", default=",".join(str(r) for r in SERVE_RATES))
     ap.add_argument("--cpu-sample", type=int, default=256 << 20)

@@ -324,12 +324,23 @@ double alpacc_gpu_last_ms(alpacc_gpu_grammar *g);
 
 /*
  * Autotuner (no counterpart in the reference, whose CUDA backend takes its
- * launch shapes from per-architecture tables, backends/cuda/lexer.cu:101-193):
- * parses the device-resident sample with each candidate number of resident
- * lexer CTAs per SM (from the occupancy limit down) and keeps the fastest for
- * this handle's grammar. *choice receives it.
+ * launch shapes from per-architecture tables, backends/cuda/lexer.cu:101-193,
+ * backends/cuda/parser.cu:82-136): times the device-resident sample under each
+ * candidate launch geometry and keeps the fastest for this handle's grammar -
+ * first the lexer's window before each chunk (16, 24 or 32 bytes) with its
+ * resident CTAs per SM (the occupancy limit and up to two below it), then
+ * (combined tables) the pair kernel's and then the depth walks' resident
+ * CTAs per SM, each on its own stages' device time. The choice is cached for
+ * the process per (grammar, device): handles loaded afterwards for the same
+ * tables on the same device start with it. *choice receives the lexer's CTAs
+ * per SM. The call synchronises with the handle's stream.
  */
 int alpacc_gpu_autotune(alpacc_gpu_grammar *g, const uint8_t *d_sample, uint64_t n, int *choice);
+
+/* The handle's launch geometry: lexer window bytes, lexer / pair / walk
+   resident CTAs per SM, whether it came from the autotuner's cache at load,
+   the grammar digest that keys that cache. Returns the number of values (6). */
+int alpacc_gpu_geometry(const alpacc_gpu_grammar *g, int64_t *vals, int n);
 
 /* The cudaStream_t the handle launches on, so a caller can order its own work
    (copies, events) with it. */

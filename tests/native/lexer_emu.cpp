@@ -1,7 +1,7 @@
 // Test harness (tests only): a sequential CPU emulation of the tile algorithm
 // of alpacc_b200/csrc/lexer.cu - the same shared-memory tables
 // (build_lexer_table: the machine and its window machine), tile and chunk
-// geometry, the window walk over the 16 bytes before each chunk (in the
+// geometry, the window walk over the 16 to 32 bytes before each chunk (in the
 // window machine, or as an explicit state set from the first window byte's
 // image), the single walk of each chunk whose window left one candidate
 // ("known"), per-candidate end states and codes of the other ("open")
@@ -22,7 +22,7 @@
 
 namespace {
 
-constexpr int kThreads = 256, kWords = 15, kChunk = 60, kWin = 16;
+constexpr int kThreads = 256, kWords = 15, kChunk = 60, kWin = 32;  // kWin: bytes loaded before a tile
 constexpr int kData = kThreads * kChunk, kLoad = kWin + kData;
 enum { kEmpty = 0, kKnown = 1, kOpen = 2, kOpenTail = 3 };
 
@@ -45,9 +45,10 @@ uint32_t pack_codes(uint32_t e0, uint32_t e1, uint32_t e2, uint32_t e3) {
 }  // namespace
 
 // sets: walk windows as explicit state sets (the kernel's variant for
-// machines without a window machine). stats: [0] open chunks, [1] known
-// chunks, [2] tiles that took the look-back, [3] candidate walks.
-extern "C" int lexer_emu(const alpacc_tables *t, const uint8_t *in, uint64_t n, int open_end, int sets,
+// machines without a window machine); win: window bytes (16..32, a multiple
+// of 4). stats: [0] open chunks, [1] known chunks, [2] tiles that took the
+// look-back, [3] candidate walks.
+extern "C" int lexer_emu(const alpacc_tables *t, const uint8_t *in, uint64_t n, int open_end, int sets, int win,
                          uint64_t *out, uint64_t cap, uint64_t *count, int64_t *stats, uint64_t *last_boundary) {
   alpacc::HostGrammar hg;
   std::string why;
@@ -87,7 +88,7 @@ extern "C" int lexer_emu(const alpacc_tables *t, const uint8_t *in, uint64_t n, 
     std::vector<int> x0v(kThreads, -1);
     for (int c = 0; c < kThreads; c++) {
       uint8_t *rb = bytes.data() + kWin + c * kChunk;
-      const uint8_t *wb = rb - kWin;
+      const uint8_t *wb = rb - win;
       const long long g0 = data0 + (long long)c * kChunk;
       int nb = 0;
       if (g0 < (long long)n) nb = (int)std::min<long long>(kChunk, (long long)n - g0);
@@ -98,7 +99,7 @@ extern "C" int lexer_emu(const alpacc_tables *t, const uint8_t *in, uint64_t n, 
         x0 = lm.m0;
       } else if (!sets) {
         uint32_t f = ltab.ps_full, e = 0;
-        for (int j = 0; j < kWin; j++) {
+        for (int j = 0; j < win; j++) {
           e = E.wstep(f, E.c4(wb[j]));
           f = e;
         }
@@ -114,7 +115,7 @@ extern "C" int lexer_emu(const alpacc_tables *t, const uint8_t *in, uint64_t n, 
         std::vector<char> set(lm.M, 0);
         const int c0 = lm.cls[wb[0]];
         for (int l = 0; l < lm.img_cnt[c0]; l++) set[lm.img[(size_t)c0 * alpacc::kMaxLanes + l]] = 1;
-        for (int j = 1; j < kWin; j++) {
+        for (int j = 1; j < win; j++) {
           std::vector<char> ns(lm.M, 0);
           for (int s = 0; s < lm.M; s++)
             if (set[s]) {

@@ -174,15 +174,16 @@ def emu(tmp_path_factory):
     L = ctypes.CDLL(so)
     L.lexer_emu.restype = ctypes.c_int
     L.lexer_emu.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int,
-                            ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64), ctypes.c_void_p,
+                            ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64), ctypes.c_void_p,
                             ctypes.POINTER(ctypes.c_uint64)]
     return L
 
 
-def _emu_vs_machine(L, M, t, inputs, sets=False):
+def _emu_vs_machine(L, M, t, inputs, sets=False, win=16):
     """The tile algorithm of the lexer kernel (emulated) against the machine
     walked byte by byte: status and every lexeme. ``sets``: windows walked as
-    explicit state sets instead of in the window machine."""
+    explicit state sets instead of in the window machine; ``win``: window
+    bytes."""
     s, keep = native.make_tables(t)
     states = ctypes.c_int(0)
     stats = np.zeros(4, dtype=np.int64)
@@ -193,8 +194,8 @@ def _emu_vs_machine(L, M, t, inputs, sets=False):
         got = np.zeros(3 * cap, dtype=np.uint64)
         cw, cg, lb = ctypes.c_uint64(0), ctypes.c_uint64(0), ctypes.c_uint64(0)
         rw = M.machine_lex(ctypes.byref(s), d, len(d), want.ctypes.data, cap, ctypes.byref(cw), ctypes.byref(states))
-        rg = L.lexer_emu(ctypes.byref(s), d, len(d), 0, 1 if sets else 0, got.ctypes.data, cap, ctypes.byref(cg),
-                         stats.ctypes.data, ctypes.byref(lb))
+        rg = L.lexer_emu(ctypes.byref(s), d, len(d), 0, 1 if sets else 0, win, got.ctypes.data, cap,
+                         ctypes.byref(cg), stats.ctypes.data, ctypes.byref(lb))
         total += stats
         assert rg == rw, (t.name, len(d), d[:40], rg, rw)
         if rw == native.OK:
@@ -206,16 +207,18 @@ def _emu_vs_machine(L, M, t, inputs, sets=False):
 TILE = 15360
 
 
-@pytest.mark.parametrize("sets", [False, True], ids=["window_machine", "state_sets"])
+@pytest.mark.parametrize("sets,win", [(False, 16), (True, 16), (False, 32), (True, 24)],
+                         ids=["window_machine16", "state_sets16", "window_machine32", "state_sets24"])
 @pytest.mark.parametrize("config", sorted(cases.CONFIGS))
-def test_lexer_tile_algorithm(harness, emu, config, sets):
+def test_lexer_tile_algorithm(harness, emu, config, sets, win):
     ins = cases.case_inputs(config, sizes=(1, 59, 60, 61, 3000, TILE - 1, TILE, TILE + 1, 3 * TILE + 7),
                             seeds=(0,))
-    _emu_vs_machine(emu, harness, cases.tables(config, "both"), ins, sets)
+    _emu_vs_machine(emu, harness, cases.tables(config, "both"), ins, sets, win)
 
 
-@pytest.mark.parametrize("sets", [False, True], ids=["window_machine", "state_sets"])
-def test_lexer_tile_algorithm_open_chunks(harness, emu, sets):
+@pytest.mark.parametrize("sets,win", [(False, 16), (True, 16), (False, 32)],
+                         ids=["window_machine16", "state_sets16", "window_machine32"])
+def test_lexer_tile_algorithm_open_chunks(harness, emu, sets, win):
     """Inputs whose windows never settle on one state (a numeric array on one
     line is valid both inside and outside a JSON string): per-candidate chunk
     functions and tiles without a known chunk (transition vectors,
@@ -225,7 +228,7 @@ def test_lexer_tile_algorithm_open_chunks(harness, emu, sets):
     nums = b"[" + b", ".join(str(int(x)).encode() for x in rng.integers(0, 1000, 30000)) + b"]"
     mixed = b'{"a": ' + nums + b', "b": "x y z"}'
     bad = nums[:50000] + b"\x01" + nums[50000:]
-    stats = _emu_vs_machine(emu, harness, t, [nums, mixed, bad, nums[:TILE * 2 + 5] + b"]"], sets)
+    stats = _emu_vs_machine(emu, harness, t, [nums, mixed, bad, nums[:TILE * 2 + 5] + b"]"], sets, win)
     assert stats[0] > 1000 and stats[2] > 0  # open chunks and look-back tiles were exercised
 
 
