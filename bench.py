@@ -83,7 +83,9 @@ def ours_serve(a, rank, world, local_rank, dist):
     sizes = np.diff(offs)
     srv = Server(tables, device=local_rank, workers=2, budget=8 << 30)
     plain = Parser(tables, device=local_rank, max_input=int(sizes.max()))
-    warm = np.arange(min(64, len(sizes)), dtype=np.uint32)
+    # warm-up: every pool document once through both arms (grows their scratch
+    # to the largest batch and document before anything is timed)
+    warm = np.arange(len(sizes), dtype=np.uint32)
     srv.replay(pool, offs, warm, np.zeros(len(warm)))
     plain.replay(pool, offs, warm, np.zeros(len(warm)))
     rates = [int(r) for r in a.serve_rates.split(",")]
