@@ -363,6 +363,10 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
 
   CK(cudaMemsetAsync(g->d_status, 0, sizeof(DeviceStatus), g->stream));
   CK(cudaMemsetAsync(fb, 0, fl.total, g->stream));
+  if (g->diag) {  // phase cycles: lexer [0, 8), bracket walk [8, 16), parent walk [16, 24)
+    TRY(grow(g->diag_cycles, sizeof g->phase_cycles));
+    CK(cudaMemsetAsync(g->diag_cycles.p, 0, sizeof g->phase_cycles, g->stream));
+  }
   CK(cudaEventRecord(g->ev0, g->stream));
 
   // ---------------- lexer ----------------
@@ -371,11 +375,7 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
     CK(cudaMemcpyAsync(&g->d_status->num_tokens, &T, 8, cudaMemcpyHostToDevice, g->stream));
   } else if (lexing) {
     LexArgs a = lex_args(g, d_in, n, lex_tiles);
-    if (g->diag) {
-      TRY(grow(g->diag_cycles, 64));
-      CK(cudaMemsetAsync(g->diag_cycles.p, 0, 64, g->stream));
-      a.phase_cycles = (unsigned long long *)g->diag_cycles.p;
-    }
+    if (g->diag) a.phase_cycles = (unsigned long long *)g->diag_cycles.p;
     a.st1_flag = (unsigned *)(fb + fl.st1_flag);
     a.st2.flags = (unsigned *)(fb + fl.st2_flags);
     if (win) {
@@ -435,6 +435,7 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
       pa.resolve_ticket = pa.ticket + 1;
       pa.st.flags = (unsigned *)(fb + fl.pse_flags[walk]);
       pa.super_key = (uint32_t *)(fb + fl.super_key[walk]);
+      if (g->diag) pa.phase_cycles = (unsigned long long *)g->diag_cycles.p + 8 + 8 * walk;
       const uint64_t tiles = (pa.elem_cap + kPseTile - 1) / kPseTile;
       stage_begin(g, 2 + 2 * walk);
       pse_tile_kernel<<<(unsigned)std::max<uint64_t>(std::min<uint64_t>(tiles, (uint64_t)g->pse_grid), 1), kPseThreads,
@@ -443,7 +444,7 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
       stage_end(g, 2 + 2 * walk);
       CK(cudaGetLastError());
       stage_begin(g, 3 + 2 * walk);
-      pse_resolve_kernel<<<148 * 8, 256, 0, g->stream>>>(pa);
+      pse_resolve_kernel<<<resolve_blocks(tiles), 256, 0, g->stream>>>(pa);
       ++g->launches;
       stage_end(g, 3 + 2 * walk);
       CK(cudaGetLastError());
@@ -466,7 +467,8 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
   }
   int rc = sync_status(g);
   if (rc == ALPACC_OK && g->h_status->overflow) rc = ALPACC_E_CAPACITY;  // grown and run again by run_device
-  if (g->diag && lexing && cudaMemcpy(g->phase_cycles, g->diag_cycles.p, 64, cudaMemcpyDeviceToHost) != cudaSuccess)
+  if (g->diag && cudaMemcpy(g->phase_cycles, g->diag_cycles.p, sizeof g->phase_cycles, cudaMemcpyDeviceToHost) !=
+                     cudaSuccess)
     cudaGetLastError();
   float ms = 0;
   if (cudaEventElapsedTime(&ms, g->ev0, g->ev1) == cudaSuccess) g->last_ms = ms;
@@ -1029,16 +1031,15 @@ uint64_t alpacc_device_allocations(void) { return alpacc::g_device_allocs.load(s
 
 int alpacc_gpu_counts(const alpacc_gpu_grammar *g, int64_t *vals, int n) {
   if (!g || !vals || !g->h_status) return ALPACC_E_INVALID;
-  const int64_t v[17] = {(int64_t)g->h_status->num_tokens, (int64_t)g->h_status->num_brackets,
-                         (int64_t)g->h_status->num_productions, (int64_t)g->h_status->num_nodes,
-                         (int64_t)g->h_status->scratch[0], (int64_t)g->h_status->scratch[1],
-                         (int64_t)g->h_status->scratch[2], (int64_t)g->h_status->scratch[3],
-                         (int64_t)g->launches,
-                         (int64_t)g->phase_cycles[0], (int64_t)g->phase_cycles[1], (int64_t)g->phase_cycles[2],
-                         (int64_t)g->phase_cycles[3], (int64_t)g->phase_cycles[4], (int64_t)g->phase_cycles[5],
-                         (int64_t)g->phase_cycles[6], (int64_t)g->phase_cycles[7]};
-  for (int i = 0; i < n && i < 17; i++) vals[i] = v[i];
-  return 17;
+  int64_t v[9 + 24] = {(int64_t)g->h_status->num_tokens, (int64_t)g->h_status->num_brackets,
+                       (int64_t)g->h_status->num_productions, (int64_t)g->h_status->num_nodes,
+                       (int64_t)g->h_status->scratch[0], (int64_t)g->h_status->scratch[1],
+                       (int64_t)g->h_status->scratch[2], (int64_t)g->h_status->scratch[3],
+                       (int64_t)g->launches};
+  for (int i = 0; i < 24; i++) v[9 + i] = (int64_t)g->phase_cycles[i];
+  const int nv = (int)(sizeof v / sizeof v[0]);
+  for (int i = 0; i < n && i < nv; i++) vals[i] = v[i];
+  return nv;
 }
 
 void alpacc_gpu_set_diagnostics(alpacc_gpu_grammar *g, int on) {

@@ -233,7 +233,7 @@ int run_batch(alpacc_gpu_grammar *g, const uint8_t *bytes, const int64_t *offset
     pa.batch = d_bd;
     pa.status = bd.status;
     pse_tile_kernel<<<(unsigned)std::min<uint64_t>(ub, (uint64_t)g->pse_grid), kPseThreads, 0, s>>>(pa);
-    pse_resolve_kernel<<<148 * 8, 256, 0, s>>>(pa);
+    pse_resolve_kernel<<<resolve_blocks(ub), 256, 0, s>>>(pa);
     g->launches += 2;
     BCK(cudaGetLastError());
   }

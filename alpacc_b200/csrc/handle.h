@@ -108,8 +108,8 @@ struct alpacc_gpu_grammar {
   // scratch
   DevBuf in;                                   // device copy of host input
   DevBuf flags;                                // per-call flags, tickets, counters (zeroed each call)
-  DevBuf diag_cycles;                          // diagnostics: lexer phase cycles
-  unsigned long long phase_cycles[8] = {};     // of the last call
+  DevBuf diag_cycles;                          // diagnostics: lexer and walk phase cycles
+  unsigned long long phase_cycles[24] = {};    // of the last call
   DevBuf lex_ticket, st1_flag, st1_state, st1_vec, st2_flags, st2_agg, st2_inc;
   DevBuf codes, tile_cnt, tile_pos, tile_off, tile_prev;  // staged lexer output
   DevBuf tok_ids, tok_starts, tok_lens;

@@ -216,6 +216,11 @@ struct PseArgs {
   PairTileState st;                 // (sum of steps, terminal count)
   DeviceStatus *status;
   const BatchDesc *batch;           // null: one document; else virtual tiles (br_tile0 / pr_tile0)
+  // diagnostics: SM cycles of each phase of pse_tile_kernel summed over tiles
+  // (thread 0's clock): 0 load + steps + scan, 1 depths + windows, 2 own and
+  // previous chunk queries, 3 the warps' queued queries, 4 look-back,
+  // 5 staircase + unanswered queries, 6 tree entries, 7 next tile; null when off
+  unsigned long long *phase_cycles;
 };
 
 __global__ void pse_tile_kernel(PseArgs args);

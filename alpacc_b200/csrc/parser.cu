@@ -349,6 +349,15 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
       s_arity[i] = __ldg(a.arity + i);
       s_is_term[i] = __ldg(a.is_term + i);
     }
+  unsigned long long *pcyc = a.phase_cycles;
+  long long tp = clock64();
+// diagnostics: thread 0 adds the cycles since the previous mark to phase k
+#define PSE_PHASE(k)                                        \
+  if (pcyc && t == 0) {                                     \
+    const long long now_ = clock64();                       \
+    atomicAdd(pcyc + (k), (unsigned long long)(now_ - tp)); \
+    tp = now_;                                              \
+  }
   unsigned long long total;
   if (a.batch) {
     total = (parents ? a.batch->pr_tile0 : a.batch->br_tile0)[a.batch->docs];
@@ -367,6 +376,7 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   }
   for (;;) {
   __syncthreads();  // the previous tile's shared data is consumed
+  PSE_PHASE(7);
   if (t == 0) s_tile = atomicAdd(a.ticket, 1u);
   __syncthreads();
   const unsigned long long tile = s_tile;  // virtual tile in a batch
@@ -420,6 +430,7 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   const long long tot_s = (tot - tot_t) >> 32;
   // publish the aggregate at once; tile 0's aggregate is its inclusive prefix
   if (t == 0) publish_pair(a.st, (long long)tile, Pair64{tot_s, tot_t}, lt == 0);
+  PSE_PHASE(0);
 
   // ---- relative depths, chunk minimum, warp windows ----
   int cmin = INT_MAX;
@@ -442,6 +453,7 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   for (int k = 0; k < 6; ++k) sm.lv[k][t] = L[k];
   if (lane == kWarp - 1) sm.wmin[warp] = L[5];
   __syncthreads();
+  PSE_PHASE(1);
 
   // ---- queries: own chunk, then the previous chunk ----
   // ans: local index of the answer; -1 pending; -2 no query; -3 the root
@@ -491,6 +503,7 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
       need |= 1u << j;
     }
   }
+  PSE_PHASE(2);
   // ---- earlier chunks of the tile: the warp's pending queries, 32 at a
   // time (one per lane, whichever thread they came from) ----
   {
@@ -544,6 +557,7 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
     }
   }
 
+  PSE_PHASE(3);
   // ---- the tile's prefix: look-back by warp 0, now that predecessors had time ----
   if (t < kWarp) {
     Pair64 prefix{0, 0};
@@ -565,6 +579,7 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   }
   __syncthreads();
 
+  PSE_PHASE(4);
   // ---- staircase, unanswered queries, tile minimum ----
   // An element is on the staircase when every later element of the tile is
   // deeper: only those can answer a later tile's query. In position order the
@@ -626,6 +641,7 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
       a.q_cnt[tile] = (uint32_t)(ctot & 0xffffffffll);
     }
   }
+  PSE_PHASE(5);
   if (parents) {
     const int row = t * kPseStride;
 #pragma unroll
@@ -642,7 +658,9 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
       }
     }
   }
+  PSE_PHASE(6);
   }  // tiles
+#undef PSE_PHASE
 }
 
 namespace {

@@ -147,6 +147,12 @@ inline PairArgs pair_args(alpacc_gpu_grammar *g) {
   return a;
 }
 
+// CTAs of pse_resolve_kernel for a walk of at most `tiles` tiles: one warp
+// per tile (8 per CTA), at most 8 CTAs per SM.
+inline unsigned resolve_blocks(uint64_t tiles) {
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(148 * 8, (tiles + 7) / 8));
+}
+
 // Bytes of the walk's per-tile regions for `tiles` tiles: staircase depths,
 // query values, their terminal counts (4 bytes each per entry), staircase and
 // query offsets (2 bytes each), then the two per-tile counts.

@@ -436,14 +436,20 @@ class Parser:
         return wire.encode_record(self.parse(data), self.layout)
 
     def counts(self) -> dict:
-        """Tokens, brackets, productions, nodes of the last call."""
-        vals = (ctypes.c_int64 * 17)()
-        lib().alpacc_gpu_counts(self._h, vals, 17)
+        """Tokens, brackets, productions, nodes of the last call; lexer
+        diagnostic counters; kernel launches; per-phase SM cycles of the lexer
+        and of the two walks' tile kernels (diagnostics on)."""
+        vals = (ctypes.c_int64 * 33)()
+        lib().alpacc_gpu_counts(self._h, vals, 33)
+        walk_phases = ("load_scan", "windows", "near_queries", "queued_queries", "lookback", "staircase",
+                       "tree", "next_tile")
         return {"T": vals[0], "B": vals[1], "P": vals[2], "N": vals[3], "lookback_tiles": vals[4],
                 "known_chunks": vals[5], "chain_evals": vals[6], "candidate_jobs": vals[7], "launches": vals[8],
                 "lexer_phase_cycles": {k: vals[9 + i] for i, k in enumerate(
                     ("load", "window", "walks", "known_scan", "start_states", "open_codes_masks_scan",
-                     "count_lookback", "writes"))}}
+                     "count_lookback", "writes"))},
+                "bracket_walk_phase_cycles": {k: vals[17 + i] for i, k in enumerate(walk_phases)},
+                "parent_walk_phase_cycles": {k: vals[25 + i] for i, k in enumerate(walk_phases)}}
 
     def set_diagnostics(self, on: bool):
         lib().alpacc_gpu_set_diagnostics(self._h, 1 if on else 0)

@@ -376,7 +376,11 @@ int alpacc_gpu_stage_ms(const alpacc_gpu_grammar *g, double *out, int n);
    lexer's CTAs spent in each phase, summed over tiles: load, window walk,
    chunk and candidate walks, known-chunk scan, start states, open chunks'
    codes with the masks and the count scan, the count look-back, the token or
-   code writes. */
+   code writes; then the same for the bracket walk's and the parent walk's
+   tile kernel: load with steps and scan, depths and windows, own and previous
+   chunk queries, the warps' queued queries, look-back, staircase and
+   unanswered queries, tree entries, next tile. Returns the number of values
+   (33). */
 int alpacc_gpu_counts(const alpacc_gpu_grammar *g, int64_t *vals, int n);
 void alpacc_gpu_set_diagnostics(alpacc_gpu_grammar *g, int on);
 /* Number of device allocations (cudaMalloc) this library has made in the
