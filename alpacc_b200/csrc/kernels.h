@@ -46,12 +46,12 @@ __device__ __forceinline__ int batch_doc(const unsigned long long *tile0, int do
 enum PlanKind : int { kPlanPairs = 0, kPlanBrackets = 1, kPlanParents = 2 };
 __global__ void batch_plan_kernel(BatchDesc b, int kind, unsigned long long *tile0, unsigned long long tile);
 
-// ---- lexer tiles: 256 chunks x 15 words (60 bytes), loaded with the 32
-// bytes before the tile (room for the first chunk's window) ----
+// ---- lexer tiles: 256 chunks x 15 words (60 bytes), loaded with the 64
+// bytes before the tile (the first chunk's longest window) ----
 constexpr int kLexThreads = 256;
 constexpr int kLexWords = 15;
 constexpr int kLexChunk = kLexWords * 4;
-constexpr int kLexWin = 32;                                     // most window bytes before a chunk
+constexpr int kLexWin = 64;                                     // bytes loaded before a tile
 constexpr int kLexData = kLexThreads * kLexChunk;               // bytes per tile
 constexpr int kLexLoad = kLexWin + kLexData;                    // bytes loaded per tile
 constexpr int kLexLanes = kMaxLanes;                            // candidate starts of an open chunk

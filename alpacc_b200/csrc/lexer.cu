@@ -13,7 +13,7 @@
 // (entry & 0xFFFFFF) ^ class * 4) and one shared-memory load.
 //
 // A tile is 256 chunks of 60 bytes (15 words: an odd word stride, so per-thread
-// rows are bank-conflict free), loaded with the 32 bytes before it.
+// rows are bank-conflict free), loaded with the 64 bytes before it.
 //
 // Window: each chunk walks the 16 (up to 32: a per-grammar choice of the
 // autotuner) bytes before it in the window machine (the
@@ -21,7 +21,9 @@
 //   of them), which yields the set of states the chunk can start in. On JSON
 //   that set is one state for ~95% of chunks, on s-expressions for all: the
 //   chunk's start is then known without looking at any other chunk
-//   ("known"). The window walk is the same fixed number of steps in every
+//   ("known"). A tile's first chunk whose window leaves several candidates
+//   walks the whole 64 bytes loaded before the tile once more, so that the
+//   tile rarely needs its predecessor's state. The window walk is the same fixed number of steps in every
 //   thread.
 //   Machines whose subset automaton is too large walk the window as an
 //   explicit state set instead.
@@ -410,6 +412,8 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
       } else {
         StateSet<W> cand;
         x0 = window_start<W, kPs>(a, tb, tw, row - a.win_words, a.win_words, &cand);
+        if (x0 < 0 && t == 0 && a.win_words < kWinWords)  // the tile's first chunk: the longest window
+          x0 = window_start<W, kPs>(a, tb, tw, row - kWinWords, kWinWords, &cand);
         if (x0 < 0) {
 #pragma unroll
           for (int i = 0; i < W; i++) sm->cand[i][t] = cand.w[i];

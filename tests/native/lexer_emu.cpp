@@ -1,7 +1,8 @@
 // Test harness (tests only): a sequential CPU emulation of the tile algorithm
 // of alpacc_b200/csrc/lexer.cu - the same shared-memory tables
 // (build_lexer_table: the machine and its window machine), tile and chunk
-// geometry, the window walk over the 16 to 32 bytes before each chunk (in the
+// geometry, the window walk over the 16 to 32 bytes before each chunk (64 for
+// a tile's first chunk whose shorter window leaves candidates; in the
 // window machine, or as an explicit state set from the first window byte's
 // image), the single walk of each chunk whose window left one candidate
 // ("known"), per-candidate end states and codes of the other ("open")
@@ -22,7 +23,7 @@
 
 namespace {
 
-constexpr int kThreads = 256, kWords = 15, kChunk = 60, kWin = 32;  // kWin: bytes loaded before a tile
+constexpr int kThreads = 256, kWords = 15, kChunk = 60, kWin = 64;  // kWin: bytes loaded before a tile
 constexpr int kData = kThreads * kChunk, kLoad = kWin + kData;
 enum { kEmpty = 0, kKnown = 1, kOpen = 2, kOpenTail = 3 };
 
@@ -88,48 +89,54 @@ extern "C" int lexer_emu(const alpacc_tables *t, const uint8_t *in, uint64_t n, 
     std::vector<int> x0v(kThreads, -1);
     for (int c = 0; c < kThreads; c++) {
       uint8_t *rb = bytes.data() + kWin + c * kChunk;
-      const uint8_t *wb = rb - win;
       const long long g0 = data0 + (long long)c * kChunk;
       int nb = 0;
       if (g0 < (long long)n) nb = (int)std::min<long long>(kChunk, (long long)n - g0);
       nbv[c] = nb;
       if (nb == 0) continue;
-      int x0 = -1;
-      if (g0 == 0) {
-        x0 = lm.m0;
-      } else if (!sets) {
-        uint32_t f = ltab.ps_full, e = 0;
-        for (int j = 0; j < win; j++) {
-          e = E.wstep(f, E.c4(wb[j]));
-          f = e;
-        }
-        const uint32_t info = e >> 24;
-        if (info != 0xFF) {
-          x0 = (int)info;
-        } else {
+      // the window of `len` bytes ending at the chunk: its one state (the dead
+      // state when none), or -1 with the candidates in cv
+      auto window = [&](int len, std::vector<int> &cv) -> int {
+        const uint8_t *w0 = rb - len;
+        cv.clear();
+        if (!sets) {
+          uint32_t f = ltab.ps_full, e = 0;
+          for (int j = 0; j < len; j++) {
+            e = E.wstep(f, E.c4(w0[j]));
+            f = e;
+          }
+          const uint32_t info = e >> 24;
+          if (info != 0xFF) return (int)info;
           const int p = E.state_of(e);
           for (int s = 0; s < lm.M; s++)
-            if (ltab.ps_mask[(size_t)p * 4 + (s >> 6)] >> (s & 63) & 1) cand[c].push_back(s);
+            if (ltab.ps_mask[(size_t)p * 4 + (s >> 6)] >> (s & 63) & 1) cv.push_back(s);
+          return -1;
         }
-      } else {
         std::vector<char> set(lm.M, 0);
-        const int c0 = lm.cls[wb[0]];
+        const int c0 = lm.cls[w0[0]];
         for (int l = 0; l < lm.img_cnt[c0]; l++) set[lm.img[(size_t)c0 * alpacc::kMaxLanes + l]] = 1;
-        for (int j = 1; j < win; j++) {
+        for (int j = 1; j < len; j++) {
           std::vector<char> ns(lm.M, 0);
           for (int s = 0; s < lm.M; s++)
             if (set[s]) {
-              const int nx = E.state_of(E.step(E.row_of((uint32_t)s), E.c4(wb[j])));
+              const int nx = E.state_of(E.step(E.row_of((uint32_t)s), E.c4(w0[j])));
               if (nx != dead) ns[nx] = 1;
             }
           set.swap(ns);
         }
         const int live = (int)std::count(set.begin(), set.end(), 1);
-        if (live == 0) x0 = dead;
-        else if (live == 1) x0 = (int)(std::find(set.begin(), set.end(), 1) - set.begin());
-        else
-          for (int s = 0; s < lm.M; s++)
-            if (set[s]) cand[c].push_back(s);
+        if (live == 0) return dead;
+        if (live == 1) return (int)(std::find(set.begin(), set.end(), 1) - set.begin());
+        for (int s = 0; s < lm.M; s++)
+          if (set[s]) cv.push_back(s);
+        return -1;
+      };
+      int x0 = -1;
+      if (g0 == 0) {
+        x0 = lm.m0;
+      } else {
+        x0 = window(win, cand[c]);
+        if (x0 < 0 && c == 0 && win < kWin) x0 = window(kWin, cand[c]);  // the tile's first chunk: the longest window
       }
       x0v[c] = x0;
     }
