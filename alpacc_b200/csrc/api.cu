@@ -79,6 +79,11 @@ int upload_tables(alpacc_gpu_grammar *g) {
   g->cp_shift = lt.shift;
   g->swz = lt.swz;
   g->wide_cls = lt.wide_cls;
+  // ALPACC_LEX_OUTPUT=direct writes the tokens from the lexer kernel itself
+  // (counts chained by decoupled look-back) instead of staging boundary codes
+  // for the scan and emit kernels
+  const char *ov = std::getenv("ALPACC_LEX_OUTPUT");
+  g->lex_direct = ov && std::strcmp(ov, "direct") == 0 ? 1 : 0;
   // ALPACC_LEX_WINDOW=sets walks windows as explicit state sets even when the
   // window machine exists (tests run that kernel on small machines too)
   const char *wv = std::getenv("ALPACC_LEX_WINDOW");
@@ -146,11 +151,17 @@ int sync_status(alpacc_gpu_grammar *g) {
   return ALPACC_OK;
 }
 
+// Per-stage device times (events around each stage's launches), recorded
+// only while stage timing is on: two event records per stage cost host time
+// that a small input's call feels.
 void stage_begin(alpacc_gpu_grammar *g, int k) {
+  if (!g->stage_timing) return;
   cudaEventRecord(g->sev[2 * k], g->stream);
   g->stage_used[k] = true;
 }
-void stage_end(alpacc_gpu_grammar *g, int k) { cudaEventRecord(g->sev[2 * k + 1], g->stream); }
+void stage_end(alpacc_gpu_grammar *g, int k) {
+  if (g->stage_timing) cudaEventRecord(g->sev[2 * k + 1], g->stream);
+}
 void collect_stages(alpacc_gpu_grammar *g) {
   for (int k = 0; k < alpacc_gpu_grammar::kStages; k++) {
     float ms = 0;
@@ -395,11 +406,13 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
       a.tile_end = t1;
       a.ticket = (unsigned *)(fb + fl.lex_ticket) + 4 + k;
       const unsigned grid = (unsigned)std::min<uint64_t>(t1 - t0, (uint64_t)g->lex_grid);
-      CK(launch_lex(g, a, grid, g->stream));
+      CK(g->lex_direct ? launch_lex_direct(g, a, grid, g->stream) : launch_lex(g, a, grid, g->stream));
       ++g->launches;
     }
-    CK(launch_lex_emit(lex_emit_args(g, a), g->stream));
-    g->launches += 2;
+    if (!g->lex_direct) {
+      CK(launch_lex_emit(lex_emit_args(g, a), g->stream));
+      g->launches += 2;
+    }
     stage_end(g, 0);
   }
   CK(cudaEventRecord(g->lex_done, g->stream));
@@ -946,6 +959,12 @@ int alpacc_gpu_autotune(alpacc_gpu_grammar *g, const uint8_t *d_sample, uint64_t
     return ms / 2;
   };
   Geometry geo{g->lex_win_words, g->lex_grid / sms, g->pair_grid / sms, g->pse_grid / sms};
+  struct TimingOn {  // stage times while tuning; the caller's setting afterwards
+    alpacc_gpu_grammar *g;
+    int was;
+    ~TimingOn() { g->stage_timing = was; }
+  } timing_on{g, g->stage_timing};
+  g->stage_timing = 1;
   double best = -1.0;
   // lexer: window length x resident CTAs per SM (fewer CTAs: less contention
   // for shared-memory banks and the look-back; more: more latency hidden)
@@ -1044,6 +1063,10 @@ int alpacc_gpu_counts(const alpacc_gpu_grammar *g, int64_t *vals, int n) {
 
 void alpacc_gpu_set_diagnostics(alpacc_gpu_grammar *g, int on) {
   if (g) g->diag = on;
+}
+
+void alpacc_gpu_set_stage_timing(alpacc_gpu_grammar *g, int on) {
+  if (g) g->stage_timing = on ? 1 : 0;
 }
 
 int alpacc_gpu_stage_ms(const alpacc_gpu_grammar *g, double *out, int n) {

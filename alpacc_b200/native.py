@@ -138,6 +138,7 @@ def lib():
         L.alpacc_gpu_counts.restype = ctypes.c_int
         L.alpacc_gpu_counts.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
         L.alpacc_gpu_set_diagnostics.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.alpacc_gpu_set_stage_timing.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.alpacc_gpu_stream.restype = ctypes.c_void_p
         L.alpacc_gpu_stream.argtypes = [ctypes.c_void_p]
         L.alpacc_gpu_last_error.restype = ctypes.c_char_p
@@ -453,6 +454,10 @@ class Parser:
 
     def set_diagnostics(self, on: bool):
         lib().alpacc_gpu_set_diagnostics(self._h, 1 if on else 0)
+
+    def set_stage_timing(self, on: bool):
+        """Record per-stage device times (stage_ms); off by default."""
+        lib().alpacc_gpu_set_stage_timing(self._h, 1 if on else 0)
 
     def stream_handle(self) -> int:
         """The cudaStream_t the handle launches on."""

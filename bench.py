@@ -447,6 +447,7 @@ def ours(a, rank, world, local_rank, dist):
 
     if not a.no_autotune:  # launch geometry for this grammar, tuned on the document (outside the timed region)
         parser.autotune(d_in.data_ptr(), n)
+    parser.set_stage_timing(True)  # per-stage device times for the line's stage_ms and roofline
     for _ in range(a.warmup):
         rc, r = step()
     if rc != (1 if wl["reject"] else 0):

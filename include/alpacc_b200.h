@@ -364,9 +364,12 @@ void *alpacc_gpu_stream(alpacc_gpu_grammar *g);
  */
 int alpacc_gpu_info(const alpacc_gpu_grammar *g, int64_t *vals, int nvals);
 const char *alpacc_gpu_last_error(const alpacc_gpu_grammar *g);
-/* Device time of each kernel of the last call (ms): lexer, pair expansion,
-   bracket walk, bracket resolve, parent walk, parent resolve, compaction. */
+/* Device time of each stage of the last call (ms): lexer, pair expansion,
+   bracket walk, bracket resolve, parent walk, parent resolve; zeros unless
+   stage timing is on (alpacc_gpu_set_stage_timing, off by default: its event
+   records cost a small input's call host time). */
 int alpacc_gpu_stage_ms(const alpacc_gpu_grammar *g, double *out, int n);
+void alpacc_gpu_set_stage_timing(alpacc_gpu_grammar *g, int on);
 /* Tokens, brackets, productions and tree nodes of the last call, then four
    lexer diagnostic counters (collected when diagnostics are on): tiles that
    read their incoming state from the previous tile, chunks whose start state
