@@ -79,6 +79,9 @@ constexpr int kWinWords = kLexWin / 4;  // words loaded before the tile
 // one job per thread); the first kCodeJobs keep their codes, so the chunk's
 // second pass copies the true candidate's codes instead of walking again.
 constexpr int kCodeJobs = 64;
+// Tokens staged per window by lex_emit_kernel before consecutive threads
+// write them out.
+constexpr int kTokWin = 2048;
 
 // The set of states an open chunk can start in, W 64-bit words.
 template <int W>
@@ -796,6 +799,9 @@ __global__ void __launch_bounds__(kLexScanThreads) lex_scan_kernel(LexEmitArgs a
 // byte n) after the last chunk's.
 __global__ void __launch_bounds__(256) lex_emit_kernel(LexEmitArgs a) {
   __shared__ __align__(16) uint32_t rows[kLexThreads * kLexWords];
+  // window of the tile's tokens, written out by consecutive threads
+  __shared__ uint32_t s_start[kTokWin], s_len[kTokWin];
+  __shared__ uint8_t s_id[kTokWin];
   __shared__ int sa[8], sb[8];
   const int t = threadIdx.x;
   for (unsigned long long tile = blockIdx.x; tile < a.num_tiles; tile += gridDim.x) {
@@ -808,7 +814,7 @@ __global__ void __launch_bounds__(256) lex_emit_kernel(LexEmitArgs a) {
       n = (long long)a.batch->n[d];
       st = a.batch->status + d;
     }
-    __syncthreads();  // the previous tile's rows are consumed
+    __syncthreads();  // the previous tile's rows and window are consumed
     const uint4 *src = reinterpret_cast<const uint4 *>(a.codes + tile * (unsigned long long)kLexData);
     for (int v = t; v < kLexData / 16; v += kLexThreads) reinterpret_cast<uint4 *>(rows)[v] = src[v];
     __syncthreads();
@@ -836,36 +842,54 @@ __global__ void __launch_bounds__(256) lex_emit_kernel(LexEmitArgs a) {
     const int lastb = bmask ? (int)(g0 + 63 - __clzll((long long)bmask)) : 0;
     int cnt_ex, pos_ex, cnt_tot, pos_tot;
     block_exclusive_scan2(sa, sb, cnt, lastb, &cnt_ex, &pos_ex, &cnt_tot, &pos_tot);
-    if (nb > 0) {
-      unsigned long long out = a.tile_off[tile] + (unsigned long long)cnt_ex;
-      const long long tp = (long long)a.tile_prev[tile];
-      long long prev = tp > pos_ex ? tp : pos_ex;  // 0: the token starts at byte 0
-      const unsigned long long len_max = a.len_max;
-      const unsigned long long base = a.index_base;
-      bool too_long = false;
-      for (unsigned long long m = bmask; m; m &= m - 1) {
-        const int j = __ffsll((long long)m) - 1;
-        const long long p = g0 + j;
-        const uint32_t code = rb[j];
-        if (code < kIgnored) {
-          const unsigned long long len = (unsigned long long)(p - prev);
-          too_long |= len > len_max;
-          store_uint(a.tok_ids, out, a.term_w, code);
-          store_uint(a.tok_starts, out, a.idx_w, base + (unsigned long long)prev);
-          store_uint(a.tok_lens, out, a.len_w, len);
-          ++out;
+    const unsigned long long out0 = a.tile_off[tile];
+    const long long tp = (long long)a.tile_prev[tile];
+    const unsigned long long len_max = a.len_max;
+    const unsigned long long base = a.index_base;
+    const uint32_t final_term = final_kept ? (uint32_t)st->final_term : 0u;
+    bool too_long = false;
+    // the tile's tokens in windows of kTokWin: each thread puts its chunk's
+    // tokens that fall in the window at their places, then consecutive
+    // threads write the window out (positions are < 2^31: 32-bit staging)
+    for (int w0 = 0; w0 < cnt_tot; w0 += kTokWin) {
+      if (nb > 0 && cnt_ex < w0 + kTokWin && cnt_ex + cnt > w0) {
+        int o = cnt_ex - w0;
+        long long prev = tp > pos_ex ? tp : pos_ex;  // 0: the token starts at byte 0
+        for (unsigned long long m = bmask; m; m &= m - 1) {
+          const int j = __ffsll((long long)m) - 1;
+          const long long p = g0 + j;
+          const uint32_t code = rb[j];
+          if (code < kIgnored) {
+            if (o >= 0 && o < kTokWin) {
+              const unsigned long long len = (unsigned long long)(p - prev);
+              too_long |= len > len_max;
+              s_id[o] = (uint8_t)code;
+              s_start[o] = (uint32_t)prev;
+              s_len[o] = (uint32_t)len;
+            }
+            ++o;
+          }
+          prev = p;
         }
-        prev = p;
+        if (final_kept && o >= 0 && o < kTokWin) {
+          const unsigned long long len = (unsigned long long)(n - prev);
+          too_long |= len > len_max;
+          s_id[o] = (uint8_t)final_term;
+          s_start[o] = (uint32_t)prev;
+          s_len[o] = (uint32_t)len;
+        }
       }
-      if (final_kept) {
-        const unsigned long long len = (unsigned long long)(n - prev);
-        too_long |= len > len_max;
-        store_uint(a.tok_ids, out, a.term_w, (unsigned long long)st->final_term);
-        store_uint(a.tok_starts, out, a.idx_w, base + (unsigned long long)prev);
-        store_uint(a.tok_lens, out, a.len_w, len);
+      __syncthreads();
+      const int wn = cnt_tot - w0 < kTokWin ? cnt_tot - w0 : kTokWin;
+      const unsigned long long ob = out0 + (unsigned long long)w0;
+      for (int i = t; i < wn; i += kLexThreads) {
+        store_uint(a.tok_ids, ob + i, a.term_w, s_id[i]);
+        store_uint(a.tok_starts, ob + i, a.idx_w, base + s_start[i]);
+        store_uint(a.tok_lens, ob + i, a.len_w, s_len[i]);
       }
-      if (too_long) record_reject(st, &st->lex_reject_reason, 3);
+      __syncthreads();
     }
+    if (too_long) record_reject(st, &st->lex_reject_reason, 3);
   }
 }
 
