@@ -262,13 +262,19 @@ struct PseSmem {
   int32_t tc[kPseThreads * kPseStride];  // parents: inclusive terminal count, relative to the tile start
   int32_t lv[6][kPseThreads];            // lv[k][i]: minimum of chunk minima over (i - 2^k, i] within i's warp
   int32_t wmin[kPseWarps];               // minimum of each warp's chunk minima
-  uint16_t wq[kPseTile];                 // per warp: its pending queries (element index in the tile)
-  int16_t wans[kPseTile];                // answer of a pending query (element index), or -1
+  union {
+    struct {
+      uint16_t wq[kPseTile];    // per warp: its pending queries (element index in the tile)
+      int16_t wans[kPseTile];   // answer of a pending query (element index), or -1
+    };
+    int32_t pnew[kPseTile];     // parents, after the queries: each element's tree parent, or kNoParent
+  };
   long long tmp[kPseWarps];
   long long prefix_a, prefix_b;
 };
 
 constexpr int kPseSmemProds = 1024;  // production tables copied to shared memory up to this size
+constexpr int32_t kNoParent = INT_MIN;  // the element's parent is found by the resolve kernel
 
 // compact_tree's output for production e (parser.c:126-153): terminal
 // productions give their token's parent, the others a tree node; parents are
@@ -643,19 +649,29 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   }
   PSE_PHASE(5);
   if (parents) {
-    const int row = t * kPseStride;
+    // each element's parent (answered in this tile) into shared memory, then
+    // the tree entries written by consecutive threads for consecutive
+    // elements (their places in each output array are consecutive)
 #pragma unroll
     for (int j = 0; j < kPseItems; ++j) {
       const int an = ans[j];
-      const int tc = sm.tc[row + j];
-      const bool term = tc != (j > 0 ? sm.tc[row + j - 1] : ex_t);
+      int32_t pn = kNoParent;
       if (an == -3) {  // the root: compute_parents gives it parent 0
-        emit_node(a, dv, sm.v[row + j], term, c0 + j, pb + tc, 0 - (pb + sm.tc[0]));
+        pn = (int32_t)(0 - (pb + sm.tc[0]));
       } else if (an >= 0) {
-        const long long p = tile0 + an;
-        const long long tinc_p = pb + sm.tc[(an / kPseItems) * kPseStride + an % kPseItems];
-        emit_node(a, dv, sm.v[row + j], term, c0 + j, pb + tc, p - tinc_p);
+        pn = (int32_t)(tile0 + an - (pb + sm.tc[(an / kPseItems) * kPseStride + an % kPseItems]));
       }
+      sm.pnew[t * kPseItems + j] = pn;
+    }
+    __syncthreads();
+    for (int i = t; i < kPseTile; i += kPseThreads) {
+      const long long e = tile0 + i;
+      const int32_t pn = sm.pnew[i];
+      if (e >= E || pn == kNoParent) continue;
+      const int r = (i / kPseItems) * kPseStride + i % kPseItems;
+      const int tc = sm.tc[r];
+      const int tprev = i == 0 ? 0 : sm.tc[i % kPseItems ? r - 1 : r - kPseStride + kPseItems - 1];
+      emit_node(a, dv, sm.v[r], tc != tprev, e, pb + tc, pn);
     }
   }
   PSE_PHASE(6);
