@@ -508,7 +508,7 @@ def ours(a, rank, world, local_rank, dist):
     kb = kernel_bytes(dom, n, T, B, P, N, lay)
     achieved = kb / (mean[dom] / 1e3) / 1e9 if mean[dom] > 0 else 0.0
     path_bytes = algorithmic_bytes(n, T, N, lay)
-    traffic = committed_traffic(dom)
+    traffic = committed_traffic(a.workload, dom, n)
     line = {
         "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
@@ -555,15 +555,21 @@ def record_parity(parser, pin, host: bytes, ref_config: str):
             "oracle_s": round(time.perf_counter() - t0, 2)}
 
 
-def committed_traffic(kernel: str):
-    """DRAM bytes per launch from the committed ncu summary, if one exists."""
+def committed_traffic(workload: str, kernel: str, n: int):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary of the
+    same workload family (profiles/traffic.json: bytes of one captured launch
+    and the input size it processed), scaled to n bytes of input; None when
+    there is no capture for it."""
     p = os.path.join(REPO, "profiles", "traffic.json")
     if not os.path.exists(p):
         return None
     with open(p) as f:
         d = json.load(f)
-    v = d.get(kernel)
-    return v.get("bytes_per_launch_full_size") if isinstance(v, dict) else None
+    fam = "sexp" if workload.startswith("sexp") else "json"
+    v = d.get(fam, {}).get(kernel)
+    if not isinstance(v, dict) or not v.get("input_bytes"):
+        return None
+    return int(v["bytes_per_launch"] * n / v["input_bytes"])
 
 
 def main():
