@@ -171,19 +171,26 @@ void collect_stages(alpacc_gpu_grammar *g) {
   }
 }
 
-// The kernel attribute is per function, shared by every handle: only raise it.
-int ensure_lex_smem(size_t bytes) {
+// The dynamic shared-memory attribute of the lexer kernels, per device (the
+// caller's current device) and shared by every handle on it: only raised.
+int ensure_lex_smem(int device, size_t bytes) {
   static std::mutex mu;
-  static size_t current = 0;
+  static std::map<int, size_t> current;
   std::lock_guard<std::mutex> lock(mu);
-  if (bytes <= current) return ALPACC_OK;
+  size_t &cur = current[device];
+  if (bytes <= cur) return ALPACC_OK;
+  if (cur == 0 &&
+      cudaFuncSetAttribute(lex_emit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kLexEmitSmem) != cudaSuccess) {
+    cudaGetLastError();
+    return ALPACC_E_CUDA;
+  }
   for (auto k : {lex_kernel, lex_kernel_wide, lex_kernel_sets, lex_direct_kernel, lex_direct_kernel_wide,
                  lex_direct_kernel_sets})
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) {
       cudaGetLastError();
       return ALPACC_E_CUDA;
     }
-  current = bytes;
+  cur = bytes;
   return ALPACC_OK;
 }
 
@@ -586,7 +593,7 @@ alpacc_gpu_grammar *alpacc_gpu_load(const alpacc_tables *tables, int device, uin
   }
   std::memset(g->h_status, 0, sizeof(DeviceStatus));
   rc = upload_tables(g);
-  if (rc == ALPACC_OK) rc = ensure_lex_smem(lex_dyn_smem(g));
+  if (rc == ALPACC_OK) rc = ensure_lex_smem(device, lex_dyn_smem(g));
   if (rc == ALPACC_OK) {
     int per_sm = 0, sms = 0;
     int pair_sm = 0, pse_sm = 0;

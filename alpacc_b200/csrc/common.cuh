@@ -143,6 +143,19 @@ __device__ __forceinline__ T block_exclusive_scan(T v, Op op, T identity, T *sme
   return res;
 }
 
+// 16-byte asynchronous global-to-shared copies (cp.async, cache-global):
+// issued now, waited for with cp_async_wait<n> (at most n groups left in
+// flight); both addresses 16-byte aligned.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 struct AddU64 {
   __device__ __forceinline__ unsigned long long operator()(unsigned long long a, unsigned long long b) const {
     return a + b;

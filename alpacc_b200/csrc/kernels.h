@@ -144,6 +144,7 @@ struct LexEmitArgs {
 constexpr int kLexScanThreads = 1024;
 __global__ void lex_scan_kernel(LexEmitArgs args);  // one CTA
 __global__ void lex_emit_kernel(LexEmitArgs args);  // CTAs over tiles
+constexpr int kLexEmitSmem = 2 * kLexData + 9 * 2048;  // its dynamic shared memory (bytes)
 
 // ---- pair lookup / stack-action expansion: 256 threads x 8 positions ----
 constexpr int kPairThreads = 256;

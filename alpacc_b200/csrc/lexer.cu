@@ -82,6 +82,7 @@ constexpr int kCodeJobs = 64;
 // Tokens staged per window by lex_emit_kernel before consecutive threads
 // write them out.
 constexpr int kTokWin = 2048;
+static_assert(kLexEmitSmem == 2 * kLexData + 9 * kTokWin, "emit kernel shared memory");
 
 // The set of states an open chunk can start in, W 64-bit words.
 template <int W>
@@ -798,13 +799,25 @@ __global__ void __launch_bounds__(kLexScanThreads) lex_scan_kernel(LexEmitArgs a
 // the length_t check (lexer.c:68-72); the input's last token (kept, ending at
 // byte n) after the last chunk's.
 __global__ void __launch_bounds__(256) lex_emit_kernel(LexEmitArgs a) {
-  __shared__ __align__(16) uint32_t rows[kLexThreads * kLexWords];
-  // window of the tile's tokens, written out by consecutive threads
-  __shared__ uint32_t s_start[kTokWin], s_len[kTokWin];
-  __shared__ uint8_t s_id[kTokWin];
+  // dynamic shared memory (kLexEmitSmem bytes): two buffers of a tile's
+  // codes (the next tile's are copied in while this one's are turned into
+  // tokens), then a window of the tile's tokens written out by consecutive
+  // threads
+  extern __shared__ __align__(16) unsigned char emit_smem[];
+  uint32_t(*rows2)[kLexThreads * kLexWords] = reinterpret_cast<uint32_t(*)[kLexThreads * kLexWords]>(emit_smem);
+  uint32_t *s_start = reinterpret_cast<uint32_t *>(emit_smem + 2 * kLexData);
+  uint32_t *s_len = s_start + kTokWin;
+  uint8_t *s_id = reinterpret_cast<uint8_t *>(s_len + kTokWin);
   __shared__ int sa[8], sb[8];
   const int t = threadIdx.x;
-  for (unsigned long long tile = blockIdx.x; tile < a.num_tiles; tile += gridDim.x) {
+  auto fetch = [&](unsigned long long tl, uint32_t *dst) {
+    const uint8_t *src = a.codes + tl * (unsigned long long)kLexData;
+    for (int v = t; v < kLexData / 16; v += kLexThreads) cp_async16(dst + 4 * v, src + 16 * v);
+  };
+  if (blockIdx.x < a.num_tiles) fetch(blockIdx.x, rows2[0]);
+  cp_async_commit();
+  int buf = 0;
+  for (unsigned long long tile = blockIdx.x; tile < a.num_tiles; tile += gridDim.x, buf ^= 1) {
     long long n = (long long)a.n;
     unsigned long long lt = tile;
     DeviceStatus *st = a.status;
@@ -814,10 +827,13 @@ __global__ void __launch_bounds__(256) lex_emit_kernel(LexEmitArgs a) {
       n = (long long)a.batch->n[d];
       st = a.batch->status + d;
     }
-    __syncthreads();  // the previous tile's rows and window are consumed
-    const uint4 *src = reinterpret_cast<const uint4 *>(a.codes + tile * (unsigned long long)kLexData);
-    for (int v = t; v < kLexData / 16; v += kLexThreads) reinterpret_cast<uint4 *>(rows)[v] = src[v];
+    // the next tile's codes into the other buffer (read by everyone for the
+    // tile before this one: the barrier that ended it has passed)
+    if (tile + gridDim.x < a.num_tiles) fetch(tile + gridDim.x, rows2[buf ^ 1]);
+    cp_async_commit();
+    cp_async_wait<1>();  // this tile's copies (all but the group just issued)
     __syncthreads();
+    const uint32_t *rows = rows2[buf];
     const long long g0 = (long long)lt * kLexData + (long long)t * kLexChunk;
     int nb = 0;
     if (g0 < n) nb = (int)min((long long)kLexChunk, n - g0);
@@ -890,7 +906,9 @@ __global__ void __launch_bounds__(256) lex_emit_kernel(LexEmitArgs a) {
       __syncthreads();
     }
     if (too_long) record_reject(st, &st->lex_reject_reason, 3);
+    __syncthreads();  // this tile's rows and window are consumed
   }
+  cp_async_wait<0>();
 }
 
 }  // namespace alpacc

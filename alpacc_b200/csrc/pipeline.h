@@ -108,7 +108,7 @@ inline LexEmitArgs lex_emit_args(const alpacc_gpu_grammar *g, const LexArgs &a) 
 // The scan and emit kernels after the staged lexer's launches.
 inline cudaError_t launch_lex_emit(const LexEmitArgs &e, cudaStream_t s) {
   lex_scan_kernel<<<1, kLexScanThreads, 0, s>>>(e);
-  lex_emit_kernel<<<(unsigned)std::min<unsigned long long>(e.num_tiles, 148ull * 8), 256, 0, s>>>(e);
+  lex_emit_kernel<<<(unsigned)std::min<unsigned long long>(e.num_tiles, 148ull * 4), 256, kLexEmitSmem, s>>>(e);
   return cudaGetLastError();
 }
 
