@@ -156,6 +156,14 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// L2 prefetch of the 16-byte-aligned interior of [p, p + bytes) with one
+// bulk prefetch (nothing outside the range is touched).
+__device__ __forceinline__ void prefetch_l2(const void *p, unsigned long long bytes) {
+  const unsigned long long a = ((unsigned long long)p + 15) & ~15ull;
+  const unsigned long long e = ((unsigned long long)p + bytes) & ~15ull;
+  if (e > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a), "r"((unsigned)(e - a)) : "memory");
+}
+
 struct AddU64 {
   __device__ __forceinline__ unsigned long long operator()(unsigned long long a, unsigned long long b) const {
     return a + b;

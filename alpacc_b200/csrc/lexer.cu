@@ -355,6 +355,13 @@ __device__ __forceinline__ void lex_body(const LexArgs &a, unsigned char *dyn_sm
     __syncthreads();
     const unsigned long long tile = a.tile_begin + sm->tile;
     if (tile >= tile_end) break;
+    if (t == 0 && !a.batch && tile + gridDim.x < tile_end) {
+      // warm L2 with the bytes of the tile a CTA takes about one tile time
+      // from now (tickets go out in order)
+      const long long p0 = (long long)(tile + gridDim.x) * kLexData - kLexWin;
+      const long long p1 = min((long long)a.n, p0 + (long long)kLexLoad);
+      if (p1 > p0) prefetch_l2(a.in + p0, (unsigned long long)(p1 - p0));
+    }
     // this tile's document: the whole input, or one document of a batch
     // (virtual tile `tile` is local tile `lt` of `tiles_t`)
     const uint8_t *in_base = a.in;

@@ -394,6 +394,13 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   const unsigned long long lt = tile - dv.tile_first;
   const long long tile0 = (long long)lt * kPseTile;  // elements are indexed within the document
   if (tile0 >= E) continue;
+  if (t == 0 && !a.batch && tile0 + (long long)gridDim.x * kPseTile < E) {
+    // warm L2 with the elements of the tile a CTA takes about one tile time
+    // from now (tickets go out in order)
+    const long long e0 = tile0 + (long long)gridDim.x * kPseTile;
+    const long long e1 = min(E, e0 + (long long)kPseTile);
+    prefetch_l2(dv.elems + e0, (unsigned long long)(e1 - e0) * 4);
+  }
   const long long c0 = tile0 + (long long)t * kPseItems;  // first element of this thread's chunk
 
   // ---- load ----
