@@ -277,7 +277,7 @@ struct LexWindow {
 // buffer, zeroed by one memset per call (byte offsets, 16-byte aligned).
 struct FlagLayout {
   size_t lex_ticket = 0, st1_flag = 0, st2_flags = 0, pair_ticket = 0, pst_flags = 0;
-  size_t pse_ticket[2] = {}, pse_flags[2] = {}, super_key[2] = {};
+  size_t pse_ticket[2] = {}, pse_flags[2] = {}, super_key[2] = {}, walk_step[2] = {}, walk_term = 0;
   size_t total = 0;
   size_t take(size_t bytes) {
     const size_t off = total;
@@ -345,7 +345,9 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
     fl.pse_ticket[w] = fl.take(16);
     fl.pse_flags[w] = fl.take(parsing ? pse_tiles * 4 : 0);
     fl.super_key[w] = fl.take(parsing ? super_n * 4 : 0);
+    fl.walk_step[w] = fl.take(parsing ? pse_tiles * 4 : 0);
   }
+  fl.walk_term = fl.take(parsing ? pse_tiles * 4 : 0);
   TRY(grow(g->flags, fl.total));
   uint8_t *fb = (uint8_t *)g->flags.p;
   if (lexing) {
@@ -374,6 +376,7 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
     TRY(grow(g->pse_inc, pse_tiles * 16));
     TRY(grow(g->tile_min, pse_tiles * 4));
     TRY(grow(g->pse_regions, pse_region_bytes(pse_tiles)));
+    TRY(grow(g->walk_prefix, std::max<uint64_t>(pse_tiles, 1) * 3 * 8));
     TRY(grow(g->node_prods, std::max<uint64_t>(pr_cap, 1) * prod_w));
     TRY(grow(g->node_parents, std::max<uint64_t>(pr_cap, 1) * idx_w));
     TRY(grow(g->token_parents, std::max<uint64_t>(T_ub, 1) * idx_w));
@@ -440,11 +443,32 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
     a.pr_cap = pr_cap;
     a.ticket = (unsigned *)(fb + fl.pair_ticket);
     a.st.flags = (unsigned *)(fb + fl.pst_flags);
+    // the walks' tile prefixes come from the pair kernel's aggregates
+    a.walk_step[0] = (int *)(fb + fl.walk_step[0]);
+    a.walk_step[1] = (int *)(fb + fl.walk_step[1]);
+    a.walk_term = (int *)(fb + fl.walk_term);
+    a.walk_tiles_cap = pse_tiles;
+    long long *pfx = (long long *)g->walk_prefix.p;
+    const uint64_t pt_n = std::max<uint64_t>(pse_tiles, 1);
     stage_begin(g, 1);
     pair_kernel<<<(unsigned)std::min<uint64_t>(pair_tiles, (uint64_t)g->pair_grid), kPairThreads, 0, g->stream>>>(a);
     ++g->launches;
-    stage_end(g, 1);
     CK(cudaGetLastError());
+    {
+      WalkPrefixArgs w{};
+      w.walk_step[0] = a.walk_step[0];
+      w.walk_step[1] = a.walk_step[1];
+      w.walk_term = a.walk_term;
+      w.prefix_s[0] = pfx;
+      w.prefix_s[1] = pfx + pt_n;
+      w.prefix_t = pfx + 2 * pt_n;
+      w.tiles_cap = pse_tiles;
+      w.status = g->d_status;
+      walk_prefix_kernel<<<1, 1024, 0, g->stream>>>(w);
+      ++g->launches;
+      CK(cudaGetLastError());
+    }
+    stage_end(g, 1);
 
     // ------- depth walks (the parent walk also writes the compacted tree) -------
     const int walks = mode == kRunParse ? 1 : 2;  // the parser-mode result has no tree
@@ -455,6 +479,8 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
       pa.resolve_ticket = pa.ticket + 1;
       pa.st.flags = (unsigned *)(fb + fl.pse_flags[walk]);
       pa.super_key = (uint32_t *)(fb + fl.super_key[walk]);
+      pa.prefix_s = pfx + walk * pt_n;
+      pa.prefix_t = pfx + 2 * pt_n;
       if (g->diag) pa.phase_cycles = (unsigned long long *)g->diag_cycles.p + 8 + 8 * walk;
       const uint64_t tiles = (pa.elem_cap + kPseTile - 1) / kPseTile;
       stage_begin(g, 2 + 2 * walk);
@@ -636,7 +662,7 @@ void alpacc_gpu_free(alpacc_gpu_grammar *g) {
                     &g->arity, &g->is_term, &g->in, &g->lex_ticket, &g->st1_flag, &g->st1_state, &g->st1_vec,
                     &g->st2_flags, &g->st2_agg, &g->st2_inc, &g->tok_ids, &g->tok_starts, &g->tok_lens,
                     &g->pair_ticket, &g->pst_flags, &g->pst_agg, &g->pst_inc, &g->br, &g->pr, &g->pse_ticket,
-                    &g->pse_flags, &g->pse_agg, &g->pse_inc, &g->tile_min, &g->super_key, &g->pse_regions,
+                    &g->pse_flags, &g->pse_agg, &g->pse_inc, &g->tile_min, &g->super_key, &g->pse_regions, &g->walk_prefix,
                     &g->node_prods, &g->node_parents,
                     &g->token_parents, &g->flags, &g->diag_cycles, &g->codes, &g->tile_cnt, &g->tile_pos,
                     &g->tile_off, &g->tile_prev, &g->b_arrays, &g->b_desc, &g->b_status,

@@ -118,6 +118,7 @@ struct alpacc_gpu_grammar {
   DevBuf pair_ticket, pst_flags, pst_agg, pst_inc, br, pr;
   DevBuf pse_ticket, pse_flags, pse_agg, pse_inc, tile_min, super_key;
   DevBuf pse_regions;  // per walk tile: staircase and queries (pse_region_bytes)
+  DevBuf walk_prefix;  // per walk tile: depth prefixes of both walks, terminal-count prefix (i64)
   DevBuf node_prods, node_parents, token_parents;
   // batches: descriptor arrays, per-document statuses, packing ranges, packed results
   DevBuf b_arrays, b_desc, b_status, b_pack, b_packed;

@@ -173,9 +173,31 @@ struct PairArgs {
   PairTileState st;         // (brackets, productions)
   DeviceStatus *status;
   const BatchDesc *batch;   // null: one document; else virtual tiles (pair_tile0) and per-document regions
+  // one document: per depth-walk tile (kPseTile elements of the output) the
+  // sum of the depth steps of its brackets / productions and the number of
+  // its terminal productions, accumulated as the elements are written (zeroed
+  // before launch; null: not accumulated)
+  int *walk_step[2];
+  int *walk_term;
+  unsigned long long walk_tiles_cap;
+  const int32_t *arity;     // per production
+  const uint8_t *is_term;
 };
 
 __global__ void pair_kernel(PairArgs args);
+
+// Exclusive prefixes of the depth walks' tile aggregates (one CTA): per walk
+// tile the depth and (parents) the terminal-production count before it, so
+// that the walk kernels need no look-back.
+struct WalkPrefixArgs {
+  const int *walk_step[2];
+  const int *walk_term;
+  long long *prefix_s[2];
+  long long *prefix_t;
+  unsigned long long tiles_cap;
+  DeviceStatus *status;
+};
+__global__ void walk_prefix_kernel(WalkPrefixArgs args);
 
 // ---- previous-smaller search over depth walks: 256 threads x 8 elements ----
 // A chunk is one thread's 8 consecutive elements; per chunk the walk keeps the
@@ -217,6 +239,9 @@ struct PseArgs {
   PairTileState st;                 // (sum of steps, terminal count)
   DeviceStatus *status;
   const BatchDesc *batch;           // null: one document; else virtual tiles (br_tile0 / pr_tile0)
+  // one document: the tile's depth and terminal-count prefixes from
+  // walk_prefix_kernel (null: decoupled look-back over the tiles, st)
+  const long long *prefix_s, *prefix_t;
   // diagnostics: SM cycles of each phase of pse_tile_kernel summed over tiles
   // (thread 0's clock): 0 load + steps + scan, 1 depths + windows, 2 own and
   // previous chunk queries, 3 the warps' queued queries, 4 look-back,

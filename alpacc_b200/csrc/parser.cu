@@ -70,7 +70,9 @@ __global__ void __launch_bounds__(kPairThreads, 5) pair_kernel(PairArgs a) {
   __shared__ __align__(16) uint32_t s_rec[kPairTile];    // record per position
   __shared__ __align__(16) uint16_t s_cnt[kPairTile];    // brackets | productions << 8
   __shared__ __align__(16) uint32_t s_out[kPairOut];     // output window
+  __shared__ int s_wstep[8], s_wterm[8];                 // the window's walk-tile aggregates
   const int t = threadIdx.x;
+  const int lane = t & (kWarp - 1);
   const int L = a.q + a.k;
   const unsigned long long *rec = a.rec;
   const uint32_t *stacks = a.stacks, *prods = a.prods;
@@ -237,13 +239,94 @@ __global__ void __launch_bounds__(kPairThreads, 5) pair_kernel(PairArgs a) {
         }
         o += c;
       }
+      if (t < 8) {
+        s_wstep[t] = 0;
+        s_wterm[t] = 0;
+      }
       __syncthreads();
       const int wn = (int)(total - w0 < kPairOut ? total - w0 : kPairOut);
-      for (int i = t; i < wn; i += kPairThreads) dst[w0 + i] = s_out[i];
+      int *wstep = a.walk_step[pass];
+      if (!wstep) {
+        for (int i = t; i < wn; i += kPairThreads) dst[w0 + i] = s_out[i];
+      } else {
+        // also the walk tiles' aggregates: a warp's 32 consecutive elements
+        // lie in at most two walk tiles (reduced per tile in the warp, then
+        // added in shared memory: slots of the window's at most 4 tiles)
+        const long long gbase = (pass == 0 ? pre_b : pre_p) + w0;  // element index of s_out[0]
+        const long long tfirst = gbase / kPseTile;
+        for (int i0 = 0; i0 < wn; i0 += kPairThreads) {
+          const int i = i0 + t;
+          const bool in = i < wn;
+          int stp = 0, trm = 0, slot = 0;
+          if (in) {
+            const uint32_t v = s_out[i];
+            dst[w0 + i] = v;
+            if (pass == 0) {
+              stp = (v >> 31) ? 1 : -1;
+            } else {
+              stp = __ldg(a.arity + v) - 1;
+              trm = __ldg(a.is_term + v) ? 1 : 0;
+            }
+            slot = (int)((gbase + i) / kPseTile - tfirst);
+          }
+          const int s0 = __shfl_sync(0xffffffffu, slot, 0);
+          const bool same = slot == s0;
+          const int sa = __reduce_add_sync(0xffffffffu, same ? stp : 0);
+          const int sb = __reduce_add_sync(0xffffffffu, same ? 0 : stp);
+          const int ta = __reduce_add_sync(0xffffffffu, same ? trm : 0);
+          const int tb2 = __reduce_add_sync(0xffffffffu, same ? 0 : trm);
+          const bool two = __any_sync(0xffffffffu, in && !same);
+          if (lane == 0) {
+            atomicAdd(&s_wstep[s0], sa);
+            atomicAdd(&s_wterm[s0], ta);
+            if (two) {
+              atomicAdd(&s_wstep[s0 + 1], sb);
+              atomicAdd(&s_wterm[s0 + 1], tb2);
+            }
+          }
+        }
+        __syncthreads();
+        if (t < 8 && tfirst + t < (long long)a.walk_tiles_cap && (s_wstep[t] != 0 || s_wterm[t] != 0)) {
+          atomicAdd(wstep + tfirst + t, s_wstep[t]);
+          if (pass == 1) atomicAdd(a.walk_term + tfirst + t, s_wterm[t]);
+        }
+      }
       __syncthreads();
     }
   }
   }  // tiles
+}
+
+// Exclusive prefixes of the walk tiles' aggregates, both walks, by one CTA.
+__global__ void __launch_bounds__(1024) walk_prefix_kernel(WalkPrefixArgs a) {
+  __shared__ long long tmp[32];
+  const int t = threadIdx.x;
+  if (*reinterpret_cast<volatile int *>(&a.status->reject) || *reinterpret_cast<volatile int *>(&a.status->overflow))
+    return;  // the walks do not run
+  constexpr int kPer = 16;
+  for (int walk = 0; walk < 2; ++walk) {
+    const unsigned long long E = walk == 0 ? a.status->num_brackets : a.status->num_productions;
+    const unsigned long long tiles = (E + kPseTile - 1) / kPseTile;
+    if (tiles > a.tiles_cap) continue;  // the walk kernel records the overflow
+    const int *stp = a.walk_step[walk];
+    long long carry = 0;
+    for (unsigned long long base = 0; base < tiles; base += 1024ull * kPer) {
+      const unsigned long long i0 = base + (unsigned long long)t * kPer;
+      // (step sum, terminal count) packed: the count is non-negative and < 2^32
+      long long loc = 0;
+      for (int k = 0; k < kPer && i0 + k < tiles; ++k)
+        loc += (long long)stp[i0 + k] * (1ll << 32) + (walk == 1 ? (long long)a.walk_term[i0 + k] : 0);
+      long long tot;
+      long long run = carry + block_exclusive_scan<long long>(loc, AddI64(), 0ll, tmp, &tot);
+      for (int k = 0; k < kPer && i0 + k < tiles; ++k) {
+        const long long tc = run & 0xffffffffll;  // exact while the running count stays below 2^32
+        a.prefix_s[walk][i0 + k] = (run - tc) >> 32;
+        if (walk == 1) a.prefix_t[i0 + k] = tc;
+        run += (long long)stp[i0 + k] * (1ll << 32) + (walk == 1 ? (long long)a.walk_term[i0 + k] : 0);
+      }
+      carry += tot;
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -442,7 +525,7 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   const long long tot_t = tot & 0xffffffffll;
   const long long tot_s = (tot - tot_t) >> 32;
   // publish the aggregate at once; tile 0's aggregate is its inclusive prefix
-  if (t == 0) publish_pair(a.st, (long long)tile, Pair64{tot_s, tot_t}, lt == 0);
+  if (t == 0 && !a.prefix_s) publish_pair(a.st, (long long)tile, Pair64{tot_s, tot_t}, lt == 0);
   PSE_PHASE(0);
 
   // ---- relative depths, chunk minimum, warp windows ----
@@ -572,12 +655,17 @@ __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
 
   PSE_PHASE(3);
   // ---- the tile's prefix: look-back by warp 0, now that predecessors had time ----
+  // (or read from walk_prefix_kernel's output)
   if (t < kWarp) {
     Pair64 prefix{0, 0};
-    if (lt > 0) prefix = warp_lookback_pair(a.st, (long long)tile, Pair64{0, 0}, AddPair(), st, kSitePse);
+    if (a.prefix_s) {
+      if (t == 0) prefix = Pair64{a.prefix_s[tile], parents ? a.prefix_t[tile] : 0ll};
+    } else if (lt > 0) {
+      prefix = warp_lookback_pair(a.st, (long long)tile, Pair64{0, 0}, AddPair(), st, kSitePse);
+    }
     if (t == 0) {
       const Pair64 inc{prefix.a + tot_s, prefix.b + tot_t};
-      if (lt > 0) publish_pair(a.st, (long long)tile, inc, true);
+      if (lt > 0 && !a.prefix_s) publish_pair(a.st, (long long)tile, inc, true);
       sm.prefix_a = prefix.a;
       sm.prefix_b = prefix.b;
       if (tile0 + kPseTile >= E) {  // last tile: global checks

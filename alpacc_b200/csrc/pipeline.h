@@ -144,6 +144,8 @@ inline PairArgs pair_args(alpacc_gpu_grammar *g) {
   a.st = PairTileState{(unsigned *)g->pst_flags.p, (unsigned long long *)g->pst_agg.p,
                        (unsigned long long *)g->pst_inc.p};
   a.status = g->d_status;
+  a.arity = (const int32_t *)g->arity.p;
+  a.is_term = (const uint8_t *)g->is_term.p;
   return a;
 }
 
