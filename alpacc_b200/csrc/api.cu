@@ -84,6 +84,8 @@ int upload_tables(alpacc_gpu_grammar *g) {
   // for the scan and emit kernels
   const char *ov = std::getenv("ALPACC_LEX_OUTPUT");
   g->lex_direct = ov && std::strcmp(ov, "direct") == 0 ? 1 : 0;
+  const char *pv = std::getenv("ALPACC_WALK_PREFIX");
+  g->walk_lookback = pv && std::strcmp(pv, "lookback") == 0 ? 1 : 0;
   // ALPACC_LEX_WINDOW=sets walks windows as explicit state sets even when the
   // window machine exists (tests run that kernel on small machines too)
   const char *wv = std::getenv("ALPACC_LEX_WINDOW");
@@ -444,9 +446,12 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
     a.ticket = (unsigned *)(fb + fl.pair_ticket);
     a.st.flags = (unsigned *)(fb + fl.pst_flags);
     // the walks' tile prefixes come from the pair kernel's aggregates
-    a.walk_step[0] = (int *)(fb + fl.walk_step[0]);
-    a.walk_step[1] = (int *)(fb + fl.walk_step[1]);
-    a.walk_term = (int *)(fb + fl.walk_term);
+    // (ALPACC_WALK_PREFIX=lookback: the walks' own decoupled look-back, as
+    // batches use)
+    const bool pfx_on = !g->walk_lookback;
+    a.walk_step[0] = pfx_on ? (int *)(fb + fl.walk_step[0]) : nullptr;
+    a.walk_step[1] = pfx_on ? (int *)(fb + fl.walk_step[1]) : nullptr;
+    a.walk_term = pfx_on ? (int *)(fb + fl.walk_term) : nullptr;
     a.walk_tiles_cap = pse_tiles;
     long long *pfx = (long long *)g->walk_prefix.p;
     const uint64_t pt_n = std::max<uint64_t>(pse_tiles, 1);
@@ -454,7 +459,7 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
     pair_kernel<<<(unsigned)std::min<uint64_t>(pair_tiles, (uint64_t)g->pair_grid), kPairThreads, 0, g->stream>>>(a);
     ++g->launches;
     CK(cudaGetLastError());
-    {
+    if (pfx_on) {
       WalkPrefixArgs w{};
       w.walk_step[0] = a.walk_step[0];
       w.walk_step[1] = a.walk_step[1];
@@ -479,8 +484,8 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
       pa.resolve_ticket = pa.ticket + 1;
       pa.st.flags = (unsigned *)(fb + fl.pse_flags[walk]);
       pa.super_key = (uint32_t *)(fb + fl.super_key[walk]);
-      pa.prefix_s = pfx + walk * pt_n;
-      pa.prefix_t = pfx + 2 * pt_n;
+      pa.prefix_s = pfx_on ? pfx + walk * pt_n : nullptr;
+      pa.prefix_t = pfx_on ? pfx + 2 * pt_n : nullptr;
       if (g->diag) pa.phase_cycles = (unsigned long long *)g->diag_cycles.p + 8 + 8 * walk;
       const uint64_t tiles = (pa.elem_cap + kPseTile - 1) / kPseTile;
       stage_begin(g, 2 + 2 * walk);
