@@ -24,7 +24,7 @@ def parser(config):
 def mixed_docs(config, seed):
     rng = np.random.default_rng(seed)
     docs = []
-    for i, n in enumerate([2, 7, 60, 61, 500, 4000, 14880, 14881, 40000, 120000]):
+    for i, n in enumerate([2, 7, 60, 61, 500, 4000, 15360, 15361, 40000, 120000]):
         docs.append(cases.generated(config, n, seed * 100 + i))
     docs.append(b"")
     docs += [cases.mutate(d, rng) for d in docs[3:8]]  # rejects of every kind
