@@ -84,8 +84,12 @@ int upload_tables(alpacc_gpu_grammar *g) {
   // for the scan and emit kernels
   const char *ov = std::getenv("ALPACC_LEX_OUTPUT");
   g->lex_direct = ov && std::strcmp(ov, "direct") == 0 ? 1 : 0;
+  // ALPACC_WALK_PREFIX=pairs: the walks' tile prefixes from the pair kernel's
+  // aggregates and walk_prefix_kernel instead of the walks' own look-back
+  // (measured slower on json_ext and sexp: the aggregation costs the pair
+  // kernel more than the look-back costs the walks)
   const char *pv = std::getenv("ALPACC_WALK_PREFIX");
-  g->walk_lookback = pv && std::strcmp(pv, "lookback") == 0 ? 1 : 0;
+  g->walk_lookback = pv && std::strcmp(pv, "pairs") == 0 ? 0 : 1;
   // ALPACC_LEX_WINDOW=sets walks windows as explicit state sets even when the
   // window machine exists (tests run that kernel on small machines too)
   const char *wv = std::getenv("ALPACC_LEX_WINDOW");
@@ -445,9 +449,8 @@ int run_device_once(alpacc_gpu_grammar *g, const uint8_t *d_in, uint64_t n, int 
     a.pr_cap = pr_cap;
     a.ticket = (unsigned *)(fb + fl.pair_ticket);
     a.st.flags = (unsigned *)(fb + fl.pst_flags);
-    // the walks' tile prefixes come from the pair kernel's aggregates
-    // (ALPACC_WALK_PREFIX=lookback: the walks' own decoupled look-back, as
-    // batches use)
+    // the walks' tile prefixes: their own decoupled look-back, or (selected
+    // at load) the pair kernel's aggregates scanned by walk_prefix_kernel
     const bool pfx_on = !g->walk_lookback;
     a.walk_step[0] = pfx_on ? (int *)(fb + fl.walk_step[0]) : nullptr;
     a.walk_step[1] = pfx_on ? (int *)(fb + fl.walk_step[1]) : nullptr;

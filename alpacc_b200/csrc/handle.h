@@ -93,7 +93,7 @@ struct alpacc_gpu_grammar {
   int lex_win_words = 4;   // window before each chunk (words; 4..8)
   int lex_direct = 0;      // tokens written by the lexer kernel (look-back) instead of staged codes
   int stage_timing = 0;    // record per-stage events (alpacc_gpu_set_stage_timing)
-  int walk_lookback = 0;   // walks find their tile prefixes by look-back instead of walk_prefix_kernel
+  int walk_lookback = 1;   // walks find their tile prefixes by look-back (else walk_prefix_kernel)
   int sms = 0;             // SMs of the device
   uint64_t digest = 14695981039346656037ull;  // FNV-1a of the device tables (autotuner cache key)
   int geo_cached = 0;      // the launch geometry came from the autotuner's cache

@@ -1,10 +1,10 @@
 """The depth walks' tile prefixes on the GPU, both ways.
 
-On the single-document path the pair kernel adds each element's depth step
-(and terminal flag) to its walk tile's aggregate as it writes the element, and
-walk_prefix_kernel scans them, so the walk kernels read their prefixes;
-batches, and ALPACC_WALK_PREFIX=lookback, take the walks' own decoupled
-look-back instead. Both must give records byte-identical to the reference's C
+By default the walk kernels find their tiles' prefixes by decoupled look-back.
+With ALPACC_WALK_PREFIX=pairs (single-document path) the pair kernel instead
+adds each element's depth step (and terminal flag) to its walk tile's
+aggregate as it writes the element, walk_prefix_kernel scans them, and the
+walk kernels read their prefixes. Both must give records byte-identical to the reference's C
 backend (oracle/_ref), on inputs spanning many walk tiles, deep nesting and
 rejects.
 """
@@ -17,13 +17,13 @@ from tests import cases
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("mode", ["prefix", "lookback"])
+@pytest.mark.parametrize("mode", ["lookback", "pairs"])
 @pytest.mark.parametrize("config", ["json_ext_i32", "sexp_i64", "arithmetic_i64"])
 def test_walk_prefix_modes(gpu, config, mode, monkeypatch):
     from alpacc_b200 import workloads as W
     from alpacc_b200.native import Parser
-    if mode == "lookback":
-        monkeypatch.setenv("ALPACC_WALK_PREFIX", "lookback")
+    if mode == "pairs":
+        monkeypatch.setenv("ALPACC_WALK_PREFIX", "pairs")
     if not available(config):
         pytest.skip("oracle/_ref/lib%s.so is not built" % config)
     ref = RefOracle(config)
