@@ -91,6 +91,8 @@ def ours_serve(a, rank, world, local_rank, dist):
     rates = [int(r) for r in a.serve_rates.split(",")]
     sweep = []
     total_req = 0
+    clocks = ClockSampler(local_rank)
+    clocks.start()
     for rate in rates:
         rng = np.random.default_rng(1000 + rate)
         count = max(int(rate * a.serve_seconds), 1000)
@@ -106,6 +108,7 @@ def ours_serve(a, rank, world, local_rank, dist):
         sweep.append({"rate_per_s": rate, "requests": count, "arrival_s": float(arr[-1]), "bytes": int(nbytes),
                       "p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99), "gbs": nbytes / el / 1e9,
                       "plain_p50_ms": _pct(plat, 50), "plain_p99_ms": _pct(plat, 99), "plain_gbs": nbytes / pel / 1e9})
+    clk = clocks.stop()
     stt = srv.stats()
     srv.close()
     if rank != 0:
@@ -122,6 +125,7 @@ def ours_serve(a, rank, world, local_rank, dist):
         "serve": sweep,
         "p99_ms_at_max_rate": top["p99_ms"], "plain_p99_ms_at_max_rate": top["plain_p99_ms"],
         "served_over_plain_at_max_rate": top["gbs"] / top["plain_gbs"],
+        "clocks": clk,
         "e2e": {"value": top["gbs"], "unit": "GB/s", "h2d_bytes_per_step": top["bytes"], "d2h_bytes_per_step": None,
                 "note": "requests arrive as host buffers and results return to host memory"},
     }
