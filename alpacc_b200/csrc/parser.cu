@@ -4,7 +4,8 @@
 // pair_kernel     per token position: the (q, k) key around it, a dense-table
 //                 lookup of its stack actions and productions, and the scatter
 //                 of both into flat arrays at offsets from a decoupled
-//                 look-back scan (parser.c:60-84; parser.cu:378-449 phases A-C).
+//                 look-back scan (backends/c/parser.c:60-84; the reference's
+//                 CUDA form: backends/cuda/parser.cu:378-449, phases A-C).
 // pse_tile_kernel depth walk over brackets (+1 left, -1 right) or productions
 //                 (+arity-1), with the match of each right bracket / the parent
 //                 of each production found as the previous element whose depth
@@ -12,7 +13,7 @@
 //                 written straight into the compacted tree (compact_tree). Each
 //                 tile stores its staircase (the elements a later query can
 //                 find) and the queries it could not answer
-//                 (parser.c:74-87,103-118,126-153).
+//                 (backends/c/parser.c:74-87,103-118,126-153).
 // pse_resolve     one warp per tile with queries: 32 queries at a time walk
 //                 back over tile minima (super-tile minima skip long runs) and
 //                 binary-search the answering tile's staircase, then emit the
@@ -419,10 +420,14 @@ __device__ __forceinline__ void emit_node(const PseArgs &a, const PseDoc &dv, ui
 
 // One tile of 2048 elements: depth walk, then each query (a right bracket's
 // match, a production's parent) searched as the latest earlier element whose
-// depth is <= the query value - first in the thread's own chunk, then in
-// earlier chunks of the warp (binary descent over shuffled window minima),
-// then in earlier warps; what the tile cannot answer is queued. Parents found
-// here are emitted straight into the compacted tree.
+// depth is <= the query value - first in the thread's own chunk and the
+// previous one, then (the warp's pending queries through a shared queue, 32
+// at a time) in earlier chunks of the warp by binary descent over window
+// minima, then in earlier warps. The tile's prefix (global depth and terminal
+// count before it) comes from a decoupled look-back over the preceding tiles,
+// or from walk_prefix_kernel. The tile then stores its staircase and the
+// queries it could not answer for pse_resolve_kernel; parents found here are
+// written straight into the compacted tree.
 __global__ void __launch_bounds__(kPseThreads, 4) pse_tile_kernel(PseArgs a) {
   __shared__ unsigned s_tile;
   __shared__ PseSmem sm;
