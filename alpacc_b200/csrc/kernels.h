@@ -200,10 +200,9 @@ struct WalkPrefixArgs {
 __global__ void walk_prefix_kernel(WalkPrefixArgs args);
 
 // ---- previous-smaller search over depth walks: 256 threads x 8 elements ----
-// A chunk is one thread's 8 consecutive elements; per chunk the walk keeps the
-// depth before its first element, its minimum depth and (parents) the
-// terminal-production count before it, so that elements' depths and counts can
-// be recomputed from at most 7 neighbours instead of being stored.
+// A chunk is one thread's 8 consecutive elements; a tile is 256 chunks. Per
+// tile the walk keeps its minimum depth, its staircase and its unanswered
+// queries (PseArgs) for the resolve kernel.
 constexpr int kPseThreads = 256;
 constexpr int kPseItems = 8;
 constexpr int kPseTile = kPseThreads * kPseItems;
