@@ -64,9 +64,8 @@ def test_random_grammars_batch_equals_single(gpu, grammars):
 @pytest.mark.parametrize("nkw", [8, 16, 24, 32])
 def test_keyword_lexers(gpu, nkw):
     """C-like keyword lexers of 50, 86, 124 and 164 machine states (above 64:
-    256-bit candidate sets; the larger window machines exceed their budget,
-    so those lexers walk windows as explicit state sets), in all three modes
-    against the oracle, on inputs up to several lexer tiles."""
+    256-bit candidate sets; window machines of up to 347 sets), in all three
+    modes against the oracle, on inputs up to several lexer tiles."""
     from alpacc_b200.native import Parser
     from tests.random_grammars import keyword_grammar, keyword_inputs
     text = keyword_grammar(nkw)

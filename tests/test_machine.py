@@ -245,6 +245,18 @@ def test_window_machine_tables(harness):
         assert 0 < sets <= 1024 and singles > 0 and bad == 0, (config, info)
 
 
+def test_window_machine_tables_random_and_keyword_grammars(harness):
+    """The same entry check for 16 random grammars and the keyword lexers of
+    8, 24 and 32 keywords (up to 347 sets), all within the budget."""
+    grammars = [t for _, _, t in fuzz_grammars(16)]
+    grammars += [generate_parts(keyword_grammar(k), "kw%d" % k, False, "both") for k in (8, 24, 32)]
+    for t in grammars:
+        s, keep = native.make_tables(t)
+        info = np.zeros(4, dtype=np.int64)
+        assert harness.window_info(ctypes.byref(s), info.ctypes.data) == 0, t.name
+        assert info[3] == 0 and 0 < info[0] <= 1024, (t.name, info)
+
+
 def test_lexer_tile_algorithm_rejects_and_lengths(harness, emu):
     from alpacc_b200 import workloads as W
     t = cases.tables("json_ext_i32")
@@ -256,10 +268,11 @@ def test_lexer_tile_algorithm_rejects_and_lengths(harness, emu):
 @pytest.mark.parametrize("nkw", [8, 24, 32])
 def test_lexer_tile_algorithm_keyword_lexers(harness, emu, nkw):
     """Machines above 64 states (256-bit candidate sets) and many candidates;
-    the 32-keyword machine's window machine exceeds its budget, so it walks
-    windows as state sets."""
+    both window walks (the window machine, and explicit state sets)."""
     t = generate_parts(keyword_grammar(nkw), "kw%d" % nkw, False, "both")
-    _emu_vs_machine(emu, harness, t, keyword_inputs(nkw, seed=nkw, sizes=(0, 1, 20, 300, 15000, 40000)))
+    ins = keyword_inputs(nkw, seed=nkw, sizes=(0, 1, 20, 300, 15000, 40000))
+    _emu_vs_machine(emu, harness, t, ins)
+    _emu_vs_machine(emu, harness, t, ins, sets=True)
 
 
 def test_lexer_tile_algorithm_random_grammars(harness, emu):
